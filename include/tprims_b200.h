@@ -1,0 +1,282 @@
+/* libtprims_b200: a B200 (sm_100a) executor behind the TAPP C ABI of libtprims.
+ *
+ * Every entry point is plain C: integer handles (intptr_t), raw pointers and
+ * sizes. Nothing here names a CUDA, PyTorch or C++ type, so a C, Rust, Julia or
+ * Python host binds it exactly as it binds the CPU libtprims.
+ *
+ * Part 1 repeats the standard TAPP declarations (numeric values and prototypes
+ * are ABI and are kept identical to the pinned upstream headers the reference
+ * ships in crates/tprims-capi/include/tapp/*.h). When the upstream <tapp.h> has
+ * already been included, part 1 is skipped and its declarations are used.
+ *
+ * Part 2 repeats the tprims extensions of crates/tprims-capi/include/tprims/
+ * core.h and tapp_ext.h (status codes, last error, ABI version, DLPack borrows,
+ * the pooled-executor constructor).
+ *
+ * Part 3 is new to this library: a CUDA executor, the DLPack execute call that
+ * accepts kDLCUDA operands, the precision-scheme setter (plain, 3xBF16, 6xBF16,
+ * Ozaki INT8), the plan report, the dot_general front end, the batched list
+ * call and the vector-Jacobian product. */
+#ifndef TPRIMS_B200_H
+#define TPRIMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+#define TPRIMS_B200_EXPORT extern "C" __attribute__((visibility("default")))
+#else
+#define TPRIMS_B200_EXPORT __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------ part 1 */
+#ifndef TAPP_TAPP_H_
+#define TAPP_TAPP_H_
+
+typedef int TAPP_error;
+typedef intptr_t TAPP_handle;
+typedef intptr_t TAPP_executor;
+typedef intptr_t TAPP_status;
+typedef intptr_t TAPP_tensor_info;
+typedef intptr_t TAPP_tensor_product;
+typedef intptr_t TAPP_attr;
+typedef int TAPP_key;
+typedef int TAPP_datatype;
+typedef int TAPP_prectype;
+typedef int TAPP_element_op;
+
+/* tapp/datatype.h */
+enum { TAPP_F32 = 0, TAPP_F64 = 1, TAPP_C32 = 2, TAPP_C64 = 3, TAPP_F16 = 4, TAPP_BF16 = 5 };
+enum {
+  TAPP_DEFAULT_PREC = -1,
+  TAPP_F32F32_ACCUM_F32 = 0,
+  TAPP_F64F64_ACCUM_F64 = 1,
+  TAPP_F16F16_ACCUM_F16 = 4,
+  TAPP_F16F16_ACCUM_F32 = 5,
+  TAPP_BF16BF16_ACCUM_F32 = 6
+};
+/* tapp/product.h */
+enum { TAPP_IDENTITY = 0, TAPP_CONJUGATE = 1 };
+#define TAPP_IN_PLACE NULL
+
+/* tapp/error.h — crates/tprims-capi/src/status.rs:69 and :81 */
+TPRIMS_B200_EXPORT bool TAPP_check_success(TAPP_error error);
+TPRIMS_B200_EXPORT size_t TAPP_explain_error(TAPP_error error, size_t maxlen, char* message);
+/* tapp/attributes.h — crates/tprims-capi/src/handle.rs:83-127 (every key refused) */
+TPRIMS_B200_EXPORT TAPP_error TAPP_attr_set(TAPP_attr attr, TAPP_key key, void* value);
+TPRIMS_B200_EXPORT TAPP_error TAPP_attr_get(TAPP_attr attr, TAPP_key key, void** value);
+TPRIMS_B200_EXPORT TAPP_error TAPP_attr_clear(TAPP_attr attr, TAPP_key key);
+/* tapp/handle.h — crates/tprims-capi/src/handle.rs:35 and :52 */
+TPRIMS_B200_EXPORT TAPP_error TAPP_create_handle(TAPP_handle* handle);
+TPRIMS_B200_EXPORT TAPP_error TAPP_destroy_handle(TAPP_handle handle);
+/* tapp/executor.h — crates/tprims-capi/src/executor.rs:278 and :299. Here an
+   executor is one CUDA stream on the current device plus its workspace. */
+TPRIMS_B200_EXPORT TAPP_error TAPP_create_executor(TAPP_executor* exec);
+TPRIMS_B200_EXPORT TAPP_error TAPP_destroy_executor(TAPP_executor exec);
+/* tapp/status.h — crates/tprims-capi/src/handle.rs:133 (a no-op: execution is synchronous) */
+TPRIMS_B200_EXPORT TAPP_error TAPP_destroy_status(TAPP_status status);
+/* tapp/tensor.h — crates/tprims-capi/src/tensor_info.rs:58-221 */
+TPRIMS_B200_EXPORT TAPP_error TAPP_create_tensor_info(TAPP_tensor_info* info, TAPP_datatype type, int nmode,
+                                                      const int64_t* extents, const int64_t* strides);
+TPRIMS_B200_EXPORT TAPP_error TAPP_destroy_tensor_info(TAPP_tensor_info info);
+TPRIMS_B200_EXPORT int TAPP_get_nmodes(TAPP_tensor_info info);
+TPRIMS_B200_EXPORT TAPP_error TAPP_set_nmodes(TAPP_tensor_info info, int nmodes);
+TPRIMS_B200_EXPORT void TAPP_get_extents(TAPP_tensor_info info, int64_t* extents);
+TPRIMS_B200_EXPORT TAPP_error TAPP_set_extents(TAPP_tensor_info info, const int64_t* extents);
+TPRIMS_B200_EXPORT void TAPP_get_strides(TAPP_tensor_info info, int64_t* strides);
+TPRIMS_B200_EXPORT TAPP_error TAPP_set_strides(TAPP_tensor_info info, const int64_t* strides);
+/* tapp/product.h — crates/tprims-capi/src/product.rs:83 and :198 */
+TPRIMS_B200_EXPORT TAPP_error TAPP_create_tensor_product(
+    TAPP_tensor_product* plan, TAPP_handle handle, TAPP_element_op op_A, TAPP_tensor_info A, const int64_t* idx_A,
+    TAPP_element_op op_B, TAPP_tensor_info B, const int64_t* idx_B, TAPP_element_op op_C, TAPP_tensor_info C,
+    const int64_t* idx_C, TAPP_element_op op_D, TAPP_tensor_info D, const int64_t* idx_D, TAPP_prectype prec);
+TPRIMS_B200_EXPORT TAPP_error TAPP_destroy_tensor_product(TAPP_tensor_product plan);
+/* crates/tprims-capi/src/execute.rs:192. Synchronous: returns when D is written. */
+TPRIMS_B200_EXPORT TAPP_error TAPP_execute_product(TAPP_tensor_product plan, TAPP_executor exec, TAPP_status* status,
+                                                   const void* alpha, const void* A, const void* B, const void* beta,
+                                                   const void* C, void* D);
+/* crates/tprims-capi/src/execute.rs:235. Items are validated first, then run. */
+TPRIMS_B200_EXPORT TAPP_error TAPP_execute_batched_product(TAPP_tensor_product plan, TAPP_executor exec,
+                                                           TAPP_status* status, int num_batches, const void* alpha,
+                                                           const void** A, const void** B, const void* beta,
+                                                           const void** C, void** D);
+#endif /* TAPP_TAPP_H_ */
+
+/* ------------------------------------------------------------------ part 2 */
+#ifndef TPRIMS_CORE_H
+#define TPRIMS_CORE_H
+#define TPRIMS_ABI_VERSION 100 /* 0.1.0, crates/tprims-capi/src/lib.rs:140 */
+
+typedef int32_t tprims_status;
+/* crates/tprims-capi/src/status.rs:13-43 */
+#define TPRIMS_OK 0
+#define TPRIMS_ERR_INVALID_ARGUMENT 1
+#define TPRIMS_ERR_SHAPE 2
+#define TPRIMS_ERR_DTYPE 3
+#define TPRIMS_ERR_DEVICE 4
+#define TPRIMS_ERR_READ_ONLY 5
+#define TPRIMS_ERR_ALIASED 6
+#define TPRIMS_ERR_WOULD_MATERIALIZE 7
+#define TPRIMS_ERR_NUMERICAL 8
+#define TPRIMS_BUSY 9
+#define TPRIMS_ERR_WOULD_DEADLOCK 10
+#define TPRIMS_ERR_PANIC 12
+#define TPRIMS_ERR_INTERNAL 13
+#define TPRIMS_ERR_LABELS 14
+#define TPRIMS_ERR_UNSUPPORTED 15
+
+/* DLPack 1.x ABI subset (the struct layouts are the DLPack standard's). */
+#ifndef DLPACK_DLPACK_H_
+#define DLPACK_DLPACK_H_
+typedef enum { kDLCPU = 1, kDLCUDA = 2, kDLCUDAHost = 3, kDLCUDAManaged = 13 } DLDeviceType;
+typedef struct { DLDeviceType device_type; int32_t device_id; } DLDevice;
+typedef enum { kDLInt = 0, kDLUInt = 1, kDLFloat = 2, kDLBfloat = 4, kDLComplex = 5, kDLBool = 6 } DLDataTypeCode;
+typedef struct { uint8_t code; uint8_t bits; uint16_t lanes; } DLDataType;
+typedef struct {
+  void* data;
+  DLDevice device;
+  int32_t ndim;
+  DLDataType dtype;
+  int64_t* shape;
+  int64_t* strides;
+  uint64_t byte_offset;
+} DLTensor;
+typedef struct { uint32_t major; uint32_t minor; } DLPackVersion;
+typedef struct DLManagedTensorVersioned {
+  DLPackVersion version;
+  void* manager_ctx;
+  void (*deleter)(struct DLManagedTensorVersioned* self);
+  uint64_t flags;
+  DLTensor dl_tensor;
+} DLManagedTensorVersioned;
+#endif
+
+/* crates/tprims-capi/include/tprims/core.h: a borrowed operand, never freed here. */
+typedef struct { DLTensor* view; uint64_t flags; } tprims_tensor;
+TPRIMS_B200_EXPORT tprims_tensor tprims_tensor_borrow_versioned(DLManagedTensorVersioned* m); /* tensor.rs:26 */
+TPRIMS_B200_EXPORT tprims_tensor tprims_tensor_borrow_raw(DLTensor* t, uint64_t flags);       /* tensor.rs:55 */
+TPRIMS_B200_EXPORT const char* tprims_last_error(void);                                      /* status.rs:168 */
+TPRIMS_B200_EXPORT uint32_t tprims_abi_version(void);                                        /* lib.rs:143 */
+TPRIMS_B200_EXPORT int32_t tprims_has_part(const char* part);                                /* lib.rs:154 */
+TPRIMS_B200_EXPORT const char* TAPP_implementation_name(void);                               /* handle.rs:141 */
+TPRIMS_B200_EXPORT const char* TAPP_implementation_version(void);                            /* handle.rs:158 */
+#endif /* TPRIMS_CORE_H */
+
+#ifndef TPRIMS_TAPP_EXT_H
+#define TPRIMS_TAPP_EXT_H
+typedef struct { size_t stack_size; } tprims_rayon_opts;
+/* crates/tprims-capi/src/executor.rs:320-392. Kept for source compatibility:
+   nthreads == 0 is refused as in the reference; otherwise a CUDA executor on the
+   current device is created and nthreads is recorded as its host budget. */
+TPRIMS_B200_EXPORT TAPP_error tprims_tapp_executor_create_rayon(TAPP_executor* out, size_t nthreads,
+                                                                const tprims_rayon_opts* opts);
+TPRIMS_B200_EXPORT TAPP_error tprims_tapp_executor_set_budget(TAPP_executor exec, size_t budget);
+TPRIMS_B200_EXPORT TAPP_error tprims_tapp_executor_get_threads(TAPP_executor exec, size_t* pool_size,
+                                                               size_t* budget);
+#endif /* TPRIMS_TAPP_EXT_H */
+
+/* ------------------------------------------------------------------ part 3 */
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Executor on CUDA device `device` (-1 = the current device). `stream` is a
+   cudaStream_t passed as an integer; 0 makes the executor create its own
+   non-blocking stream. No reference counterpart: the reference's executors are
+   CPU thread pools (executor.rs:278-392). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_create(TAPP_executor* out, int device, uintptr_t stream);
+/* The executor's stream, as an integer cudaStream_t. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_stream(TAPP_executor exec, uintptr_t* stream);
+/* Execution mode of an executor: 1 = synchronous (the TAPP default: every
+   execute returns after the stream is drained), 0 = asynchronous (device
+   operands only; the call returns once the work is enqueued). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_sync(TAPP_executor exec, int sync);
+/* Drain the executor's stream and report any kernel-side error status word. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_synchronize(TAPP_executor exec);
+
+/* Per-kernel timing (diagnostics, off by default): with `on` != 0 the executor
+   records CUDA events on its stream around every kernel launch. The totals
+   are resolved whenever the stream is drained. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_profiling(TAPP_executor exec, int on);
+/* JSON {"kernel family": {"ms": total, "launches": n}, ...} of the resolved
+   totals (the stream is drained first); `reset` != 0 clears them. Returns the
+   full length, like snprintf. */
+TPRIMS_B200_EXPORT size_t tprims_b200_executor_kernel_times(TAPP_executor exec, char* buf, size_t maxlen, int reset);
+
+/* Precision schemes. PLAIN is the drop-in (FP32 SIMT / FP64 DMMA, complex by
+   four real products); the others are split-precision tensor-core schemes whose
+   error bound is stated in the plan report. */
+enum {
+  TPRIMS_PREC_PLAIN = 0,
+  TPRIMS_PREC_BF16X3 = 1, /* f32/c32: hi/lo BF16 split, 3 products, FP32 accumulation */
+  TPRIMS_PREC_BF16X6 = 2, /* f32/c32: 3-way BF16 split, 6 products, FP32 accumulation */
+  TPRIMS_PREC_OZAKI_INT8 = 3 /* f64/c64: INT8 slices, exact INT32 accumulation */
+};
+/* Choose the precision scheme of a product. `slices` is the INT8 slice count
+   for TPRIMS_PREC_OZAKI_INT8 (0 = the default for the dtype) and is ignored
+   otherwise. Refused (UNSUPPORTED) for a dtype the scheme does not apply to.
+   The reference has no counterpart (its C ABI has no tuning call, product.rs:48). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan, int scheme, int slices);
+/* Pin the CTA tile (0 = autotuned). Rows/cols are the oriented M/N tile. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);
+/* A NUL-terminated JSON description of the plan (the counterpart of
+   Plan::report, crates/tprims-contract/src/plan/mod.rs:237). Returns the full
+   length, like snprintf. */
+TPRIMS_B200_EXPORT size_t tprims_b200_product_report(TAPP_tensor_product plan, char* buf, size_t maxlen);
+
+/* Problem::from_dot_general (crates/tprims-contract/src/api/problem.rs:396):
+   D has extents [lhs_free, rhs_free, batch]; C is D itself (CSpec::Output).
+   `*_contract` and `*_batch` are axis lists of A and B. Produces a product
+   usable with TAPP_execute_product (C = NULL overwrites D; C = D accumulates in
+   place). dtype is a TAPP_datatype. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_from_dot_general(
+    TAPP_tensor_product* plan, TAPP_datatype dtype, int rank_a, const int64_t* ext_a, const int64_t* str_a,
+    TAPP_element_op op_a, int rank_b, const int64_t* ext_b, const int64_t* str_b, TAPP_element_op op_b, int rank_d,
+    const int64_t* ext_d, const int64_t* str_d, TAPP_element_op op_d, int n_contract, const int64_t* lhs_contract,
+    const int64_t* rhs_contract, int n_batch, const int64_t* lhs_batch, const int64_t* rhs_batch);
+
+/* Inspection for tests and diagnostics: copy scatter vector `which` of the
+   packed plan before orientation (0 a_m, 1 a_k, 2 b_k, 3 b_n, 4 c_m, 5 c_n,
+   6 d_m, 7 d_n, 8 h_a, 9 h_b, 10 h_c, 11 h_d; the fields of PackedPlan,
+   crates/tprims-contract/src/plan/analysis.rs:139-150) into `out` (at most
+   `cap` entries). Returns the vector's length, or -1 for a bad argument. */
+TPRIMS_B200_EXPORT int64_t tprims_b200_product_scatter(TAPP_tensor_product plan, int which, int64_t* out,
+                                                       int64_t cap);
+
+/* DLPack execution (the extension the reference declines: dlpack.rs:87 rejects
+   kDLCUDA). Operands are kDLCUDA on the executor's device, kDLCUDAHost or
+   kDLCPU; lanes == 1; NULL strides mean row-major; C.view may be NULL only with
+   a zero beta. The tensors' shapes and strides must equal the plan's. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_execute_product_dlpack(TAPP_tensor_product plan, TAPP_executor exec,
+                                                                 TAPP_status* status, const void* alpha,
+                                                                 tprims_tensor A, tprims_tensor B, const void* beta,
+                                                                 tprims_tensor C, tprims_tensor D);
+
+/* contract_batched (crates/tprims-contract/src/batch.rs:125): a heterogeneous
+   list, validated all-or-nothing before any D is written, then executed as one
+   grouped submission on the executor's stream. */
+typedef struct {
+  TAPP_tensor_product plan;
+  const void* alpha;
+  const void* A;
+  const void* B;
+  const void* beta;
+  const void* C;
+  void* D;
+} tprims_b200_batch_item;
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_contract_batched(TAPP_executor exec, int n,
+                                                           const tprims_b200_batch_item* items);
+
+/* Plan::vjp. For D = alpha*op_A(A)*op_B(B) (+ beta*C), given the cotangent dD,
+   write dA (when non-NULL) and dB (when non-NULL) in the layouts of A and B:
+   dA = conj-correct adjoint contraction of dD with B, scattered onto A's
+   repeated-index diagonal (every element off the diagonal is set to zero), and
+   likewise dB. No reference counterpart (the reference has no AD). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_vjp(TAPP_tensor_product plan, TAPP_executor exec, const void* alpha,
+                                                      const void* A, const void* B, const void* dD, void* dA, void* dB);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TPRIMS_B200_H */

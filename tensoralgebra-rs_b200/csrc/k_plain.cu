@@ -1,0 +1,376 @@
+// Plain (drop-in precision) contraction kernels: one launch per contraction,
+// one CTA per (batch, M tile, N tile), the whole K loop inside the CTA.
+//
+// The gather stage replaces the reference's packing (crates/tprims-kernel/src/
+// pack/pack.rs:152-203): each K step reads A'[m, k] = A[h_a + a_m[m] + a_k[k]]
+// and B'[k, n] through the scatter vectors straight into shared memory, with
+// threads running along whichever index is unit-stride in memory, and folds
+// conjugation into the sign of the imaginary plane. The register tile replaces
+// the microkernels (kernels/reference/scalar.rs:31-175): FP32 FFMA for f32,
+// FP64 DMMA (mma.sync m8n8k4) for f64, and four real products per complex MAC
+// for c32/c64 (the planar method, writeback.rs:54-97 Planar). The epilogue is
+// the scatter write-back (writeback.rs:311-486) applied once per element after
+// the full K loop.
+#include "device_common.cuh"
+
+namespace tprims {
+namespace dev {
+
+namespace {
+
+// Gather of one ROWS x BK tile (A': rows = m; B': rows = n) into registers,
+// then into planar shared memory laid out [k][row].
+template <class R, bool CPLX, int ROWS, int BK, int NT>
+struct TileGather {
+  using T = typename Elem<R, CPLX>::type;
+  static constexpr int PER = ROWS * BK / NT;
+  static_assert(ROWS * BK % NT == 0, "tile must split evenly over threads");
+  R re[PER];
+  R im[CPLX ? PER : 1];
+
+  __device__ inline void load(const T* base, const int64_t* rows_s, const int64_t* kscat, int64_t row0,
+                              int64_t nrows, int64_t k0, int64_t K, int kfast, int conj, int tid) {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int idx = tid + j * NT;
+      const int kk = kfast ? (idx % BK) : (idx / ROWS);
+      const int rr = kfast ? (idx / BK) : (idx % ROWS);
+      const int64_t r = row0 + rr, k = k0 + kk;
+      R vr = R(0), vi = R(0);
+      if (r < nrows && k < K) {
+        Elem<R, CPLX>::load(base + rows_s[rr] + __ldg(kscat + k), vr, vi);
+        if (conj) vi = -vi;
+      }
+      re[j] = vr;
+      if (CPLX) im[j] = vi;
+    }
+  }
+
+  __device__ inline void store(R* s_re, R* s_im, int stride, int kfast, int tid) const {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int idx = tid + j * NT;
+      const int kk = kfast ? (idx % BK) : (idx / ROWS);
+      const int rr = kfast ? (idx / BK) : (idx % ROWS);
+      s_re[kk * stride + rr] = re[j];
+      if (CPLX) s_im[kk * stride + rr] = im[j];
+    }
+  }
+};
+
+// ---------------------------------------------------------------- SIMT (FFMA)
+
+template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+simt_gemm_kernel(GemmArgs g) {
+  constexpr int NT = (BM / TM) * (BN / TN);
+  constexpr int PAD = 4;
+  constexpr int SA = BM + PAD, SB = BN + PAD;
+  constexpr int NPL = CPLX ? 2 : 1;
+  using T = typename Elem<R, CPLX>::type;
+
+  __shared__ __align__(16) R As[2][NPL][BK * SA];
+  __shared__ __align__(16) R Bs[2][NPL][BK * SB];
+  __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
+
+  const int tid = threadIdx.x;
+  const int64_t h = blockIdx.z;
+  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+
+  for (int i = tid; i < BM; i += NT) {
+    const int64_t m = m0 + i;
+    const bool ok = m < g.M;
+    am_s[i] = ok ? g.s.a_m[m] : 0;
+    dm_s[i] = ok ? g.s.d_m[m] : 0;
+    cm_s[i] = ok ? g.s.c_m[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int64_t n = n0 + i;
+    const bool ok = n < g.N;
+    bn_s[i] = ok ? g.s.b_n[n] : 0;
+    dn_s[i] = ok ? g.s.d_n[n] : 0;
+    cn_s[i] = ok ? g.s.c_n[n] : 0;
+  }
+  __syncthreads();
+
+  const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
+  const T* Bb = static_cast<const T*>(g.B) + g.s.h_b[h];
+
+  TileGather<R, CPLX, BM, BK, NT> ga;
+  TileGather<R, CPLX, BN, BK, NT> gb;
+
+  constexpr int HM = TM / 2, HN = TN / 2;
+  const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+  R acc_re[TM][TN], acc_im[CPLX ? TM : 1][CPLX ? TN : 1];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      acc_re[i][j] = R(0);
+      if (CPLX) acc_im[i][j] = R(0);
+    }
+
+  const int64_t nt = (g.K + BK - 1) / BK;
+  ga.load(Ab, am_s, g.s.a_k, m0, g.M, 0, g.K, g.a_kfast, g.conj_a, tid);
+  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
+  ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
+  gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
+  __syncthreads();
+
+  for (int64_t t = 0; t < nt; ++t) {
+    const int buf = (int)(t & 1);
+    if (t + 1 < nt) {
+      ga.load(Ab, am_s, g.s.a_k, m0, g.M, (t + 1) * BK, g.K, g.a_kfast, g.conj_a, tid);
+      gb.load(Bb, bn_s, g.s.b_k, n0, g.N, (t + 1) * BK, g.K, g.b_kfast, g.conj_b, tid);
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      R ar[TM], br[TN], ai[CPLX ? TM : 1], bi[CPLX ? TN : 1];
+#pragma unroll
+      for (int i = 0; i < HM; ++i) {
+        ar[i] = As[buf][0][kk * SA + tx * HM + i];
+        ar[HM + i] = As[buf][0][kk * SA + BM / 2 + tx * HM + i];
+        if (CPLX) {
+          ai[i] = As[buf][NPL - 1][kk * SA + tx * HM + i];
+          ai[HM + i] = As[buf][NPL - 1][kk * SA + BM / 2 + tx * HM + i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < HN; ++j) {
+        br[j] = Bs[buf][0][kk * SB + ty * HN + j];
+        br[HN + j] = Bs[buf][0][kk * SB + BN / 2 + ty * HN + j];
+        if (CPLX) {
+          bi[j] = Bs[buf][NPL - 1][kk * SB + ty * HN + j];
+          bi[HN + j] = Bs[buf][NPL - 1][kk * SB + BN / 2 + ty * HN + j];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+          if (CPLX) {
+            acc_re[i][j] = fma(ar[i], br[j], acc_re[i][j]);
+            acc_re[i][j] = fma(-ai[i], bi[j], acc_re[i][j]);
+            acc_im[i][j] = fma(ar[i], bi[j], acc_im[i][j]);
+            acc_im[i][j] = fma(ai[i], br[j], acc_im[i][j]);
+          } else {
+            acc_re[i][j] = fma(ar[i], br[j], acc_re[i][j]);
+          }
+        }
+    }
+    if (t + 1 < nt) {
+      ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
+      gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
+    }
+    __syncthreads();
+  }
+
+  const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
+  T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int rr = (i < HM) ? (tx * HM + i) : (BM / 2 + tx * HM + (i - HM));
+    if (m0 + rr >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int cc = (j < HN) ? (ty * HN + j) : (BN / 2 + ty * HN + (j - HN));
+      if (n0 + cc >= g.N) continue;
+      epilogue_store<R, CPLX>(g.e, acc_re[i][j], CPLX ? acc_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
+                              Db + dm_s[rr] + dn_s[cc]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- FP64 DMMA
+
+__device__ inline void dmma_884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 8x8 DMMA tiles.
+template <bool CPLX, int WM, int WN, int BK>
+__global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
+  constexpr int BM = 2 * WM, BN = 2 * WN, NT = 128;
+  constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
+  constexpr int NPL = CPLX ? 2 : 1;
+  constexpr int TI = WM / 8, TJ = WN / 8;
+  using T = typename Elem<double, CPLX>::type;
+
+  __shared__ __align__(16) double As[2][NPL][BK * SA];
+  __shared__ __align__(16) double Bs[2][NPL][BK * SB];
+  __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t h = blockIdx.z;
+  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+  const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
+
+  for (int i = tid; i < BM; i += NT) {
+    const int64_t m = m0 + i;
+    const bool ok = m < g.M;
+    am_s[i] = ok ? g.s.a_m[m] : 0;
+    dm_s[i] = ok ? g.s.d_m[m] : 0;
+    cm_s[i] = ok ? g.s.c_m[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int64_t n = n0 + i;
+    const bool ok = n < g.N;
+    bn_s[i] = ok ? g.s.b_n[n] : 0;
+    dn_s[i] = ok ? g.s.d_n[n] : 0;
+    cn_s[i] = ok ? g.s.c_n[n] : 0;
+  }
+  __syncthreads();
+
+  const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
+  const T* Bb = static_cast<const T*>(g.B) + g.s.h_b[h];
+  TileGather<double, CPLX, BM, BK, NT> ga;
+  TileGather<double, CPLX, BN, BK, NT> gb;
+
+  double cr[TI][TJ][2], ci[CPLX ? TI : 1][CPLX ? TJ : 1][2];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int j = 0; j < TJ; ++j) {
+      cr[i][j][0] = cr[i][j][1] = 0.0;
+      if (CPLX) ci[i][j][0] = ci[i][j][1] = 0.0;
+    }
+
+  const int64_t nt = (g.K + BK - 1) / BK;
+  ga.load(Ab, am_s, g.s.a_k, m0, g.M, 0, g.K, g.a_kfast, g.conj_a, tid);
+  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
+  ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
+  gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
+  __syncthreads();
+
+  const int fr = lane >> 2, fk = lane & 3;
+  for (int64_t t = 0; t < nt; ++t) {
+    const int buf = (int)(t & 1);
+    if (t + 1 < nt) {
+      ga.load(Ab, am_s, g.s.a_k, m0, g.M, (t + 1) * BK, g.K, g.a_kfast, g.conj_a, tid);
+      gb.load(Bb, bn_s, g.s.b_k, n0, g.N, (t + 1) * BK, g.K, g.b_kfast, g.conj_b, tid);
+    }
+#pragma unroll
+    for (int kq = 0; kq < BK / 4; ++kq) {
+      const int krow = kq * 4 + fk;
+      double a_re[TI], b_re[TJ], a_im[CPLX ? TI : 1], b_im[CPLX ? TJ : 1];
+#pragma unroll
+      for (int i = 0; i < TI; ++i) {
+        a_re[i] = As[buf][0][krow * SA + wm0 + i * 8 + fr];
+        if (CPLX) a_im[i] = As[buf][NPL - 1][krow * SA + wm0 + i * 8 + fr];
+      }
+#pragma unroll
+      for (int j = 0; j < TJ; ++j) {
+        b_re[j] = Bs[buf][0][krow * SB + wn0 + j * 8 + fr];
+        if (CPLX) b_im[j] = Bs[buf][NPL - 1][krow * SB + wn0 + j * 8 + fr];
+      }
+#pragma unroll
+      for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) {
+          dmma_884(cr[i][j][0], cr[i][j][1], a_re[i], b_re[j]);
+          if (CPLX) {
+            dmma_884(cr[i][j][0], cr[i][j][1], -a_im[i], b_im[j]);
+            dmma_884(ci[i][j][0], ci[i][j][1], a_re[i], b_im[j]);
+            dmma_884(ci[i][j][0], ci[i][j][1], a_im[i], b_re[j]);
+          }
+        }
+    }
+    if (t + 1 < nt) {
+      ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
+      gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
+    }
+    __syncthreads();
+  }
+
+  const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
+  T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
+#pragma unroll
+  for (int i = 0; i < TI; ++i) {
+    const int rr = wm0 + i * 8 + fr;
+    if (m0 + rr >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TJ; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int cc = wn0 + j * 8 + fk * 2 + q;
+        if (n0 + cc >= g.N) continue;
+        epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
+                                     Db + dm_s[rr] + dn_s[cc]);
+      }
+  }
+}
+
+template <int BM, int BN>
+dim3 grid_for(const GemmArgs& g) {
+  return dim3((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM), (unsigned)g.H);
+}
+
+}  // namespace
+
+const char* plain_kernel_name(int k) {
+  switch (k) {
+    case PLAIN_F32_SIMT_128x128: return "sm100.f32.simt.128x128x8";
+    case PLAIN_F32_SIMT_64x64: return "sm100.f32.simt.64x64x8";
+    case PLAIN_F64_DMMA_64x64: return "sm100.f64.dmma884.64x64x16";
+    case PLAIN_F64_DMMA_32x32: return "sm100.f64.dmma884.32x32x16";
+    case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.planar.64x64x8";
+    case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.planar.64x32x8";
+    case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
+  }
+  return "auto";
+}
+
+int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms) {
+  auto tiles = [&](int bm, int bn) { return ((M + bm - 1) / bm) * ((N + bn - 1) / bn) * H; };
+  (void)K;
+  switch (dtype) {
+    case 0: return tiles(128, 128) >= num_sms ? PLAIN_F32_SIMT_128x128 : PLAIN_F32_SIMT_64x64;
+    case 1: return tiles(64, 64) >= num_sms ? PLAIN_F64_DMMA_64x64 : PLAIN_F64_DMMA_32x32;
+    case 2: return PLAIN_C32_SIMT_64x64;
+    case 3: return tiles(64, 32) >= num_sms ? PLAIN_C64_DMMA_64x32 : PLAIN_C64_DMMA_32x32;
+  }
+  return PLAIN_AUTO;
+}
+
+cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.H <= 0) return cudaSuccess;
+  if (g.H > 65535) return cudaErrorInvalidConfiguration;
+  switch (kernel) {
+    case PLAIN_F32_SIMT_128x128:
+      if (dtype != 0) return cudaErrorInvalidValue;
+      simt_gemm_kernel<float, false, 128, 128, 8, 8, 8><<<grid_for<128, 128>(g), 256, 0, st>>>(g);
+      break;
+    case PLAIN_F32_SIMT_64x64:
+      if (dtype != 0) return cudaErrorInvalidValue;
+      simt_gemm_kernel<float, false, 64, 64, 8, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
+      break;
+    case PLAIN_C32_SIMT_64x64:
+      if (dtype != 2) return cudaErrorInvalidValue;
+      simt_gemm_kernel<float, true, 64, 64, 8, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
+      break;
+    case PLAIN_F64_DMMA_64x64:
+      if (dtype != 1) return cudaErrorInvalidValue;
+      dmma_gemm_kernel<false, 32, 32, 16><<<grid_for<64, 64>(g), 128, 0, st>>>(g);
+      break;
+    case PLAIN_F64_DMMA_32x32:
+      if (dtype != 1) return cudaErrorInvalidValue;
+      dmma_gemm_kernel<false, 16, 16, 16><<<grid_for<32, 32>(g), 128, 0, st>>>(g);
+      break;
+    case PLAIN_C64_DMMA_64x32:
+      if (dtype != 3) return cudaErrorInvalidValue;
+      dmma_gemm_kernel<true, 32, 16, 8><<<grid_for<64, 32>(g), 128, 0, st>>>(g);
+      break;
+    case PLAIN_C64_DMMA_32x32:
+      if (dtype != 3) return cudaErrorInvalidValue;
+      dmma_gemm_kernel<true, 16, 16, 8><<<grid_for<32, 32>(g), 128, 0, st>>>(g);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace tprims

@@ -1,0 +1,412 @@
+// Split-precision f32 contraction on the sm_100a tensor cores.
+//
+// f32 operands are split into BF16 planes, x = x0 + x1 (+ x2), and the
+// product is accumulated in FP32 from a subset of the plane products:
+//   bf16x3: x0*y0 + x0*y1 + x1*y0                       (2 planes, 3 products)
+//   bf16x6: bf16x3 + x0*y2 + x1*y1 + x2*y0              (3 planes, 6 products)
+// Each plane keeps the next 8 significant bits of the remainder, so bf16x6
+// carries 24 bits (the f32 significand) and drops only terms below 2^-24 of
+// the product; bf16x3 carries 16 bits.
+//
+// Two kernels:
+//  * split_pack: gathers A' (or B') through its scatter vectors (the packing of
+//    crates/tprims-kernel/src/pack/pack.rs:152-203, here into HBM once per
+//    call), transposes through shared memory so that reads run along the
+//    operand's unit-stride index and writes along k, splits, and writes the
+//    planes K-major, zero-padded to whole tiles.
+//  * tc_bf16_gemm: one CTA per 128 x BN output tile. Warp 0 issues TMA tile
+//    loads (SWIZZLE_64B, 32 k per stage) into a multi-stage ring; warp 1 owns
+//    the TMEM accumulator and issues tcgen05.mma kind::f16 (BF16 in, FP32
+//    accumulate) from one thread; warps 2-5 read the accumulator back with
+//    tcgen05.ld and apply the scatter epilogue D = op_D(alpha*acc + beta*C)
+//    (pack/writeback.rs:311-486). Every mbarrier wait is bounded by
+//    %globaltimer; a timeout sets a status bit and the kernel drains and
+//    returns. No cluster, no multicast.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "device_common.cuh"
+
+namespace tprims {
+namespace dev {
+
+namespace {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 32;  // BF16 elements per stage row: 64 bytes = one SWIZZLE_64B atom
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;
+
+__device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ inline void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ inline void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ inline void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of parity `parity` to complete, giving up after the limit.
+__device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) return false;
+  }
+  return true;
+}
+__device__ inline void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ inline void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
+               : "memory");
+}
+__device__ inline void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ inline void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+      : "memory");
+}
+__device__ inline void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ inline void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ inline void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor of a K-major SWIZZLE_64B tile: rows of 64 B,
+// 8-row core groups 512 B apart (stride byte offset), version 1, layout type 4.
+__device__ inline uint64_t sdesc_sw64(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ inline void split3(float x, __nv_bfloat16& p0, __nv_bfloat16& p1, __nv_bfloat16& p2) {
+  p0 = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(p0);
+  p1 = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(p1);
+  p2 = __float2bfloat16_rn(r2);
+}
+
+// Gather + split + K-major write of one 32-row x 64-k tile.
+__global__ void __launch_bounds__(256) split_pack_kernel(const float* __restrict__ X, const int64_t* __restrict__ rows_scat,
+                                                         const int64_t* __restrict__ k_scat,
+                                                         const int64_t* __restrict__ h_scat, int64_t nrows, int64_t K,
+                                                         int64_t rows_pad, int64_t k_pad, int64_t H, int kfast,
+                                                         int planes, __nv_bfloat16* __restrict__ out) {
+  __shared__ float tile[32][65];
+  const int tid = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 64, h = blockIdx.z;
+  const float* base = X + h_scat[h];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    int rr, kk;
+    if (kfast) {
+      rr = tid / 64 + 4 * j;
+      kk = tid % 64;
+    } else {
+      rr = tid % 32;
+      kk = tid / 32 + 8 * j;
+    }
+    const int64_t r = r0 + rr, k = k0 + kk;
+    float v = 0.f;
+    if (r < nrows && k < K) v = base[rows_scat[r] + k_scat[k]];
+    tile[rr][kk] = v;
+  }
+  __syncthreads();
+  const int64_t plane_stride = H * rows_pad * k_pad;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int p = tid + 256 * j;
+    const int rr = p / 32, kp = p % 32;
+    __nv_bfloat16 a0, a1, a2, b0, b1, b2;
+    split3(tile[rr][2 * kp], a0, a1, a2);
+    split3(tile[rr][2 * kp + 1], b0, b1, b2);
+    const int64_t off = (h * rows_pad + r0 + rr) * k_pad + k0 + 2 * kp;
+    __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + off);
+    o[0] = __halves2bfloat162(a0, b0);
+    reinterpret_cast<__nv_bfloat162*>(out + plane_stride + off)[0] = __halves2bfloat162(a1, b1);
+    if (planes > 2) reinterpret_cast<__nv_bfloat162*>(out + 2 * plane_stride + off)[0] = __halves2bfloat162(a2, b2);
+  }
+}
+
+template <int S>
+struct Pairs;
+template <>
+struct Pairs<2> {
+  static constexpr int N = 3;
+  __device__ static inline int a(int p) { return p == 2 ? 1 : 0; }
+  __device__ static inline int b(int p) { return p == 1 ? 1 : 0; }
+};
+template <>
+struct Pairs<3> {
+  static constexpr int N = 6;
+  // (0,0) (0,1) (1,0) (0,2) (1,1) (2,0)
+  __device__ static inline int a(int p) { return p < 2 ? 0 : (p == 2 ? 1 : (p == 3 ? 0 : (p == 4 ? 1 : 2))); }
+  __device__ static inline int b(int p) { return p == 0 ? 0 : (p == 1 ? 1 : (p == 2 ? 0 : (p == 3 ? 2 : (p == 4 ? 1 : 0)))); }
+};
+
+template <int S, int BN>
+struct TcCfg {
+  static constexpr int A_TILE = TC_BM * TC_BK * 2;  // bytes of one A plane tile
+  static constexpr int B_TILE = BN * TC_BK * 2;
+  static constexpr int STAGE = S * (A_TILE + B_TILE);
+  static constexpr int STAGES = (S == 3) ? 3 : 4;
+  static constexpr int RING = STAGES * STAGE;
+  static constexpr int SCAT = 2 * BN * 8;  // d_n, c_n of the tile
+  static constexpr int BAR = (2 * STAGES + 1) * 8 + 16;
+  static constexpr int SMEM = 1024 + RING + SCAT + BAR;
+};
+
+template <int S, int BN>
+__global__ void __launch_bounds__(192, 1)
+tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
+                    int64_t m_pad, int64_t n_pad, int64_t k_pad) {
+  using Cfg = TcCfg<S, BN>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* ring = smem;
+  int64_t* dn_s = reinterpret_cast<int64_t*>(smem + Cfg::RING);
+  int64_t* cn_s = dn_s + BN;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING + Cfg::SCAT);
+  uint64_t* empty = full + Cfg::STAGES;
+  uint64_t* accf = empty + Cfg::STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t h = blockIdx.z;
+  const int64_t m0 = (int64_t)blockIdx.y * TC_BM, n0 = (int64_t)blockIdx.x * BN;
+  const int nk = (int)(k_pad / TC_BK);
+
+  if (warp == 0 && lane == 0) {
+    for (int i = 0; i < Cfg::STAGES; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(accf, 1);
+    fence_barrier_init();
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, BN);
+    tmem_relinquish();
+  }
+  if (warp >= 2) {
+    for (int i = tid - 64; i < BN; i += 128) {
+      const int64_t n = n0 + i;
+      const bool ok = n < g.N;
+      dn_s[i] = ok ? g.s.d_n[n] : 0;
+      cn_s[i] = ok ? g.s.c_n[n] : 0;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < nk; ++kb) {
+        const int st = kb % Cfg::STAGES;
+        const uint32_t round = (uint32_t)(kb / Cfg::STAGES);
+        if (!mbar_wait(&empty[st], (round & 1u) ^ 1u)) {
+          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+          break;
+        }
+        mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
+        uint8_t* sbase = ring + st * Cfg::STAGE;
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+          tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kb * TC_BK, (int)((p * g.H + h) * m_pad + m0));
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+          tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kb * TC_BK,
+                      (int)((p * g.H + h) * n_pad + n0));
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t IDESC = idesc_bf16(TC_BM, BN);
+      for (int kb = 0; kb < nk; ++kb) {
+        const int st = kb % Cfg::STAGES;
+        const uint32_t round = (uint32_t)(kb / Cfg::STAGES);
+        if (!mbar_wait(&full[st], round & 1u)) {
+          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+#pragma unroll
+        for (int p = 0; p < Pairs<S>::N; ++p) {
+          const uint64_t ad = sdesc_sw64(sbase + Pairs<S>::a(p) * Cfg::A_TILE);
+          const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + Pairs<S>::b(p) * Cfg::B_TILE);
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk)
+            umma_bf16(tmem, ad + 2 * kk, bd + 2 * kk, IDESC, (kb | p | kk) != 0 ? 1u : 0u);
+        }
+        umma_commit(&empty[st]);
+      }
+      umma_commit(accf);
+    }
+  } else {
+    // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, i.e. tile rows.
+    const bool ok = mbar_wait(accf, 0);
+    if (!ok) atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+    tc_fence_after();
+    const int lane_base = 32 * (warp & 3);
+    const int64_t m = m0 + lane_base + lane;
+    const bool mok = ok && m < g.M;
+    const int64_t dm = mok ? g.s.d_m[m] : 0;
+    const int64_t cm = (mok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
+    const float* Cb = static_cast<const float*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]) + cm;
+    float* Db = static_cast<float*>(g.D) + g.s.h_d[h] + dm;
+#pragma unroll 1
+    for (int c = 0; c < BN / 32; ++c) {
+      uint32_t r[32];
+      tmem_ld_32x32b_x32(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(c * 32), r);
+      tmem_ld_wait();
+      if (mok) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int nn = c * 32 + j;
+          if (n0 + nn < g.N) epilogue_store<float, false>(g.e, __uint_as_float(r[j]), 0.f, Cb + cn_s[nn], Db + dn_s[nn]);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, BN);
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+bool make_map(CUtensorMap* map, const void* base, int64_t k_pad, int64_t rows_total, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows_total};
+  cuuint64_t strides[1] = {(cuuint64_t)(k_pad * 2)};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int S, int BN>
+cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, cudaStream_t st) {
+  using Cfg = TcCfg<S, BN>;
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, ap, L.k_pad, (int64_t)S * L.H * L.m_pad, TC_BM)) return cudaErrorInvalidValue;
+  if (!make_map(&mb, bp, L.k_pad, (int64_t)S * L.H * L.n_pad, BN)) return cudaErrorInvalidValue;
+  // Per call: the attribute belongs to the current device's context.
+  cudaError_t e =
+      cudaFuncSetAttribute(tc_bf16_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)(L.n_pad / BN), (unsigned)(L.m_pad / TC_BM), (unsigned)L.H);
+  tc_bf16_gemm_kernel<S, BN><<<grid, 192, Cfg::SMEM, st>>>(ma, mb, g, L.m_pad, L.n_pad, L.k_pad);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+SplitLayout split_layout(int scheme, int64_t M, int64_t N, int64_t K, int64_t H) {
+  SplitLayout L;
+  L.planes = (scheme == 2) ? 3 : 2;
+  L.m_pad = (M + TC_BM - 1) / TC_BM * TC_BM;
+  L.n_pad = (N + 255) / 256 * 256;
+  L.k_pad = (K + 63) / 64 * 64;
+  L.H = H;
+  return L;
+}
+
+size_t split_workspace_bytes(const SplitLayout& L) {
+  return (size_t)L.planes * (size_t)L.H * (size_t)(L.m_pad + L.n_pad) * (size_t)L.k_pad * 2 + 256;
+}
+
+cudaError_t launch_split_pack_f32(const GemmArgs& g, int which, const SplitLayout& L, void* planes, cudaStream_t st) {
+  const bool a = which == 0;
+  const int64_t rows_pad = a ? L.m_pad : L.n_pad;
+  dim3 grid((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H);
+  if (L.H > 65535 || rows_pad / 32 > 65535) return cudaErrorInvalidConfiguration;
+  split_pack_kernel<<<grid, 256, 0, st>>>(static_cast<const float*>(a ? g.A : g.B), a ? g.s.a_m : g.s.b_n,
+                                          a ? g.s.a_k : g.s.b_k, a ? g.s.h_a : g.s.h_b, a ? g.M : g.N, g.K, rows_pad,
+                                          L.k_pad, L.H, a ? g.a_kfast : g.b_kfast, L.planes,
+                                          static_cast<__nv_bfloat16*>(planes));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, int scheme,
+                                cudaStream_t st) {
+  if ((int64_t)L.planes * L.H * (L.m_pad > L.n_pad ? L.m_pad : L.n_pad) >= (int64_t)1 << 31)
+    return cudaErrorInvalidValue;
+  if (L.H > 65535) return cudaErrorInvalidConfiguration;
+  if (scheme == 2) return run_tc<3, 256>(g, L, ap, bp, st);
+  return run_tc<2, 256>(g, L, ap, bp, st);
+}
+
+}  // namespace dev
+}  // namespace tprims

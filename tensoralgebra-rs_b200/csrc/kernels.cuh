@@ -1,0 +1,92 @@
+// Device-side interface shared by the host runtime and the kernels.
+//
+// Every kernel reads its operands through the oriented scatter vectors of a
+// plan: element (h, m, k) of A' lives at A + h_a[h] + a_m[m] + a_k[k], element
+// (h, k, n) of B' at B + h_b[h] + b_k[k] + b_n[n], and element (h, m, n) of the
+// output at D + h_d[h] + d_m[m] + d_n[n] (likewise C). Offsets are in elements
+// of the storage type. The reference packs panels through the same vectors
+// (crates/tprims-kernel/src/pack/pack.rs:152-203) and writes back through them
+// (pack/writeback.rs:311-486).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tprims {
+namespace dev {
+
+struct Scatters {
+  const int64_t *a_m, *a_k, *b_k, *b_n, *c_m, *c_n, *d_m, *d_n, *h_a, *h_b, *h_c, *h_d;
+};
+
+// D = op_D(alpha * acc + beta * op_C(C)); beta_zero means C is never read.
+struct Epilogue {
+  double alpha_re, alpha_im, beta_re, beta_im;
+  int beta_zero;  // C not read
+  int plain;      // alpha == 1, beta == 0, no conj on D: store acc as is
+  int conj_c, conj_d;
+};
+
+// Bits of the device status word an executor owns. A kernel that gives up on a
+// bounded wait or meets an inconsistent argument sets a bit and returns; the
+// host turns a non-zero word into an error status.
+enum : unsigned {
+  STATUS_WAIT_TIMEOUT = 1u,
+  STATUS_BAD_ARGUMENT = 2u,
+};
+
+struct GemmArgs {
+  Scatters s;
+  const void* A;
+  const void* B;
+  const void* C;
+  void* D;
+  int64_t M, N, K, H;
+  int conj_a, conj_b;
+  int a_kfast, b_kfast, d_mfast;
+  Epilogue e;
+  unsigned* status;
+};
+
+// Kernel families of the plain (drop-in) path.
+enum PlainKernel : int {
+  PLAIN_AUTO = 0,
+  PLAIN_F32_SIMT_128x128 = 1,
+  PLAIN_F32_SIMT_64x64 = 2,
+  PLAIN_F64_DMMA_64x64 = 3,
+  PLAIN_F64_DMMA_32x32 = 4,
+  PLAIN_C32_SIMT_64x64 = 5,
+  PLAIN_C64_DMMA_64x32 = 6,
+  PLAIN_C64_DMMA_32x32 = 7,
+};
+
+// dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).
+cudaError_t launch_output_pass(int dtype, const GemmArgs& g, cudaStream_t st);
+cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st);
+const char* plain_kernel_name(int kernel);
+// The family the autotuner would pick for a shape (no launch).
+int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
+
+// ---- split precision (tensor cores) ----------------------------------------
+
+// Layout of the packed split operands: planes[S][H][rows_pad][k_pad] BF16,
+// k contiguous (K-major), zero-padded to the tile multiples.
+struct SplitLayout {
+  int planes;       // S: 2 (hi/lo) or 3 (hi/mid/lo)
+  int64_t m_pad, n_pad, k_pad;
+  int64_t H;
+};
+
+// Pack A' (rows = M) and B' (rows = N) into BF16 planes. `which` 0 = A', 1 = B'.
+cudaError_t launch_split_pack_f32(const GemmArgs& g, int which, const SplitLayout& L, void* planes,
+                                  cudaStream_t st);
+// The tcgen05 GEMM over packed planes, with the scatter epilogue.
+// npairs/pairs: the list of (a_plane, b_plane) products accumulated.
+cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const void* a_planes, const void* b_planes,
+                                int scheme, cudaStream_t st);
+// Bytes of packed workspace a split scheme needs.
+size_t split_workspace_bytes(const SplitLayout& L);
+SplitLayout split_layout(int scheme, int64_t M, int64_t N, int64_t K, int64_t H);
+
+}  // namespace dev
+}  // namespace tprims

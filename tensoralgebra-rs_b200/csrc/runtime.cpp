@@ -1,0 +1,525 @@
+// Executors, device state of products, operand staging and kernel dispatch.
+#include "runtime.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+namespace tprims {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();  // clear a sticky launch error of this thread
+  const int st = (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice)
+                     ? ERR_DEVICE
+                     : ERR_INTERNAL;
+  throw Error(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+// Makes `device` current for the scope and restores the caller's device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {
+    check_cuda(cudaGetDevice(&prev), "cudaGetDevice");
+    if (prev != device) check_cuda(cudaSetDevice(device), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+Executor* Executor::create(int device, uintptr_t stream) {
+  int ndev = 0;
+  check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  if (device >= ndev) throw Error(ERR_DEVICE, "no CUDA device " + std::to_string(device));
+  std::unique_ptr<Executor> ex(new Executor());
+  ex->device = device;
+  DeviceGuard g(device);
+  if (stream == 0) {
+    check_cuda(cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ex->own_stream = true;
+  } else {
+    ex->stream = reinterpret_cast<cudaStream_t>(stream);
+  }
+  check_cuda(cudaMalloc(&ex->status, 256), "cudaMalloc(status)");
+  check_cuda(cudaMemset(ex->status, 0, 256), "cudaMemset(status)");
+  check_cuda(cudaDeviceGetAttribute(&ex->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+  return ex.release();
+}
+
+Executor::~Executor() {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  if (ws) cudaFree(ws);
+  if (status) cudaFree(status);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+void* Executor::workspace(size_t bytes) {
+  if (bytes <= ws_bytes) return ws;
+  // Growing: earlier work on the stream may still use the old arena.
+  check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  if (ws) cudaFree(ws);
+  ws = nullptr;
+  ws_bytes = 0;
+  const size_t want = std::max(bytes, ws_bytes + ws_bytes / 2);
+  check_cuda(cudaMalloc(&ws, want), "cudaMalloc(workspace)");
+  ws_bytes = want;
+  return ws;
+}
+
+Product::Product(const Problem& p) : problem(p) {
+  packed = PackedPlan::from_problem(p);
+  view = orient(packed, packed.transposes_gemm(32));
+}
+
+Product::~Product() {
+  for (auto& kv : dev) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(kv.first);
+    cudaFree(kv.second.buf);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+}
+
+const dev::Scatters& Product::scatters(int device) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = dev.find(device);
+  if (it != dev.end()) return it->second.s;
+  const std::vector<int64_t>* vs[12] = {&view.a_m, &view.a_k, &view.b_k, &view.b_n, &view.c_m, &view.c_n,
+                                        &view.d_m, &view.d_n, &view.h_a, &view.h_b, &view.h_c, &view.h_d};
+  std::vector<int64_t> host;
+  size_t offs[12];
+  for (int i = 0; i < 12; ++i) {
+    offs[i] = host.size();
+    host.insert(host.end(), vs[i]->begin(), vs[i]->end());
+    host.push_back(0);  // never empty
+    while (host.size() % 4) host.push_back(0);
+  }
+  DeviceScatters ds;
+  check_cuda(cudaMalloc(&ds.buf, host.size() * sizeof(int64_t)), "cudaMalloc(scatters)");
+  check_cuda(cudaMemcpy(ds.buf, host.data(), host.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
+             "cudaMemcpy(scatters)");
+  const int64_t* b = ds.buf;
+  ds.s = dev::Scatters{b + offs[0], b + offs[1], b + offs[2],  b + offs[3],  b + offs[4],  b + offs[5],
+                       b + offs[6], b + offs[7], b + offs[8], b + offs[9], b + offs[10], b + offs[11]};
+  return dev.emplace(device, ds).first->second.s;
+}
+
+namespace {
+
+const char* scheme_name(Scheme s) {
+  switch (s) {
+    case Scheme::Plain: return "plain";
+    case Scheme::Bf16x3: return "bf16x3";
+    case Scheme::Bf16x6: return "bf16x6";
+    case Scheme::OzakiInt8: return "ozaki-int8";
+  }
+  return "?";
+}
+
+std::string axes_json(const std::vector<Axis>& ax) {
+  std::ostringstream o;
+  o << "[";
+  for (size_t i = 0; i < ax.size(); ++i) {
+    if (i) o << ",";
+    o << "{\"extent\":" << ax[i].extent << ",\"sa\":" << ax[i].sa << ",\"sb\":" << ax[i].sb << ",\"sc\":" << ax[i].sc
+      << ",\"sd\":" << ax[i].sd << "}";
+  }
+  o << "]";
+  return o.str();
+}
+
+// Relative Frobenius error bound a scheme is designed for (stated, measured in
+// the tests): unit roundoff of the storage type times a small factor for the
+// plain path; the dropped split terms for the split paths.
+double stated_bound(DType t, Scheme s) {
+  switch (s) {
+    case Scheme::Plain: return dtype_double(t) ? 1e-13 : 1e-6;
+    case Scheme::Bf16x3: return 1e-5;
+    case Scheme::Bf16x6: return 1e-6;
+    case Scheme::OzakiInt8: return 1e-12;
+  }
+  return 0;
+}
+
+}  // namespace
+
+std::string Product::report() const {
+  std::ostringstream o;
+  const auto& st = packed.stats;
+  int kernel = kernel_pin ? kernel_pin
+                          : dev::choose_plain_kernel((int)problem.dtype, view.M, view.N, view.K, view.H, 148);
+  std::string family = scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
+                       : scheme == Scheme::Bf16x3 ? "sm100.f32.tcgen05.bf16x3.128x256x32"
+                       : scheme == Scheme::Bf16x6 ? "sm100.f32.tcgen05.bf16x6.128x256x32"
+                                                  : "sm100.ozaki.int8";
+  o << "{\"algorithm\":\"packed\",\"dtype\":\"" << dtype_name(problem.dtype) << "\",\"m\":" << st.m
+    << ",\"n\":" << st.n << ",\"k\":" << st.k << ",\"batch\":" << st.batch
+    << ",\"is_pure_gemm\":" << (st.is_pure_gemm ? "true" : "false") << ",\"m_axes\":" << axes_json(st.m_axes)
+    << ",\"n_axes\":" << axes_json(st.n_axes) << ",\"k_axes\":" << axes_json(st.k_axes)
+    << ",\"h_axes\":" << axes_json(st.h_axes) << ",\"swapped\":" << (view.swapped ? "true" : "false")
+    << ",\"a_kfast\":" << (view.a_kfast ? "true" : "false") << ",\"b_kfast\":" << (view.b_kfast ? "true" : "false")
+    << ",\"d_mfast\":" << (view.d_mfast ? "true" : "false") << ",\"scheme\":\"" << scheme_name(scheme)
+    << "\",\"family\":\"" << family << "\",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)
+    << ",\"regular_rows\":" << regular_fraction(build_block_scatter(view.d_m, 32))
+    << ",\"regular_cols\":" << regular_fraction(build_block_scatter(view.d_n, 32))
+    << ",\"macs\":" << problem.macs() << "}";
+  return o.str();
+}
+
+Scalar read_scalar(DType t, const void* p) {
+  Scalar s;
+  switch (t) {
+    case DType::F32: { float v; std::memcpy(&v, p, 4); s.re = v; break; }
+    case DType::F64: { double v; std::memcpy(&v, p, 8); s.re = v; break; }
+    case DType::C32: { float v[2]; std::memcpy(v, p, 8); s.re = v[0]; s.im = v[1]; break; }
+    case DType::C64: { double v[2]; std::memcpy(v, p, 16); s.re = v[0]; s.im = v[1]; break; }
+  }
+  return s;
+}
+
+namespace {
+
+// Byte range [lo, hi) an operand can address from `origin` (null: none).
+bool byte_range(const Problem& p, int slot, const void* origin, __int128* lo, __int128* hi) {
+  if (!origin) return false;
+  const Span& sp = p.spans[slot];
+  if (sp.empty) return false;
+  const Operand& op = slot == SA ? p.a : slot == SB ? p.b : slot == SC ? p.c : p.d;
+  const __int128 off = op.layout.offset, sz = (__int128)dtype_size(p.dtype);
+  const __int128 base = (__int128)(uintptr_t)origin;
+  *lo = base + (sp.lo - off) * sz;
+  *hi = base + (sp.hi - off + 1) * sz;
+  return true;
+}
+
+bool overlaps(const Problem& p, int s1, const void* o1, int s2, const void* o2) {
+  __int128 a0, a1, b0, b1;
+  if (!byte_range(p, s1, o1, &a0, &a1) || !byte_range(p, s2, o2, &b0, &b1)) return false;
+  return a0 < b1 && b0 < a1;
+}
+
+}  // namespace
+
+void validate_item(const Product& pr, const Item& it, bool beta_zero) {
+  if (!it.a || !it.b || !it.d) throw Error(ERR_INVALID_ARGUMENT, "A, B or D data pointer is null or zero");
+  if (!it.c && !beta_zero)
+    throw Error(ERR_UNSUPPORTED,
+                "a null C (TAPP_IN_PLACE) with a nonzero beta is ambiguous in TAPP and not supported; pass D as C to "
+                "accumulate in place");
+  const Problem& p = pr.problem;
+  if (p.out_empty) return;
+  if (overlaps(p, SD, it.d, SA, it.a)) throw Error(ERR_ALIASED, "D overlaps A");
+  if (overlaps(p, SD, it.d, SB, it.b)) throw Error(ERR_ALIASED, "D overlaps B");
+  if (p.cmode == CMode::Separate && it.c) {
+    const bool same = it.c == it.d && p.c_matches_d;
+    if (!same && overlaps(p, SD, it.d, SC, it.c)) throw Error(ERR_ALIASED, "C and D overlap without being the same mapping");
+  }
+}
+
+namespace {
+
+enum class Where { Device, Host };
+
+Where classify(const void* ptr, int device) {
+  cudaPointerAttributes at;
+  cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return Where::Host;
+  }
+  if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+    if (at.type == cudaMemoryTypeDevice && at.device != device)
+      throw Error(ERR_DEVICE, "operand lives on CUDA device " + std::to_string(at.device) + ", the executor on " +
+                                  std::to_string(device));
+    return Where::Device;
+  }
+  return Where::Host;
+}
+
+struct Staged {
+  const void* host = nullptr;  // origin as passed
+  char* dev_origin = nullptr;  // origin on the device
+  char* buf = nullptr;         // start of the copied span
+  size_t bytes = 0;
+  int64_t lo_bytes = 0;  // byte offset of the span start from the origin
+  bool staged = false;
+};
+
+// Element offsets an operand addresses relative to its origin, in bytes.
+void span_bytes(const Problem& p, int slot, int64_t* lo, size_t* bytes) {
+  const Span& sp = p.spans[slot];
+  const Operand& op = slot == SA ? p.a : slot == SB ? p.b : slot == SC ? p.c : p.d;
+  const int64_t sz = (int64_t)dtype_size(p.dtype);
+  *lo = (int64_t)(sp.lo - op.layout.offset) * sz;
+  *bytes = (size_t)((sp.hi - sp.lo + 1) * sz);
+}
+
+bool dense(const Problem& p, int slot) {
+  const Span& sp = p.spans[slot];
+  const Operand& op = slot == SD ? p.d : p.c;
+  __int128 n = 1;
+  for (auto e : op.layout.dims) n *= e;
+  return n == sp.hi - sp.lo + 1;
+}
+
+dev::Epilogue make_epilogue(const Product& pr, Scalar alpha, Scalar beta, bool c_read) {
+  dev::Epilogue e{};
+  e.alpha_re = alpha.re;
+  e.alpha_im = alpha.im;
+  e.beta_re = beta.re;
+  e.beta_im = beta.im;
+  e.beta_zero = c_read ? 0 : 1;
+  const bool cplx = dtype_complex(pr.problem.dtype);
+  e.conj_c = (cplx && pr.view.conj_c && c_read) ? 1 : 0;
+  e.conj_d = (cplx && pr.view.conj_d) ? 1 : 0;
+  e.plain = (!c_read && alpha.is_one() && !e.conj_d) ? 1 : 0;
+  return e;
+}
+
+// Records the launch of one kernel family on the executor's stream when the
+// executor profiles; a no-op otherwise.
+struct Timed {
+  Executor& ex;
+  KernelTimes::Pending p{};
+  Timed(Executor& e, const std::string& name) : ex(e) {
+    if (!ex.profile) return;
+    p.name = name;
+    p.beg = ex.times.take();
+    p.end = ex.times.take();
+    cudaEventRecord(p.beg, ex.stream);
+  }
+  ~Timed() {
+    if (!ex.profile) return;
+    cudaEventRecord(p.end, ex.stream);
+    ex.times.pending.push_back(p);
+  }
+};
+
+void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool output_only, char* scratch,
+                        size_t scratch_bytes) {
+  const int dt = (int)pr.problem.dtype;
+  if (output_only) {
+    Timed t(ex, "output_pass");
+    check_cuda(dev::launch_output_pass(dt, g, ex.stream), "output pass launch");
+    return;
+  }
+  switch (pr.scheme) {
+    case Scheme::Plain: {
+      int k = pr.kernel_pin ? pr.kernel_pin : dev::choose_plain_kernel(dt, g.M, g.N, g.K, g.H, ex.num_sms);
+      Timed t(ex, dev::plain_kernel_name(k));
+      check_cuda(dev::launch_plain_gemm(dt, k, g, ex.stream), "plain contraction launch");
+      return;
+    }
+    case Scheme::Bf16x3:
+    case Scheme::Bf16x6: {
+      const dev::SplitLayout L = dev::split_layout((int)pr.scheme, g.M, g.N, g.K, g.H);
+      if (dev::split_workspace_bytes(L) > scratch_bytes) throw Error(ERR_INTERNAL, "split workspace too small");
+      char* ap = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
+      char* bp = ap + (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
+      {
+        Timed t(ex, "split_pack");
+        check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
+        check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, ex.stream), "split pack B");
+      }
+      Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
+      check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream), "tcgen05 contraction launch");
+      return;
+    }
+    case Scheme::OzakiInt8:
+      throw Error(ERR_UNSUPPORTED, "the Ozaki INT8 scheme is not available in this build");
+  }
+}
+
+size_t scheme_scratch(const Product& pr) {
+  if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6) {
+    const auto& v = pr.view;
+    return dev::split_workspace_bytes(dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H));
+  }
+  return 0;
+}
+
+}  // namespace
+
+cudaEvent_t KernelTimes::take() {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+void KernelTimes::resolve() {
+  for (auto& p : pending) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p.beg, p.end) == cudaSuccess) {
+      totals[p.name].ms += ms;
+      totals[p.name].launches += 1;
+    }
+    pool.push_back(p.beg);
+    pool.push_back(p.end);
+  }
+  pending.clear();
+}
+
+KernelTimes::~KernelTimes() {
+  for (auto e : pool) cudaEventDestroy(e);
+  for (auto& p : pending) {
+    cudaEventDestroy(p.beg);
+    cudaEventDestroy(p.end);
+  }
+}
+
+std::string kernel_times_json(Executor& ex, bool reset) {
+  std::ostringstream o;
+  o << "{";
+  bool first = true;
+  for (auto& kv : ex.times.totals) {
+    if (!first) o << ",";
+    first = false;
+    o << "\"" << kv.first << "\":{\"ms\":" << kv.second.ms << ",\"launches\":" << kv.second.launches << "}";
+  }
+  o << "}";
+  if (reset) ex.times.totals.clear();
+  return o.str();
+}
+
+void finish(Executor& ex) {
+  check_cuda(cudaStreamSynchronize(ex.stream), "kernel execution");
+  if (!ex.times.pending.empty()) ex.times.resolve();
+  unsigned word = 0;
+  check_cuda(cudaMemcpy(&word, ex.status, sizeof(word), cudaMemcpyDeviceToHost), "status read");
+  if (word != 0) {
+    cudaMemset(ex.status, 0, sizeof(unsigned));
+    if (word & dev::STATUS_WAIT_TIMEOUT)
+      throw Error(ERR_INTERNAL, "a kernel gave up on a bounded wait (device status word " + std::to_string(word) + ")");
+    throw Error(ERR_INTERNAL, "a kernel reported device status word " + std::to_string(word));
+  }
+}
+
+namespace {
+
+// Enqueue one item; returns whether host copies were involved (the caller
+// must then drain the stream before returning to the host).
+bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
+  const Problem& p = pr.problem;
+  if (p.out_empty) return false;
+  const bool c_read = it.c != nullptr && !beta.is_zero();
+  const bool output_only = p.k_empty || alpha.is_zero();
+  if (output_only && c_read && it.c == it.d && p.c_matches_d && beta.is_one() && !pr.view.conj_c &&
+      !pr.view.conj_d)
+    return false;  // in-place identity update: nothing changes (plan/mod.rs:515-519)
+
+  // Which operands are read / written, and where they live.
+  const bool need_ab = !output_only;
+  const bool in_place = c_read && it.c == it.d;
+  Staged st[4];
+  const void* origins[4] = {it.a, it.b, it.c, it.d};
+  bool use[4] = {need_ab, need_ab, c_read && !in_place, true};
+  size_t total = 0;
+  for (int s = 0; s < 4; ++s) {
+    if (!use[s] || p.spans[s].empty) continue;
+    st[s].host = origins[s];
+    if (classify(origins[s], ex.device) == Where::Device) {
+      st[s].dev_origin = const_cast<char*>(static_cast<const char*>(origins[s]));
+      continue;
+    }
+    st[s].staged = true;
+    span_bytes(p, s, &st[s].lo_bytes, &st[s].bytes);
+    total = align_up(total, 256) + st[s].bytes;
+  }
+  const size_t scratch = output_only ? 0 : scheme_scratch(pr);
+  char* ws = static_cast<char*>(ex.workspace(align_up(total, 256) + scratch + 512));
+  size_t off = 0;
+  for (int s = 0; s < 4; ++s) {
+    if (!st[s].staged) continue;
+    off = align_up(off, 256);
+    st[s].buf = ws + off;
+    st[s].dev_origin = st[s].buf - st[s].lo_bytes;
+    off += st[s].bytes;
+    const bool copy_in = s != SD || c_read || !dense(p, SD);
+    if (copy_in)
+      check_cuda(cudaMemcpyAsync(st[s].buf, static_cast<const char*>(st[s].host) + st[s].lo_bytes, st[s].bytes,
+                                 cudaMemcpyHostToDevice, ex.stream),
+                 "host-to-device copy");
+  }
+  char* scratch_ptr = ws + align_up(off, 256);
+
+  const dev::Scatters& sc = pr.scatters(ex.device);
+  dev::GemmArgs g{};
+  g.s = sc;
+  // Orientation: the kernels see A' and B'; the swap exchanges the operands.
+  const char* a_dev = st[SA].dev_origin;
+  const char* b_dev = st[SB].dev_origin;
+  g.A = pr.view.swapped ? b_dev : a_dev;
+  g.B = pr.view.swapped ? a_dev : b_dev;
+  g.C = c_read ? (in_place ? st[SD].dev_origin : st[SC].dev_origin) : nullptr;
+  g.D = st[SD].dev_origin;
+  g.M = pr.view.M;
+  g.N = pr.view.N;
+  g.K = pr.view.K;
+  g.H = pr.view.H;
+  const bool cplx = dtype_complex(p.dtype);
+  g.conj_a = cplx && pr.view.conj_a;
+  g.conj_b = cplx && pr.view.conj_b;
+  g.a_kfast = pr.view.a_kfast;
+  g.b_kfast = pr.view.b_kfast;
+  g.d_mfast = pr.view.d_mfast;
+  g.e = make_epilogue(pr, alpha, beta, c_read);
+  g.status = ex.status;
+  launch_contraction(pr, ex, g, output_only, scratch_ptr, scratch);
+
+  if (st[SD].staged)
+    check_cuda(cudaMemcpyAsync(const_cast<void*>(static_cast<const void*>(static_cast<const char*>(st[SD].host) +
+                                                                          st[SD].lo_bytes)),
+                               st[SD].buf, st[SD].bytes, cudaMemcpyDeviceToHost, ex.stream),
+               "device-to-host copy");
+  for (auto& s : st)
+    if (s.staged) return true;
+  return false;
+}
+
+}  // namespace
+
+void execute_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
+  std::lock_guard<std::mutex> lk(ex.mu);
+  DeviceGuard g(ex.device);
+  const bool staged = enqueue_item(pr, ex, alpha, beta, it);
+  if (ex.sync || staged) finish(ex);
+}
+
+void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
+                   const Item* items) {
+  std::lock_guard<std::mutex> lk(ex.mu);
+  DeviceGuard g(ex.device);
+  bool staged = false;
+  for (int i = 0; i < n; ++i) {
+    staged |= enqueue_item(*plans[i], ex, alpha[i], beta[i], items[i]);
+    // A staged item's workspace is reused by the next item: drain between.
+    if (staged && i + 1 < n) finish(ex);
+  }
+  if (ex.sync || staged) finish(ex);
+}
+
+void execute_vjp(Product&, Executor&, Scalar, const void*, const void*, const void*, void*, void*) {
+  throw Error(ERR_UNSUPPORTED, "Plan::vjp is not available in this build");
+}
+
+}  // namespace tprims

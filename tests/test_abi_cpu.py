@@ -1,0 +1,242 @@
+"""The C ABI without a GPU: the library loads, exports every declared symbol,
+and plans (lowering, folding, scatter vectors, orientation) and refuses what
+the reference refuses, with the reference's status codes. Nothing here
+launches a kernel."""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = json.load(open(os.path.join(REPO, "tests", "golden", "known_answers.json")))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(REPO, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(REPO, "include", fn)).read()
+            names |= set(re.findall(r"(?m)^TPRIMS_B200_EXPORT[^;(]*?\b(\w+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol(tp):
+    decl = declared_symbols()
+    assert len(decl) >= 40
+    for name in sorted(decl):
+        assert hasattr(tp.lib, name), name
+    assert set(tp.ABI_SYMBOLS) == decl
+
+
+def test_identity_queries(tp):
+    assert tp.lib.tprims_abi_version() == 100
+    assert tp.lib.tprims_has_part(b"core") == 1 and tp.lib.tprims_has_part(b"tapp") == 1
+    assert tp.lib.tprims_has_part(b"blas") == 0 and tp.lib.tprims_has_part(None) == 0
+    assert tp.lib.TAPP_implementation_version().decode() == "0.1.0"
+    assert tp.lib.TAPP_check_success(0) and not tp.lib.TAPP_check_success(14)
+    assert tp.explain(14) == "invalid index labels"
+
+
+def test_explain_error_truncates_like_snprintf(tp):
+    import ctypes as C
+
+    full = tp.lib.TAPP_explain_error(2, 0, None)
+    buf = C.create_string_buffer(5)
+    assert tp.lib.TAPP_explain_error(2, 5, buf) == full
+    assert buf.value == b"inco"
+
+
+def test_attributes_refuse_every_key(tp):
+    import ctypes as C
+
+    v = C.c_void_p(1234)
+    assert tp.lib.TAPP_attr_get(1, 0, C.byref(v)) == tp.ERR_UNSUPPORTED and v.value is None
+    assert tp.lib.TAPP_attr_set(1, 0, None) == tp.ERR_UNSUPPORTED
+    assert tp.lib.TAPP_attr_clear(1, 0) == tp.ERR_UNSUPPORTED
+
+
+def _product(tp, a, b, d, c=None, prec=-1, dtype=None, ops=(0, 0, 0, 0)):
+    dtype = tp.F64 if dtype is None else dtype
+    h = tp.Handle()
+    infos = [tp.TensorInfo(dtype, x["ext"], x["str"]) for x in (a, b, c or d, d)]
+    labs = [a["lab"], b["lab"], (c or d)["lab"], d["lab"]]
+    p = tp.TensorProduct.create(h, *[(ops[i], infos[i], labs[i]) for i in range(4)], prec=prec)
+    p._keep = (h, infos)
+    return p
+
+
+@pytest.mark.parametrize("name", sorted(GOLD["plans"]))
+def test_planner_matches_the_reference_analysis_tests(tp, name):
+    case = GOLD["plans"][name]
+    p = _product(tp, case["a"], case["b"], case["d"])
+    rep = p.report()
+    if "mnkb" in case:
+        assert [rep["m"], rep["n"], rep["k"], rep["batch"]] == case["mnkb"]
+        assert rep["is_pure_gemm"] == case["pure_gemm"]
+    if "m_axes" in case:
+        assert len(rep["m_axes"]) == case["m_axes"]
+    if "vector" in case:
+        v = tp.product_scatter(p, case["vector"])
+        if "want" in case:
+            assert v == case["want"]
+        if "want_prefix" in case:
+            assert v[: len(case["want_prefix"])] == case["want_prefix"]
+        assert rep["k"] == case["k"]
+
+
+@pytest.mark.parametrize("name", sorted(GOLD["scatters"]))
+def test_scatter_vectors(tp, name):
+    case = GOLD["scatters"][name]
+    # A one-role plan whose M scatter is the vector under test: D[m...] = A[m...,k] B[k].
+    ext, st = case["extents"], case["strides"]
+    n = len(ext)
+    span = 1 + sum((e - 1) * abs(s) for e, s in zip(ext, st))
+    a = {"ext": ext + [1], "str": st + [span], "lab": list(range(n)) + [99]}
+    b = {"ext": [1], "str": [1], "lab": [99]}
+    # D is column-major, so sorting the M axes by |stride in D| keeps the
+    # example's fastest-first order and A's strides generate the vector.
+    d = {"ext": ext, "str": [int(np.prod(ext[:i])) for i in range(n)], "lab": list(range(n))}
+    p = _product(tp, a, b, d)
+    assert tp.product_scatter(p, "a_m") == case["want"]
+
+
+def test_c1_plan_shape(tp):
+    # D[a,b,c,d] = sum_{e,f} A[a,e,b,f] B[f,c,e,d], extents 24, column-major.
+    cm = lambda n: [24 ** i for i in range(n)]
+    A = {"ext": [24] * 4, "str": cm(4), "lab": [0, 4, 1, 5]}
+    B = {"ext": [24] * 4, "str": cm(4), "lab": [5, 2, 4, 3]}
+    D = {"ext": [24] * 4, "str": cm(4), "lab": [0, 1, 2, 3]}
+    rep = _product(tp, A, B, D).report()
+    assert (rep["m"], rep["n"], rep["k"], rep["batch"]) == (576, 576, 576, 1)
+    assert len(rep["m_axes"]) == 2 and len(rep["k_axes"]) == 2
+    assert rep["swapped"] is False and rep["d_mfast"] is True
+
+
+def test_c2_plan_shape(tp):
+    # A[k1,m1,k2,m2] with strides (2,128,8192,524288), B[n1,k2,n2,k1], D[m1,n1,m2,n2] column-major.
+    cm = lambda n: [64 ** i for i in range(n)]
+    A = {"ext": [64] * 4, "str": [2, 128, 8192, 524288], "lab": [10, 0, 11, 1]}
+    B = {"ext": [64] * 4, "str": cm(4), "lab": [2, 11, 3, 10]}
+    D = {"ext": [64] * 4, "str": cm(4), "lab": [0, 2, 1, 3]}
+    rep = _product(tp, A, B, D, dtype=tp.F32).report()
+    assert (rep["m"], rep["n"], rep["k"]) == (4096, 4096, 4096)
+    assert rep["a_kfast"] is True and rep["b_kfast"] is False
+
+
+REJECT = [
+    # (description, A, B, D, expected status)
+    ("extent mismatch", {"ext": [2, 3], "str": [1, 2], "lab": [0, 2]},
+     {"ext": [4, 2], "str": [1, 4], "lab": [2, 1]}, None, 2),
+    ("output-only label", None, None, {"ext": [2, 2, 3], "str": [1, 2, 4], "lab": [0, 1, 9]}, 15),
+    ("non-injective D", None, None, {"ext": [2, 2], "str": [1, 1], "lab": [0, 1]}, 6),
+    ("negative extent", {"ext": [2, -2], "str": [1, 2], "lab": [0, 2]}, None, None, 2),
+]
+
+
+@pytest.mark.parametrize("desc,A,B,D,status", REJECT, ids=[r[0] for r in REJECT])
+def test_rejections(tp, desc, A, B, D, status):
+    A = A or {"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}
+    B = B or {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]}
+    D = D or {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]}
+    with pytest.raises(tp.TprimsError) as e:
+        _product(tp, A, B, D)
+    assert e.value.status == status, e.value.message
+
+
+def test_c_and_d_must_carry_the_same_labels(tp):
+    # validate.rs:236-238: OutputLabelMismatch maps to LABELS (abi.rs:100-102).
+    with pytest.raises(tp.TprimsError) as e:
+        _product(tp, {"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}, {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]},
+                 {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]}, c={"ext": [2, 2], "str": [1, 2], "lab": [0, 2]})
+    assert e.value.status == tp.ERR_LABELS
+
+
+def test_mixed_dtypes_and_precisions(tp):
+    h = tp.Handle()
+    i64 = tp.TensorInfo(tp.F64, [2, 2], [1, 2])
+    i32 = tp.TensorInfo(tp.F32, [2, 2], [1, 2])
+    L = ([0, 2], [2, 1], [0, 1], [0, 1])
+    with pytest.raises(tp.TprimsError) as e:
+        tp.TensorProduct.create(h, (0, i64, L[0]), (0, i32, L[1]), (0, i64, L[2]), (0, i64, L[3]))
+    assert e.value.status == tp.ERR_DTYPE
+    for prec, ok in ((-1, True), (1, True), (0, False), (6, False), (42, False)):
+        if ok:
+            tp.TensorProduct.create(h, (0, i64, L[0]), (0, i64, L[1]), (0, i64, L[2]), (0, i64, L[3]), prec=prec)
+        else:
+            with pytest.raises(tp.TprimsError) as e:
+                tp.TensorProduct.create(h, (0, i64, L[0]), (0, i64, L[1]), (0, i64, L[2]), (0, i64, L[3]), prec=prec)
+            assert e.value.status == tp.ERR_UNSUPPORTED
+    with pytest.raises(tp.TprimsError) as e:
+        tp.TensorProduct.create(h, (2, i64, L[0]), (0, i64, L[1]), (0, i64, L[2]), (0, i64, L[3]))
+    assert e.value.status == tp.ERR_UNSUPPORTED
+
+
+def test_tensor_info_setters_and_f16_refusal(tp):
+    import ctypes as C
+
+    t = tp.TensorInfo(tp.F64, [5, 3], [1, 5])
+    assert t.extents() == [5, 3] and t.strides() == [1, 5]
+    assert tp.lib.TAPP_set_nmodes(t.h, 3) == 0
+    assert t.extents() == [5, 3, 1] and t.strides() == [1, 5, 0]
+    ext = (C.c_int64 * 3)(2, 2, 2)
+    assert tp.lib.TAPP_set_extents(t.h, ext) == 0 and t.extents() == [2, 2, 2]
+    out = C.c_ssize_t(0)
+    assert tp.lib.TAPP_create_tensor_info(C.byref(out), tp.F16, 0, None, None) == tp.ERR_DTYPE
+    assert tp.lib.TAPP_get_nmodes(0) == -1
+    assert tp.lib.TAPP_destroy_tensor_info(0) == tp.ERR_INVALID_ARGUMENT
+
+
+def test_null_c_with_nonzero_beta_is_rejected_before_any_device_work(tp):
+    # execute.rs:34-39: refused during validation, which precedes any CUDA call.
+    p = _product(tp, {"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}, {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]},
+                 {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]})
+    a, b, d = np.ones(4), np.ones(4), np.zeros(4)
+    assert p.execute(None, 1.0, a, b, 1.0, None, d) == tp.ERR_UNSUPPORTED
+    assert np.all(d == 0)
+    # D overlapping A is ALIASED, also before any device work.
+    assert p.execute(None, 1.0, a, b, 0.0, None, a) == tp.ERR_ALIASED
+
+
+def test_dot_general_front_end(tp):
+    # DotGeneral::new(&[2], &[1], &[0], &[0]) on [3,5,4] x [3,4,2] -> [5,2,3] (dot_general.rs:14-18)
+    a = tp.OperandSpec(tp.LayoutSpec.col_major([3, 5, 4]))
+    b = tp.OperandSpec(tp.LayoutSpec.col_major([3, 4, 2]))
+    d = tp.OperandSpec(tp.LayoutSpec.col_major([5, 2, 3]))
+    plan = tp.Plan(tp.Problem.from_dot_general(tp.F64, a, b, d, tp.DotGeneral([2], [1], [0], [0])))
+    rep = plan.report()
+    assert (rep["m"], rep["n"], rep["k"], rep["batch"]) == (5, 2, 4, 3)
+    bad = tp.OperandSpec(tp.LayoutSpec.col_major([5, 3, 2]))
+    with pytest.raises(tp.TprimsError) as e:
+        tp.Plan(tp.Problem.from_dot_general(tp.F64, a, b, bad, tp.DotGeneral([2], [1], [0], [0])))
+    assert e.value.status == tp.ERR_SHAPE
+    with pytest.raises(tp.TprimsError) as e:
+        tp.Plan(tp.Problem.from_dot_general(tp.F64, a, b, d, tp.DotGeneral([2, 1], [1], [0], [0])))
+    assert e.value.status == tp.ERR_INVALID_ARGUMENT
+
+
+def test_split_precision_applies_to_f32_only(tp):
+    p = _product(tp, {"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}, {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]},
+                 {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]})
+    with pytest.raises(tp.TprimsError) as e:
+        p.set_precision(tp.PREC_BF16X3)
+    assert e.value.status == tp.ERR_UNSUPPORTED
+    q = _product(tp, {"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}, {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]},
+                 {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]}, dtype=tp.F32)
+    q.set_precision(tp.PREC_BF16X6)
+    assert q.report()["scheme"] == "bf16x6"
+
+
+def test_executor_handles_without_a_gpu(tp):
+    import ctypes as C
+
+    h = C.c_ssize_t(0)
+    assert tp.lib.tprims_tapp_executor_create_rayon(C.byref(h), 0, None) == tp.ERR_INVALID_ARGUMENT
+    assert tp.lib.tprims_tapp_executor_create_rayon(C.byref(h), 4, None) == 0
+    ps, bd = C.c_size_t(), C.c_size_t()
+    assert tp.lib.tprims_tapp_executor_set_budget(h.value, 2) == 0
+    assert tp.lib.tprims_tapp_executor_get_threads(h.value, C.byref(ps), C.byref(bd)) == 0
+    assert (ps.value, bd.value) == (4, 2)
+    assert tp.lib.TAPP_destroy_executor(h.value) == 0
+    assert tp.lib.TAPP_destroy_executor(0) == 0

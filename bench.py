@@ -78,6 +78,20 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries
+    (profiles/*.md lines `traffic_bytes_per_launch[<kernel>]: <bytes>`)."""
+    import glob
+    import re
+
+    for path in sorted(glob.glob(os.path.join(REPO, "profiles", "*.md"))):
+        with open(path) as f:
+            m = re.search(r"traffic_bytes_per_launch\[" + re.escape(kernel) + r"\]:\s*(\d+)", f.read())
+        if m:
+            return int(m.group(1)), os.path.relpath(path, REPO)
+    return None, None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
 
@@ -137,7 +151,7 @@ def cpu_rate(threads, target_s):
         t0 = time.perf_counter()
         oracle.packed_contract(1.0, A, B, 0.0, None, D, nthreads=threads)
         dt = time.perf_counter() - t0
-        flop = 2.0 * M * (E * E * s) * K
+        flop = 2.0 * M * (E * s) * K
         best = (flop / dt, s, dt)
         if dt * 2 > target_s or s >= E:
             break
@@ -151,7 +165,7 @@ def run_reference(args, rank):
     threads = os.cpu_count() or 1
     per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
     rate, s, dt = cpu_rate(threads, per_step)
-    sample = f"packed CPU driver restatement on n2 in [0,{s}) of 64 (M={M}, N={E * E * s}, K={K}), {dt:.2f} s per step"
+    sample = f"packed CPU driver restatement on n2 in [0,{s}) of 64 (M={M}, N={E * s}, K={K}), {dt:.2f} s per step"
     # The warm-up and the timed steps re-run the same sample; the rate is the best of them.
     rates = []
     for i in range(args.warmup + args.steps):
@@ -177,6 +191,7 @@ def main():
     ap.add_argument("--scheme", default="bf16x6", choices=list(SCHEMES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -267,13 +282,14 @@ def main():
         achieved = PRODUCTS[head] * FLOP / (dom_avg_ms * 1e-3) / 1e12
         peak = peaks.get("bf16_tflops", 1590.0)
         peak_unit, peak_note = "TFLOP/s", f"dense BF16 burst peak ({peak_src})"
+    traffic, traffic_src = profiled_traffic(dom_name) if dom_name else (None, None)
     launches = sum(v["launches"] for v in kt.values())
     kernel_launches = launches + (kt.get("split_pack", {}).get("launches", 0))  # split_pack covers 2 launches
 
     # The other schemes, shorter runs, for the comparison.
     others = {}
     for name in SCHEMES:
-        if name == head:
+        if name == head or args.only_head:
             continue
         st = max(5, args.steps // 10) if name != "plain" else max(3, args.steps // 50)
         oms, okt, _ = timed(name, st, 2)
@@ -310,7 +326,7 @@ def main():
         rate, s, dt = cpu_rate(threads, 12.0)
         cpu = {"value": rate / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": f"restated packed CPU driver (oracle/oracle.c), f32, n2 in [0,{s}) of 64 "
-                         f"(M=4096, N={E * E * s}, K=4096), one run of {dt:.2f} s"}
+                         f"(M=4096, N={E * s}, K=4096), one run of {dt:.2f} s"}
 
     if world > 1:
         dist.destroy_process_group()
@@ -324,7 +340,7 @@ def main():
                    "rel_err_measured": err_head, "l2": "inputs larger than L2 (A 128 MB + B 64 MB read per step)",
                    "parallelism": f"independent shards x{world}"},
         "roofline": {"bound": "tensor" if head != "plain" else "fp32-simt", "achieved": achieved, "peak": peak,
-                     "unit": peak_unit, "frac": achieved / peak, "traffic": None, "kernel": dom_name,
+                     "unit": peak_unit, "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src, "kernel": dom_name,
                      "kernel_avg_ms": dom_avg_ms, "peak_source": peak_note,
                      "flops_counted": f"{PRODUCTS[head]} x 2MNK per launch"},
         "comparison": others,

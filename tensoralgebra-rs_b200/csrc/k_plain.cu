@@ -19,7 +19,9 @@ namespace dev {
 namespace {
 
 // Gather of one ROWS x BK tile (A': rows = m; B': rows = n) into registers,
-// then into planar shared memory laid out [k][row].
+// then into planar shared memory laid out [k][row]. The k-scatter offsets of a
+// tile are fetched one tile ahead of its elements (load_idx), so an element
+// load never waits on the index load in front of it.
 template <class R, bool CPLX, int ROWS, int BK, int NT>
 struct TileGather {
   using T = typename Elem<R, CPLX>::type;
@@ -27,18 +29,33 @@ struct TileGather {
   static_assert(ROWS * BK % NT == 0, "tile must split evenly over threads");
   R re[PER];
   R im[CPLX ? PER : 1];
+  int64_t koff[PER];  // k-scatter offsets of the tile whose elements load next
 
-  __device__ inline void load(const T* base, const int64_t* rows_s, const int64_t* kscat, int64_t row0,
-                              int64_t nrows, int64_t k0, int64_t K, int kfast, int conj, int tid) {
+  __device__ static inline void coords(int idx, int kfast, int& kk, int& rr) {
+    kk = kfast ? (idx % BK) : (idx / ROWS);
+    rr = kfast ? (idx / BK) : (idx % ROWS);
+  }
+
+  __device__ inline void load_idx(const int64_t* kscat, int64_t k0, int64_t K, int kfast, int tid) {
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-      const int idx = tid + j * NT;
-      const int kk = kfast ? (idx % BK) : (idx / ROWS);
-      const int rr = kfast ? (idx / BK) : (idx % ROWS);
-      const int64_t r = row0 + rr, k = k0 + kk;
+      int kk, rr;
+      coords(tid + j * NT, kfast, kk, rr);
+      const int64_t k = k0 + kk;
+      koff[j] = k < K ? __ldg(kscat + k) : INT64_MIN;
+    }
+  }
+
+  __device__ inline void load(const T* base, const int64_t* rows_s, int64_t row0, int64_t nrows, int kfast, int conj,
+                              int tid) {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      int kk, rr;
+      coords(tid + j * NT, kfast, kk, rr);
+      const int64_t r = row0 + rr;
       R vr = R(0), vi = R(0);
-      if (r < nrows && k < K) {
-        Elem<R, CPLX>::load(base + rows_s[rr] + __ldg(kscat + k), vr, vi);
+      if (r < nrows && koff[j] != INT64_MIN) {
+        Elem<R, CPLX>::load(base + rows_s[rr] + koff[j], vr, vi);
         if (conj) vi = -vi;
       }
       re[j] = vr;
@@ -46,12 +63,18 @@ struct TileGather {
     }
   }
 
+  // Index-and-load in one step (used where latency hiding is not the issue).
+  __device__ inline void load(const T* base, const int64_t* rows_s, const int64_t* kscat, int64_t row0,
+                              int64_t nrows, int64_t k0, int64_t K, int kfast, int conj, int tid) {
+    load_idx(kscat, k0, K, kfast, tid);
+    load(base, rows_s, row0, nrows, kfast, conj, tid);
+  }
+
   __device__ inline void store(R* s_re, R* s_im, int stride, int kfast, int tid) const {
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-      const int idx = tid + j * NT;
-      const int kk = kfast ? (idx % BK) : (idx / ROWS);
-      const int rr = kfast ? (idx / BK) : (idx % ROWS);
+      int kk, rr;
+      coords(tid + j * NT, kfast, kk, rr);
       s_re[kk * stride + rr] = re[j];
       if (CPLX) s_im[kk * stride + rr] = im[j];
     }
@@ -60,8 +83,11 @@ struct TileGather {
 
 // ---------------------------------------------------------------- SIMT (FFMA)
 
+// Each K tile is accumulated into a fresh register tile that is then added to
+// the running total (round-to-nearest FADD), which keeps the FP32 rounding
+// error of a deep K near u * (sqrt(BK) + sqrt(K / BK)) instead of u * sqrt(K).
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1)
 simt_gemm_kernel(GemmArgs g) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int PAD = 4;
@@ -101,13 +127,13 @@ simt_gemm_kernel(GemmArgs g) {
 
   constexpr int HM = TM / 2, HN = TN / 2;
   const int tx = tid % (BM / TM), ty = tid / (BM / TM);
-  R acc_re[TM][TN], acc_im[CPLX ? TM : 1][CPLX ? TN : 1];
+  R tot_re[TM][TN], tot_im[CPLX ? TM : 1][CPLX ? TN : 1];
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      acc_re[i][j] = R(0);
-      if (CPLX) acc_im[i][j] = R(0);
+      tot_re[i][j] = R(0);
+      if (CPLX) tot_im[i][j] = R(0);
     }
 
   const int64_t nt = (g.K + BK - 1) / BK;
@@ -115,14 +141,26 @@ simt_gemm_kernel(GemmArgs g) {
   gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
+  if (nt > 1) {
+    ga.load_idx(g.s.a_k, BK, g.K, g.a_kfast, tid);
+    gb.load_idx(g.s.b_k, BK, g.K, g.b_kfast, tid);
+  }
   __syncthreads();
 
   for (int64_t t = 0; t < nt; ++t) {
     const int buf = (int)(t & 1);
     if (t + 1 < nt) {
-      ga.load(Ab, am_s, g.s.a_k, m0, g.M, (t + 1) * BK, g.K, g.a_kfast, g.conj_a, tid);
-      gb.load(Bb, bn_s, g.s.b_k, n0, g.N, (t + 1) * BK, g.K, g.b_kfast, g.conj_b, tid);
+      ga.load(Ab, am_s, m0, g.M, g.a_kfast, g.conj_a, tid);
+      gb.load(Bb, bn_s, n0, g.N, g.b_kfast, g.conj_b, tid);
     }
+    R acc_re[TM][TN], acc_im[CPLX ? TM : 1][CPLX ? TN : 1];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        acc_re[i][j] = R(0);
+        if (CPLX) acc_im[i][j] = R(0);
+      }
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       R ar[TM], br[TN], ai[CPLX ? TM : 1], bi[CPLX ? TN : 1];
@@ -158,9 +196,20 @@ simt_gemm_kernel(GemmArgs g) {
           }
         }
     }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        tot_re[i][j] += acc_re[i][j];
+        if (CPLX) tot_im[i][j] += acc_im[i][j];
+      }
     if (t + 1 < nt) {
       ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
       gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
+      if (t + 2 < nt) {
+        ga.load_idx(g.s.a_k, (t + 2) * BK, g.K, g.a_kfast, tid);
+        gb.load_idx(g.s.b_k, (t + 2) * BK, g.K, g.b_kfast, tid);
+      }
     }
     __syncthreads();
   }
@@ -175,7 +224,7 @@ simt_gemm_kernel(GemmArgs g) {
     for (int j = 0; j < TN; ++j) {
       const int cc = (j < HN) ? (ty * HN + j) : (BN / 2 + ty * HN + (j - HN));
       if (n0 + cc >= g.N) continue;
-      epilogue_store<R, CPLX>(g.e, acc_re[i][j], CPLX ? acc_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
+      epilogue_store<R, CPLX>(g.e, tot_re[i][j], CPLX ? tot_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
                               Db + dm_s[rr] + dn_s[cc]);
     }
   }
@@ -311,11 +360,11 @@ dim3 grid_for(const GemmArgs& g) {
 
 const char* plain_kernel_name(int k) {
   switch (k) {
-    case PLAIN_F32_SIMT_128x128: return "sm100.f32.simt.128x128x8";
-    case PLAIN_F32_SIMT_64x64: return "sm100.f32.simt.64x64x8";
+    case PLAIN_F32_SIMT_128x128: return "sm100.f32.simt.128x128x16";
+    case PLAIN_F32_SIMT_64x64: return "sm100.f32.simt.64x64x16";
     case PLAIN_F64_DMMA_64x64: return "sm100.f64.dmma884.64x64x16";
     case PLAIN_F64_DMMA_32x32: return "sm100.f64.dmma884.32x32x16";
-    case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.planar.64x64x8";
+    case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.planar.64x64x16";
     case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.planar.64x32x8";
     case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
   }
@@ -340,15 +389,15 @@ cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStre
   switch (kernel) {
     case PLAIN_F32_SIMT_128x128:
       if (dtype != 0) return cudaErrorInvalidValue;
-      simt_gemm_kernel<float, false, 128, 128, 8, 8, 8><<<grid_for<128, 128>(g), 256, 0, st>>>(g);
+      simt_gemm_kernel<float, false, 128, 128, 16, 8, 8><<<grid_for<128, 128>(g), 256, 0, st>>>(g);
       break;
     case PLAIN_F32_SIMT_64x64:
       if (dtype != 0) return cudaErrorInvalidValue;
-      simt_gemm_kernel<float, false, 64, 64, 8, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
+      simt_gemm_kernel<float, false, 64, 64, 16, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
       break;
     case PLAIN_C32_SIMT_64x64:
       if (dtype != 2) return cudaErrorInvalidValue;
-      simt_gemm_kernel<float, true, 64, 64, 8, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
+      simt_gemm_kernel<float, true, 64, 64, 16, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
       break;
     case PLAIN_F64_DMMA_64x64:
       if (dtype != 1) return cudaErrorInvalidValue;

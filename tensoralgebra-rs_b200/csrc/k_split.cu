@@ -16,9 +16,10 @@
 //    planes K-major, zero-padded to whole tiles.
 //  * tc_bf16_gemm: one CTA per 128 x BN output tile. Warp 0 issues TMA tile
 //    loads (SWIZZLE_64B, 32 k per stage) into a multi-stage ring; warp 1 owns
-//    the TMEM accumulator and issues tcgen05.mma kind::f16 (BF16 in, FP32
-//    accumulate) from one thread; warps 2-5 read the accumulator back with
-//    tcgen05.ld and apply the scatter epilogue D = op_D(alpha*acc + beta*C)
+//    the TMEM accumulators and issues tcgen05.mma kind::f16 (BF16 in, FP32
+//    accumulate) from one thread; warps 2-9 drain the accumulators with
+//    tcgen05.ld into FP32 registers (two-level accumulation, see below) and
+//    apply the scatter epilogue D = op_D(alpha*acc + beta*C)
 //    (pack/writeback.rs:311-486). Every mbarrier wait is bounded by
 //    %globaltimer; a timeout sets a status bit and the kernel drains and
 //    returns. No cluster, no multicast.
@@ -105,6 +106,14 @@ __device__ inline void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
         "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ inline void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
 __device__ inline void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -195,15 +204,26 @@ struct TcCfg {
   static constexpr int STAGES = (S == 3) ? 3 : 4;
   static constexpr int RING = STAGES * STAGE;
   static constexpr int SCAT = 2 * BN * 8;  // d_n, c_n of the tile
-  static constexpr int BAR = (2 * STAGES + 1) * 8 + 16;
+  static constexpr int BAR = (2 * STAGES + 3) * 8 + 16;
   static constexpr int SMEM = 1024 + RING + SCAT + BAR;
+  static constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, each half of the columns
+  static constexpr int THREADS = 64 + 32 * EPI_WARPS;
+  static constexpr int COLS_PER_THREAD = BN / 2;
 };
 
-template <int S, int BN>
-__global__ void __launch_bounds__(192, 1)
+// Two-level accumulation. The tensor core's FP32 accumulate truncates, so its
+// error grows with the number of MMA steps folded into one accumulator. The
+// leading product x0*y0 therefore goes into a "main" TMEM accumulator that is
+// restarted every CK k-blocks; the epilogue warps drain each chunk into FP32
+// registers with round-to-nearest adds. The cross terms, 2^-8 smaller, go to
+// a second ("corr") accumulator that lives for the whole K loop. TMEM columns:
+// main [0, BN), corr [BN, 2 BN).
+template <int S, int BN, int CK>
+__global__ void __launch_bounds__(TcCfg<S, BN>::THREADS, 1)
 tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
                     int64_t m_pad, int64_t n_pad, int64_t k_pad) {
   using Cfg = TcCfg<S, BN>;
+  constexpr int CPT = Cfg::COLS_PER_THREAD;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* ring = smem;
@@ -211,30 +231,33 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   int64_t* cn_s = dn_s + BN;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING + Cfg::SCAT);
   uint64_t* empty = full + Cfg::STAGES;
-  uint64_t* accf = empty + Cfg::STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* main_full = empty + Cfg::STAGES;
+  uint64_t* main_empty = main_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(main_empty + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t h = blockIdx.z;
   const int64_t m0 = (int64_t)blockIdx.y * TC_BM, n0 = (int64_t)blockIdx.x * BN;
   const int nk = (int)(k_pad / TC_BK);
+  const int nchunks = (nk + CK - 1) / CK;
 
   if (warp == 0 && lane == 0) {
     for (int i = 0; i < Cfg::STAGES; ++i) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
-    mbar_init(accf, 1);
+    mbar_init(main_full, 1);
+    mbar_init(main_empty, Cfg::EPI_WARPS);
     fence_barrier_init();
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, BN);
+    tmem_alloc(tmem_slot, 2 * BN);
     tmem_relinquish();
   }
   if (warp >= 2) {
-    for (int i = tid - 64; i < BN; i += 128) {
+    for (int i = tid - 64; i < BN; i += 32 * Cfg::EPI_WARPS) {
       const int64_t n = n0 + i;
       const bool ok = n < g.N;
       dn_s[i] = ok ? g.s.d_n[n] : 0;
@@ -245,6 +268,7 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem_main = tmem, tmem_corr = tmem + BN;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -269,7 +293,8 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t IDESC = idesc_bf16(TC_BM, BN);
-      for (int kb = 0; kb < nk; ++kb) {
+      bool ok = true;
+      for (int kb = 0; kb < nk && ok; ++kb) {
         const int st = kb % Cfg::STAGES;
         const uint32_t round = (uint32_t)(kb / Cfg::STAGES);
         if (!mbar_wait(&full[st], round & 1u)) {
@@ -278,40 +303,80 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         }
         tc_fence_after();
         const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+        // Cross terms first: they overlap the drain of the previous chunk.
 #pragma unroll
-        for (int p = 0; p < Pairs<S>::N; ++p) {
+        for (int p = 1; p < Pairs<S>::N; ++p) {
           const uint64_t ad = sdesc_sw64(sbase + Pairs<S>::a(p) * Cfg::A_TILE);
           const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + Pairs<S>::b(p) * Cfg::B_TILE);
 #pragma unroll
           for (int kk = 0; kk < TC_BK / 16; ++kk)
-            umma_bf16(tmem, ad + 2 * kk, bd + 2 * kk, IDESC, (kb | p | kk) != 0 ? 1u : 0u);
+            umma_bf16(tmem_corr, ad + 2 * kk, bd + 2 * kk, IDESC, (kb | (p - 1) | kk) != 0 ? 1u : 0u);
+        }
+        const int chunk = kb / CK, in_chunk = kb % CK;
+        if (in_chunk == 0 && !mbar_wait(main_empty, ((uint32_t)chunk & 1u) ^ 1u)) {
+          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+          ok = false;
+        }
+        tc_fence_after();
+        {
+          const uint64_t ad = sdesc_sw64(sbase);
+          const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE);
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk)
+            umma_bf16(tmem_main, ad + 2 * kk, bd + 2 * kk, IDESC, (in_chunk | kk) != 0 ? 1u : 0u);
         }
         umma_commit(&empty[st]);
+        if (in_chunk == CK - 1 || kb == nk - 1) umma_commit(main_full);
       }
-      umma_commit(accf);
+      if (!ok) umma_commit(main_full);
     }
   } else {
-    // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, i.e. tile rows.
-    const bool ok = mbar_wait(accf, 0);
-    if (!ok) atomicOr(g.status, STATUS_WAIT_TIMEOUT);
-    tc_fence_after();
+    // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31 (tile rows) and half
+    // of the columns; it keeps the running FP32 sum of its 128 outputs.
     const int lane_base = 32 * (warp & 3);
+    const int col0 = ((warp - 2) >> 2) * CPT;
+    const uint32_t lane_addr = (uint32_t)lane_base << 16;
+    float run[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) run[j] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      if (!mbar_wait(main_full, (uint32_t)c & 1u)) {
+        atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+#pragma unroll
+      for (int q = 0; q < CPT / 16; ++q) {
+        uint32_t r[16];
+        tmem_ld_32x32b_x16(tmem_main + lane_addr + (uint32_t)(col0 + 16 * q), r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) run[16 * q + j] += __uint_as_float(r[j]);
+      }
+      tc_fence_before();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(main_empty)) : "memory");
+    }
     const int64_t m = m0 + lane_base + lane;
     const bool mok = ok && m < g.M;
     const int64_t dm = mok ? g.s.d_m[m] : 0;
     const int64_t cm = (mok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
     const float* Cb = static_cast<const float*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]) + cm;
     float* Db = static_cast<float*>(g.D) + g.s.h_d[h] + dm;
-#pragma unroll 1
-    for (int c = 0; c < BN / 32; ++c) {
-      uint32_t r[32];
-      tmem_ld_32x32b_x32(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(c * 32), r);
+    // The last main_full commit also covers every cross-term MMA.
+#pragma unroll
+    for (int q = 0; q < CPT / 16; ++q) {
+      uint32_t r[16];
+      tmem_ld_32x32b_x16(tmem_corr + lane_addr + (uint32_t)(col0 + 16 * q), r);
       tmem_ld_wait();
       if (mok) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int nn = c * 32 + j;
-          if (n0 + nn < g.N) epilogue_store<float, false>(g.e, __uint_as_float(r[j]), 0.f, Cb + cn_s[nn], Db + dn_s[nn]);
+        for (int j = 0; j < 16; ++j) {
+          const int nn = col0 + 16 * q + j;
+          if (n0 + nn < g.N)
+            epilogue_store<float, false>(g.e, run[16 * q + j] + __uint_as_float(r[j]), 0.f, Cb + cn_s[nn],
+                                         Db + dn_s[nn]);
         }
       }
     }
@@ -321,7 +386,7 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, BN);
+    tmem_dealloc(tmem, 2 * BN);
   }
 }
 
@@ -356,7 +421,7 @@ bool make_map(CUtensorMap* map, const void* base, int64_t k_pad, int64_t rows_to
   return r == CUDA_SUCCESS;
 }
 
-template <int S, int BN>
+template <int S, int BN, int CK>
 cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, cudaStream_t st) {
   using Cfg = TcCfg<S, BN>;
   CUtensorMap ma, mb;
@@ -364,10 +429,10 @@ cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, cons
   if (!make_map(&mb, bp, L.k_pad, (int64_t)S * L.H * L.n_pad, BN)) return cudaErrorInvalidValue;
   // Per call: the attribute belongs to the current device's context.
   cudaError_t e =
-      cudaFuncSetAttribute(tc_bf16_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+      cudaFuncSetAttribute(tc_bf16_gemm_kernel<S, BN, CK>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)(L.n_pad / BN), (unsigned)(L.m_pad / TC_BM), (unsigned)L.H);
-  tc_bf16_gemm_kernel<S, BN><<<grid, 192, Cfg::SMEM, st>>>(ma, mb, g, L.m_pad, L.n_pad, L.k_pad);
+  tc_bf16_gemm_kernel<S, BN, CK><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(ma, mb, g, L.m_pad, L.n_pad, L.k_pad);
   return cudaGetLastError();
 }
 
@@ -404,8 +469,8 @@ cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const v
   if ((int64_t)L.planes * L.H * (L.m_pad > L.n_pad ? L.m_pad : L.n_pad) >= (int64_t)1 << 31)
     return cudaErrorInvalidValue;
   if (L.H > 65535) return cudaErrorInvalidConfiguration;
-  if (scheme == 2) return run_tc<3, 256>(g, L, ap, bp, st);
-  return run_tc<2, 256>(g, L, ap, bp, st);
+  if (scheme == 2) return run_tc<3, 256, 4>(g, L, ap, bp, st);
+  return run_tc<2, 256, 4>(g, L, ap, bp, st);
 }
 
 }  // namespace dev

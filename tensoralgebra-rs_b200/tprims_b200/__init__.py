@@ -191,6 +191,8 @@ def scalar_bytes(dtype: int, value) -> C.Array:
     """The bytes of a scalar of the plan's element type (alpha, beta)."""
     import numpy as np
 
+    if dtype in (F32, F64):
+        value = complex(value).real  # the imaginary part of a real scalar is dropped
     v = np.array([value], dtype=_NP_NAMES[dtype])
     buf = (C.c_char * v.nbytes).from_buffer_copy(v.tobytes())
     return buf

@@ -457,3 +457,17 @@ def test_dlpack_execute_with_cuda_tensors(tp, ex, torch_cuda):
     assert st == 0, tp.last_error()
     torch.cuda.synchronize()
     assert torch.allclose(D, A @ B, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("prog", ["standard_consumer", "abi_test", "c_consumer"])
+def test_reference_c_consumers_run_against_this_library(prog):
+    """The reference's own C programs (crates/tprims-capi/tests/c/standard_consumer.c,
+    abi_test.c, examples/c-consumer/main.c), built from their sources against the
+    reference's headers and linked to libtprims_b200 (oracle/Makefile ref_consumers)."""
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", prog)
+    if not os.path.exists(exe):
+        pytest.skip("reference consumers not built (the reference tree was absent at build time)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr

@@ -182,6 +182,235 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def c4_items(n_items, dtype, seed=20261203 + 4000):
+    """The config-4 list: `n_items` environment updates E'[a',s',b'] =
+    sum E[a,s,b] Ma[a,p,a'] W[s,p,s',q] conj(Mb[b,q,b']) with a, b log-uniform
+    in [16, 256], s in {4, 8, 16}, p = q in {2, 4}; every tensor unit-norm.
+    Returns per item the extents and the host tensors (column-major)."""
+    g = np.random.default_rng(seed + (10 if dtype == "complex128" else 0))
+    items = []
+    for _ in range(n_items):
+        a = int(round(np.exp(g.uniform(np.log(16), np.log(256)))))
+        b = int(round(np.exp(g.uniform(np.log(16), np.log(256)))))
+        s_ = int(g.choice([4, 8, 16]))
+        p = int(g.choice([2, 4]))
+
+        def t(*ext):
+            x = g.standard_normal(int(np.prod(ext)))
+            if dtype == "complex128":
+                x = x + 1j * g.standard_normal(x.size)
+            x = x / np.linalg.norm(x)
+            return x.astype(dtype)
+
+        items.append({"a": a, "b": b, "s": s_, "p": p, "E": t(a, s_, b), "Ma": t(a, p, a), "W": t(s_, p, s_, p),
+                      "Mb": t(b, p, b)})
+    return items
+
+
+# Labels of the three binary steps (a=0, s=1, b=2, p=3, a'=4, s'=5, q=6, b'=7):
+C4_STEPS = [
+    # S1: T1[s,b,p,a'] = sum_a E[a,s,b] Ma[a,p,a']
+    ("E", [0, 1, 2], "Ma", [0, 3, 4], "T1", [1, 2, 3, 4], False),
+    # S2: T2[b,a',s',q] = sum_{s,p} T1[s,b,p,a'] W[s,p,s',q]
+    ("T1", [1, 2, 3, 4], "W", [1, 3, 5, 6], "T2", [2, 4, 5, 6], False),
+    # S3: E'[a',s',b'] = sum_{b,q} T2[b,a',s',q] conj(Mb[b,q,b'])
+    ("T2", [2, 4, 5, 6], "Mb", [2, 6, 7], "Ep", [4, 5, 7], True),
+]
+
+
+def c4_extents(it):
+    return {0: it["a"], 1: it["s"], 2: it["b"], 3: it["p"], 4: it["a"], 5: it["s"], 6: it["p"], 7: it["b"]}
+
+
+def c4_flops(items, complex_):
+    f = 0.0
+    for it in items:
+        a, b, s_, p = it["a"], it["b"], it["s"], it["p"]
+        f += a * s_ * b * p * a + s_ * b * p * a * s_ * p + b * a * s_ * p * b
+    return f * (8.0 if complex_ else 2.0)
+
+
+def run_config(args, tp, torch, ex):
+    """Timing lines for the other configurations (parity-test cases in the test
+    suite): C1 (f64, extents 24, beta 0.5), C3 (c64 batched, conj(A), batch
+    innermost) and C5 (f64 forward + Plan::vjp with a repeated index)."""
+    import oracle
+
+    def col_major(ext):
+        st, acc = [], 1
+        for e in ext:
+            st.append(acc)
+            acc *= e
+        return st
+
+    def product(dtype, specs, ops=(0, 0, 0, 0)):
+        h = tp.Handle()
+        infos = [tp.TensorInfo(dtype, e, s) for e, s, _ in specs]
+        p = tp.TensorProduct.create(h, *[(ops[i], infos[i], specs[i][2]) for i in range(4)])
+        p._keep = (h, infos)
+        return p
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        ex.synchronize()
+        ex.kernel_times(reset=True)
+        stream = torch.cuda.ExternalStream(ex.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        ex.synchronize()
+        return e0.elapsed_time(e1) / steps, ex.kernel_times(reset=True)
+
+    cfg = args.config
+    out = {"config": cfg, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "unit": "TFLOP/s"}
+    if cfg == "c1":
+        e = 24
+        cm = col_major([e] * 4)
+        g = lambda i: np.random.default_rng(20261203 + 1000 + 10 + i).uniform(-1, 1, e ** 4)
+        a, b, c = g(0), g(1), g(2)
+        specs = [([e] * 4, cm, [0, 4, 1, 5]), ([e] * 4, cm, [5, 2, 4, 3]), ([e] * 4, cm, [0, 1, 2, 3]),
+                 ([e] * 4, cm, [0, 1, 2, 3])]
+        A, B, Cd = (torch.from_numpy(x).cuda() for x in (a, b, c))
+        D = torch.zeros_like(Cd)
+        want = np.zeros(e ** 4)
+        views = [oracle.View(x, *sp) for x, sp in zip((a, b, c, want), specs)]
+        oracle.packed_contract(1.0, views[0], views[1], 0.5, views[2], views[3])
+        flop = 2.0 * e ** 6
+        out["workload"] = "f64 D[a,b,c,d] = sum_{e,f} A[a,e,b,f] B[f,c,e,d] + 0.5 C, extents 24"
+        for scheme, code in (("plain", 0), ("ozaki-int8", 3)):
+            p = product(tp.F64, specs)
+            try:
+                if code:
+                    p.set_precision(code)
+            except tp.TprimsError as err:
+                out[scheme] = {"unavailable": err.message}
+                continue
+            fn = lambda: tp.check(p.execute(ex, 1.0, A.data_ptr(), B.data_ptr(), 0.5, Cd.data_ptr(), D.data_ptr()))
+            ms, kt = timed(fn, args.steps, args.warmup)
+            out[scheme] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
+                           "rel_err_vs_packed_oracle": oracle.rel_frobenius(D.cpu().numpy(), want),
+                           "family": p.report()["family"]}
+    elif cfg == "c3":
+        nb, n = 64, 384
+        ext = [nb, n, n]
+        cm = col_major(ext)
+        g = lambda i: (np.random.default_rng(20261203 + 3000 + 30 + i).uniform(-1, 1, nb * n * n)
+                       + 1j * np.random.default_rng(20261203 + 3000 + 30 + i + 100).uniform(-1, 1, nb * n * n))
+        a, b = g(0), g(1)
+        specs = [(ext, cm, [9, 2, 0]), (ext, cm, [9, 2, 1]), (ext, cm, [9, 0, 1]), (ext, cm, [9, 0, 1])]
+        A, B = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+        D = torch.zeros_like(A)
+        flop = 8.0 * nb * n ** 3
+        out["workload"] = "c64 D[b,i,j] = sum_k conj(A[b,k,i]) B[b,k,j], b=64, i=j=k=384, batch innermost"
+        A3 = a.reshape(n, n, nb, order="F")  # [b,k,i] column-major -> index [b,k,i] via F order
+        A3 = a.reshape((nb, n, n), order="F")
+        B3 = b.reshape((nb, n, n), order="F")
+        rs = np.random.default_rng(1).integers(0, [nb, n, n], size=(256, 3))
+        for scheme, code in (("plain", 0), ("ozaki-int8", 3)):
+            p = product(tp.C64, specs, ops=(1, 0, 0, 0))
+            try:
+                if code:
+                    p.set_precision(code)
+            except tp.TprimsError as err:
+                out[scheme] = {"unavailable": err.message}
+                continue
+            fn = lambda: tp.check(p.execute(ex, 1.0, A.data_ptr(), B.data_ptr(), 0.0, None, D.data_ptr()))
+            ms, kt = timed(fn, args.steps, args.warmup)
+            Dh = D.cpu().numpy().reshape((nb, n, n), order="F")
+            num = den = 0.0
+            for bb, i, j in rs:
+                ref = np.dot(np.conj(A3[bb, :, i]), B3[bb, :, j])
+                num += abs(Dh[bb, i, j] - ref) ** 2
+                den += abs(ref) ** 2
+            out[scheme] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
+                           "rel_err_sampled": (num / den) ** 0.5, "family": p.report()["family"]}
+    elif cfg in ("c4", "c4c"):
+        dt = "complex128" if cfg == "c4c" else "float64"
+        tdt = tp.C64 if cfg == "c4c" else tp.F64
+        items = c4_items(args.items, dt)
+        plans = {}
+
+        def plan_for(step, ext, la, lb, ld, conj_b):
+            key = (step, tuple(ext[l] for l in la), tuple(ext[l] for l in lb))
+            if key not in plans:
+                ea, eb, ed = [ext[l] for l in la], [ext[l] for l in lb], [ext[l] for l in ld]
+                prob = tp.Problem.from_labels(tdt, tp.OperandSpec(tp.LayoutSpec.col_major(ea)),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major(eb), conj_b),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major(ed)), la, lb, ld)
+                plans[key] = tp.Plan(prob)
+            return plans[key]
+
+        dev, lists = [], [[], [], []]
+        for it in items:
+            ext = c4_extents(it)
+            t = {k: torch.from_numpy(it[k]).cuda() for k in ("E", "Ma", "W", "Mb")}
+            for name, labs in (("T1", C4_STEPS[0][5]), ("T2", C4_STEPS[1][5]), ("Ep", C4_STEPS[2][5])):
+                t[name] = torch.zeros(int(np.prod([ext[l] for l in labs])), dtype=t["E"].dtype, device="cuda")
+            dev.append(t)
+            for si, (xa, la, xb, lb, xd, ld, cj) in enumerate(C4_STEPS):
+                lists[si].append(tp.Item(plan_for(si, ext, la, lb, ld, cj), 1.0, t[xa].data_ptr(), t[xb].data_ptr(),
+                                         t[xd].data_ptr()))
+        prepared = [tp.PreparedBatch(l) for l in lists]
+        flop = c4_flops(items, cfg == "c4c")
+        out["workload"] = (f"{len(items)} environment updates ({dt}), 3 binary steps each, a,b log-uniform in "
+                           f"[16,256], s in {{4,8,16}}, p=q in {{2,4}}; {len(plans)} distinct plans")
+        out["flops_per_step"] = flop
+
+        def step():
+            for pb in prepared:
+                pb.run(ex)
+
+        for grouping in (True, False):
+            ex.set_grouping(grouping)
+            ms, kt = timed(step, args.steps if grouping else max(2, args.steps // 4), min(args.warmup, 3))
+            out["grouped" if grouping else "per_item_loop"] = {"tflops": flop / (ms * 1e-3) / 1e12,
+                                                               "ms_per_step": ms, "kernels": kt}
+        ex.set_grouping(True)
+        step()
+        ex.synchronize()
+        # Sampled check of the final E' against the four-tensor contraction in complex128.
+        worst = 0.0
+        for i in np.random.default_rng(9).choice(len(items), size=min(8, len(items)), replace=False):
+            it = items[i]
+            a_, b_, s_, p_ = it["a"], it["b"], it["s"], it["p"]
+            E = it["E"].reshape((a_, s_, b_), order="F").astype(np.complex128)
+            Ma = it["Ma"].reshape((a_, p_, a_), order="F").astype(np.complex128)
+            W = it["W"].reshape((s_, p_, s_, p_), order="F").astype(np.complex128)
+            Mb = it["Mb"].reshape((b_, p_, b_), order="F").astype(np.complex128)
+            want = np.einsum("asb,apx,spyq,bqz->xyz", E, Ma, W, np.conj(Mb), optimize=True)
+            got = dev[i]["Ep"].cpu().numpy().reshape((a_, s_, b_), order="F")
+            worst = max(worst, float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+        out["rel_err_sampled_items"] = worst
+        out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
+    elif cfg == "c5":
+        i, k, l = 512, 128, 256
+        ea, eb, ed = [i, k, k, l], [l, i, k], [i, i]
+        gen = torch.Generator(device="cuda").manual_seed(20261203 + 5000 + 10)
+        A = torch.randn(i * k * k * l, dtype=torch.float64, device="cuda", generator=gen)
+        B = torch.randn(l * i * k, dtype=torch.float64, device="cuda", generator=gen)
+        dD = torch.randn(i * i, dtype=torch.float64, device="cuda", generator=gen)
+        D = torch.zeros(i * i, dtype=torch.float64, device="cuda")
+        dA = torch.empty_like(A)
+        dB = torch.empty_like(B)
+        p = product(tp.F64, [(ea, col_major(ea), [0, 2, 2, 3]), (eb, col_major(eb), [3, 1, 2]),
+                             (ed, col_major(ed), [0, 1]), (ed, col_major(ed), [0, 1])])
+        flop = 2.0 * i * i * k * l
+
+        def step():
+            tp.check(p.execute(ex, 1.0, A.data_ptr(), B.data_ptr(), 0.0, None, D.data_ptr()))
+            tp.check(p.vjp(ex, 1.0, A.data_ptr(), B.data_ptr(), dD.data_ptr(), dA.data_ptr(), dB.data_ptr()))
+
+        ms, kt = timed(step, args.steps, args.warmup)
+        out["workload"] = "f64 D[i,j] = sum_{k,l} A[i,k,k,l] B[l,j,k], i=j=512, k=128, l=256; forward + vjp"
+        out["plain"] = {"tflops": 3 * flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
+                        "flops_counted": "forward + dA + dB, 3 x 2*i*j*k*l; the dA zero fill (17.2 GB) is extra",
+                        "family": p.report()["family"]}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,6 +421,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
+    ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5"],
+                    help="c2 is the metric's workload; c1/c3/c5 print timing lines of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -211,6 +443,13 @@ def main():
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.config != "c2":
+        ex = tp.Executor(device=local)
+        ex.set_sync(False)
+        ex.set_profiling(True)
+        run_config(args, tp, torch, ex)
+        return
 
     a_h, b_h = host_inputs()
     A = torch.from_numpy(a_h).cuda()

@@ -195,6 +195,11 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_sync(TAPP_executor exec, 
 /* Drain the executor's stream and report any kernel-side error status word. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_synchronize(TAPP_executor exec);
 
+/* Grouped submission of lists (contract_batched, TAPP_execute_batched_product):
+   with `on` != 0 (the default) the plain-precision items whose operands are in
+   device memory run as one persistent grouped launch per kernel family,
+   replayed from a cached CUDA graph; with 0 every item is its own launch. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on);
 /* Per-kernel timing (diagnostics, off by default): with `on` != 0 the executor
    records CUDA events on its stream around every kernel launch. The totals
    are resolved whenever the stream is drained. */

@@ -489,11 +489,16 @@ extern "C" TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan
         p.scheme = scheme == TPRIMS_PREC_BF16X3 ? Scheme::Bf16x3 : Scheme::Bf16x6;
         break;
       case TPRIMS_PREC_OZAKI_INT8:
-        throw Error(ERR_UNSUPPORTED, "the Ozaki INT8 scheme is not available in this build");
+        if (t != DType::F64 && t != DType::C64)
+          throw Error(ERR_UNSUPPORTED, "the Ozaki INT8 scheme applies to f64 and c64 storage");
+        if (slices != 0 && (slices < 4 || slices > 8))
+          throw Error(ERR_INVALID_ARGUMENT, "Ozaki slice count must be 0 (default) or 4..8");
+        p.scheme = Scheme::OzakiInt8;
+        p.ozaki_slices = slices == 0 ? 7 : slices;
+        return;
       default:
         throw Error(ERR_INVALID_ARGUMENT, "unknown precision scheme " + std::to_string(scheme));
     }
-    p.ozaki_slices = slices;
   });
 }
 
@@ -690,4 +695,12 @@ extern "C" size_t tprims_b200_executor_kernel_times(TAPP_executor exec, char* bu
     buf[n] = 0;
   }
   return s.size();
+}
+
+extern "C" TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on) {
+  return ffi([&] {
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    ex.grouping = on != 0;
+  });
 }

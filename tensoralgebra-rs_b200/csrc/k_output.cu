@@ -61,5 +61,52 @@ cudaError_t launch_output_pass(int dtype, const GemmArgs& g, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Zero every element a layout addresses (rank <= 16): the off-diagonal part of
+// a cotangent whose operand has a repeated label.
+struct FillLayout {
+  int rank;
+  int64_t dims[16];
+  int64_t strides[16];
+};
+
+template <class W>
+__global__ void fill_zero_kernel(W* base, FillLayout L, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t rem = i, off = 0;
+    for (int a = 0; a < L.rank; ++a) {
+      off += (rem % L.dims[a]) * L.strides[a];
+      rem /= L.dims[a];
+    }
+    base[off] = W{};
+  }
+}
+
+struct W16 {
+  double a, b;
+};
+
+cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t* dims, const int64_t* strides,
+                             cudaStream_t st) {
+  if (rank > 16) return cudaErrorInvalidValue;
+  FillLayout L{};
+  L.rank = rank;
+  int64_t total = 1;
+  for (int a = 0; a < rank; ++a) {
+    L.dims[a] = dims[a];
+    L.strides[a] = strides[a];
+    total *= dims[a];
+  }
+  if (total <= 0) return cudaSuccess;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  switch (elem) {
+    case 4: fill_zero_kernel<float><<<blocks, 256, 0, st>>>(static_cast<float*>(origin), L, total); break;
+    case 8: fill_zero_kernel<double><<<blocks, 256, 0, st>>>(static_cast<double*>(origin), L, total); break;
+    case 16: fill_zero_kernel<W16><<<blocks, 256, 0, st>>>(static_cast<W16*>(origin), L, total); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace dev
 }  // namespace tprims

@@ -1,0 +1,453 @@
+// Ozaki-style INT8 slice contraction for f64 / c64 on the sm_100a tensor cores.
+//
+// Each row of A' (and each column of B') gets a power-of-two scale 2^e with
+// max |x| < 2^e over that row; the scaled values (|x| < 1) are cut into S
+// signed 7-bit slices, x = sum_t q_t 2^-7(t+1), q_t in [-127, 127], exactly
+// (each step multiplies by 128 and removes the integer part, both exact in
+// FP64). Slice products q_t(A) . q_u(B) accumulate exactly in INT32 on the
+// tensor cores (tcgen05.mma kind::i8); the pairs with t + u = g share the
+// weight 2^-7(g+2) and therefore one accumulator. Only pairs with t + u < S
+// are formed (S(S+1)/2 products), which drops terms below 2^-7S of the row and
+// column scales. The epilogue recombines the S accumulators in FP64 (smallest
+// weight first), applies the row and column scales, then alpha, beta and
+// conjugation (the write-back of crates/tprims-kernel/src/pack/writeback.rs:
+// 311-486).
+//
+// Complex operands are embedded as one real problem of twice the rows and
+// twice the depth: A' row 2r = [Re A_r, -Im A_r], row 2r+1 = [Im A_r, Re A_r],
+// B' depth [Re B; Im B], so rows 2r and 2r+1 of the product are the real and
+// imaginary parts of row r (the four real products of the planar method);
+// adjacent TMEM lanes hold them and the epilogue pairs them with a shuffle.
+//
+// INT32 exactness needs (g+1) K 127^2 < 2^31 for every diagonal g; the host
+// splits deeper contractions into K chunks that accumulate into D (the KC-slab
+// rule of the reference, driver/tile.rs:312-350).
+#include <climits>
+
+#include "tc_common.cuh"
+
+namespace tprims {
+namespace dev {
+
+namespace {
+
+using namespace tc;
+
+constexpr int OZ_BM = 128;
+constexpr int OZ_BN = 64;
+constexpr int OZ_BK = 64;  // INT8 per stage row: 64 bytes = one SWIZZLE_64B atom
+constexpr int EXP_NONFINITE = INT_MAX;
+
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  // D format S32 (2), A and B signed INT8 (1), K-major, N >> 3, M >> 4.
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// One element of the (possibly complex-embedded) operand X' at (row, k).
+// which == 0: A' (rows = m); which == 1: B' (rows = n).
+template <bool CPLX>
+__device__ inline double embedded(const double* X, const int64_t* rows_scat, const int64_t* k_scat, int64_t hoff,
+                                  int64_t row, int64_t k, int64_t K, int which, int conj) {
+  if (!CPLX) return X[hoff + rows_scat[row] + k_scat[k]];
+  if (which == 0) {
+    const int64_t r = row >> 1;
+    const bool second = k >= K;
+    const int64_t kk = second ? k - K : k;
+    const double* e = X + 2 * (hoff + rows_scat[r] + k_scat[kk]);
+    const double re = e[0], im = conj ? -e[1] : e[1];
+    if ((row & 1) == 0) return second ? -im : re;
+    return second ? re : im;
+  }
+  const bool second = k >= K;
+  const int64_t kk = second ? k - K : k;
+  const double* e = X + 2 * (hoff + rows_scat[row] + k_scat[kk]);
+  return second ? (conj ? -e[1] : e[1]) : e[0];
+}
+
+// Per row (complex: per complex row) exponent e with max |x| < 2^e; a row with
+// a non-finite entry gets EXP_NONFINITE. One CTA per 32 rows, looping over K.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) ozaki_exp_kernel(const double* __restrict__ X, const int64_t* rows_scat,
+                                                        const int64_t* k_scat, const int64_t* h_scat, int64_t nrows,
+                                                        int64_t K, int64_t rows_pad, int kfast, int* __restrict__ out) {
+  __shared__ unsigned long long rowmax[32];
+  const int tid = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * 32, h = blockIdx.y;
+  if (tid < 32) rowmax[tid] = 0ull;
+  __syncthreads();
+  const int64_t hoff = h_scat[h];
+  unsigned long long local[8];
+  int myrow[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    local[j] = 0ull;
+    myrow[j] = kfast ? (tid / 64 + 4 * j) : (tid % 32);
+  }
+  for (int64_t k0 = 0; k0 < K; k0 += 64) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int rr = myrow[j];
+      const int kk = kfast ? (tid % 64) : (tid / 32 + 8 * j);
+      const int64_t r = r0 + rr, k = k0 + kk;
+      if (r < nrows && k < K) {
+        const double* e = X + (CPLX ? 2 : 1) * (hoff + rows_scat[r] + k_scat[k]);
+        double m = fabs(e[0]);
+        if (CPLX) m = fmax(m, fabs(e[1]));
+        if (!(m <= 1.79769313486231570e308)) m = __longlong_as_double(0x7ff0000000000000ll);  // inf or NaN
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+        if (bits > local[j]) local[j] = bits;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) atomicMax(&rowmax[myrow[j]], local[j]);
+  __syncthreads();
+  if (tid < 32 && r0 + tid < rows_pad) {
+    const unsigned long long bits = rowmax[tid];
+    int e = 0;
+    if (bits >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
+    else if (bits != 0ull) frexp(__longlong_as_double((long long)bits), &e);
+    out[h * rows_pad + r0 + tid] = e;
+  }
+}
+
+// Gather + scale + slice of one 32-row x 64-k tile of the embedded operand,
+// written K-major into planes[S][H][rows_pad][k_pad] (INT8), zero-padded.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ X, const int64_t* rows_scat,
+                                                          const int64_t* k_scat, const int64_t* h_scat,
+                                                          const int* __restrict__ exps, int64_t nrows_emb,
+                                                          int64_t K, int64_t K_emb, int64_t rows_pad,
+                                                          int64_t exp_pad, int64_t k_pad, int64_t H, int kfast,
+                                                          int which, int conj, int S, int8_t* __restrict__ out) {
+  __shared__ double tile[32][65];
+  const int tid = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 64, h = blockIdx.z;
+  const int64_t hoff = h_scat[h];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    int rr, kk;
+    if (kfast) {
+      rr = tid / 64 + 4 * j;
+      kk = tid % 64;
+    } else {
+      rr = tid % 32;
+      kk = tid / 32 + 8 * j;
+    }
+    const int64_t r = r0 + rr, k = k0 + kk;
+    double v = 0.0;
+    if (r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, hoff, r, k, K, which, conj);
+    tile[rr][kk] = v;
+  }
+  __syncthreads();
+  const int64_t plane = H * rows_pad * k_pad;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int p = tid + 256 * j;
+    const int rr = p / 16, kq = (p % 16) * 4;
+    const int64_t r = r0 + rr;
+    const int64_t er = (CPLX && which == 0) ? (r >> 1) : r;
+    const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
+    double x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : ldexp(tile[rr][kq + q], -e);
+    int8_t* o = out + (h * rows_pad + r) * k_pad + k0 + kq;
+    for (int s = 0; s < S; ++s) {
+      char4 c;
+      signed char qv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        x[q] *= 128.0;
+        const double t = trunc(x[q]);
+        x[q] -= t;
+        qv[q] = (signed char)(int)t;
+      }
+      c.x = qv[0];
+      c.y = qv[1];
+      c.z = qv[2];
+      c.w = qv[3];
+      *reinterpret_cast<char4*>(o + s * plane) = c;
+    }
+  }
+}
+
+template <int S>
+struct OzCfg {
+  static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A plane tile
+  static constexpr int B_TILE = OZ_BN * OZ_BK;
+  static constexpr int STAGE = S * (A_TILE + B_TILE);
+  static constexpr int STAGES = (S <= 6) ? 3 : 2;
+  static constexpr int RING = STAGES * STAGE;
+  static constexpr int SCAT = 2 * OZ_BN * 8 + OZ_BN * 4;  // d_n, c_n, column exponents
+  static constexpr int BAR = (2 * STAGES + 1) * 8 + 16;
+  static constexpr int SMEM = 1024 + RING + SCAT + BAR;
+  static constexpr int TMEM_COLS = (S * OZ_BN <= 256) ? 256 : 512;
+  static_assert(S * OZ_BN <= 512, "one INT32 accumulator per diagonal must fit in TMEM");
+};
+
+// One CTA per 128 x 64 tile of the embedded product over k-blocks
+// [kb0, kb1). Warp 0: TMA producer; warp 1: TMEM owner and MMA issuer;
+// warps 2-5: epilogue (TMEM lanes = tile rows).
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(192, 1)
+ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
+                  const int* __restrict__ exp_a, const int* __restrict__ exp_b, int64_t m_emb, int64_t m_pad,
+                  int64_t n_pad, int64_t exp_a_pad, int kb0, int kb1) {
+  using Cfg = OzCfg<S>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* ring = smem;
+  int64_t* dn_s = reinterpret_cast<int64_t*>(smem + Cfg::RING);
+  int64_t* cn_s = dn_s + OZ_BN;
+  int* en_s = reinterpret_cast<int*>(cn_s + OZ_BN);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING + Cfg::SCAT);
+  uint64_t* empty = full + Cfg::STAGES;
+  uint64_t* accf = empty + Cfg::STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t h = blockIdx.z;
+  const int64_t m0 = (int64_t)blockIdx.y * OZ_BM, n0 = (int64_t)blockIdx.x * OZ_BN;
+  const int nk = kb1 - kb0;
+
+  if (warp == 0 && lane == 0) {
+    for (int i = 0; i < Cfg::STAGES; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(accf, 1);
+    fence_barrier_init();
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (warp >= 2) {
+    for (int i = tid - 64; i < OZ_BN; i += 128) {
+      const int64_t n = n0 + i;
+      const bool ok = n < g.N;
+      dn_s[i] = ok ? g.s.d_n[n] : 0;
+      cn_s[i] = ok ? g.s.c_n[n] : 0;
+      en_s[i] = exp_b[h * n_pad + n0 + i];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int i = 0; i < nk; ++i) {
+        const int st = i % Cfg::STAGES;
+        const uint32_t round = (uint32_t)(i / Cfg::STAGES);
+        if (!mbar_wait(&empty[st], (round & 1u) ^ 1u)) {
+          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+          break;
+        }
+        mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
+        uint8_t* sbase = ring + st * Cfg::STAGE;
+        const int kx = (kb0 + i) * OZ_BK;
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+          tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + m0));
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+          tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kx, (int)((p * g.H + h) * n_pad + n0));
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t IDESC = idesc_i8(OZ_BM, OZ_BN);
+      for (int i = 0; i < nk; ++i) {
+        const int st = i % Cfg::STAGES;
+        const uint32_t round = (uint32_t)(i / Cfg::STAGES);
+        if (!mbar_wait(&full[st], round & 1u)) {
+          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+#pragma unroll
+        for (int gd = 0; gd < S; ++gd) {
+#pragma unroll
+          for (int t = 0; t <= gd; ++t) {
+            const int u = gd - t;
+            const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
+            const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u * Cfg::B_TILE);
+#pragma unroll
+            for (int kk = 0; kk < OZ_BK / 32; ++kk)
+              umma_i8(tmem + (uint32_t)(gd * OZ_BN), ad + 2 * kk, bd + 2 * kk, IDESC,
+                      (i | t | kk) != 0 ? 1u : 0u);
+          }
+        }
+        umma_commit(&empty[st]);
+      }
+      umma_commit(accf);
+    }
+  } else {
+    const bool ok = mbar_wait(accf, 0);
+    if (!ok) atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+    tc_fence_after();
+    const int lane_base = 32 * (warp & 3);
+    const uint32_t lane_addr = (uint32_t)lane_base << 16;
+    const int64_t me = m0 + lane_base + lane;  // row of the embedded product
+    const int64_t m = CPLX ? (me >> 1) : me;   // output row
+    const bool row_ok = ok && me < m_emb;
+    const int em = row_ok ? exp_a[h * exp_a_pad + m] : 0;
+    const int64_t dm = row_ok ? g.s.d_m[m] : 0;
+    const int64_t cm = (row_ok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
+    using T = typename Elem<double, CPLX>::type;
+    const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]) + cm;
+    T* Db = static_cast<T*>(g.D) + g.s.h_d[h] + dm;
+#pragma unroll 1
+    for (int c = 0; c < OZ_BN / 16; ++c) {
+      double v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = 0.0;
+#pragma unroll
+      for (int gd = S - 1; gd >= 0; --gd) {
+        uint32_t r[16];
+        tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + c * 16), r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += ldexp((double)(int)r[j], -7 * (gd + 2));
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int nn = c * 16 + j;
+        const int en = en_s[nn];
+        double x = (em == EXP_NONFINITE || en == EXP_NONFINITE) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                 : ldexp(v[j], em + en);
+        if constexpr (CPLX) {
+          const double other = __shfl_xor_sync(0xffffffffu, x, 1);
+          if (row_ok && (lane & 1) == 0 && n0 + nn < g.N)
+            epilogue_store<double, true>(g.e, x, other, Cb + cn_s[nn], Db + dn_s[nn]);
+        } else {
+          if (row_ok && n0 + nn < g.N) epilogue_store<double, false>(g.e, x, 0.0, Cb + cn_s[nn], Db + dn_s[nn]);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, Cfg::TMEM_COLS);
+  }
+}
+
+template <int S, bool CPLX>
+cudaError_t run_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ap, const void* bp, const int* ea,
+                     const int* eb, int kb0, int kb1, cudaStream_t st) {
+  using Cfg = OzCfg<S>;
+  CUtensorMap ma, mb;
+  if (!make_map_2d(&ma, ap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.m_pad, OZ_BK, OZ_BM))
+    return cudaErrorInvalidValue;
+  if (!make_map_2d(&mb, bp, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.n_pad, OZ_BK, OZ_BN))
+    return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(ozaki_gemm_kernel<S, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)(L.n_pad / OZ_BN), (unsigned)(L.m_pad / OZ_BM), (unsigned)L.H);
+  ozaki_gemm_kernel<S, CPLX><<<grid, 192, Cfg::SMEM, st>>>(ma, mb, g, ea, eb, L.m_emb, L.m_pad, L.n_pad, L.exp_a_pad,
+                                                           kb0, kb1);
+  return cudaGetLastError();
+}
+
+template <bool CPLX>
+cudaError_t gemm_dispatch(const GemmArgs& g, const OzakiLayout& L, const void* ap, const void* bp, const int* ea,
+                          const int* eb, int kb0, int kb1, cudaStream_t st) {
+  switch (L.slices) {
+    case 4: return run_gemm<4, CPLX>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+    case 5: return run_gemm<5, CPLX>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+    case 6: return run_gemm<6, CPLX>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+    case 7: return run_gemm<7, CPLX>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+    case 8: return run_gemm<8, CPLX>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K, int64_t H) {
+  OzakiLayout L{};
+  L.slices = slices;
+  L.cplx = cplx ? 1 : 0;
+  L.m_emb = cplx ? 2 * M : M;
+  L.k_emb = cplx ? 2 * K : K;
+  L.m_pad = (L.m_emb + OZ_BM - 1) / OZ_BM * OZ_BM;
+  L.n_pad = (N + OZ_BN - 1) / OZ_BN * OZ_BN;
+  L.k_pad = (L.k_emb + OZ_BK - 1) / OZ_BK * OZ_BK;
+  L.exp_a_pad = (M + 31) / 32 * 32 + 32;
+  L.H = H;
+  // INT32 exactness: (S) * k * 127^2 < 2^31 over one chunk of k-blocks.
+  int64_t kmax = ((int64_t)1 << 31) / ((int64_t)slices * 127 * 127);
+  L.kb_chunk = (int)(kmax / OZ_BK);
+  if (L.kb_chunk < 1) L.kb_chunk = 1;
+  return L;
+}
+
+size_t ozaki_workspace_bytes(const OzakiLayout& L) {
+  const size_t pa = (size_t)L.slices * L.H * L.m_pad * L.k_pad;
+  const size_t pb = (size_t)L.slices * L.H * L.n_pad * L.k_pad;
+  const size_t ex = ((size_t)L.H * L.exp_a_pad + (size_t)L.H * L.n_pad) * 4;
+  return pa + pb + ex + 4 * 256;
+}
+
+cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st) {
+  int8_t* ap = static_cast<int8_t*>(ws);
+  int8_t* bp = ap + (size_t)L.slices * L.H * L.m_pad * L.k_pad;
+  int* ea = reinterpret_cast<int*>(bp + (size_t)L.slices * L.H * L.n_pad * L.k_pad);
+  int* eb = ea + L.H * L.exp_a_pad;
+  if (L.H > 65535) return cudaErrorInvalidConfiguration;
+  const double* A = static_cast<const double*>(g.A);
+  const double* B = static_cast<const double*>(g.B);
+  // Row exponents of A (per complex row) and column exponents of B.
+  {
+    dim3 ga((unsigned)((g.M + 31) / 32), (unsigned)L.H);
+    dim3 gb((unsigned)((g.N + 31) / 32), (unsigned)L.H);
+    if (L.cplx) {
+      ozaki_exp_kernel<true><<<ga, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L.exp_a_pad, g.a_kfast, ea);
+      ozaki_exp_kernel<true><<<gb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L.n_pad, g.b_kfast, eb);
+    } else {
+      ozaki_exp_kernel<false><<<ga, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L.exp_a_pad, g.a_kfast, ea);
+      ozaki_exp_kernel<false><<<gb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L.n_pad, g.b_kfast, eb);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  dim3 sa((unsigned)(L.k_pad / 64), (unsigned)(L.m_pad / 32), (unsigned)L.H);
+  dim3 sb((unsigned)(L.k_pad / 64), (unsigned)(L.n_pad / 32), (unsigned)L.H);
+  if (L.cplx) {
+    ozaki_slice_kernel<true><<<sa, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, ea, L.m_emb, g.K, L.k_emb, L.m_pad,
+                                                  L.exp_a_pad, L.k_pad, L.H, g.a_kfast, 0, g.conj_a, L.slices, ap);
+    ozaki_slice_kernel<true><<<sb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, eb, g.N, g.K, L.k_emb, L.n_pad, L.n_pad,
+                                                  L.k_pad, L.H, g.b_kfast, 1, g.conj_b, L.slices, bp);
+  } else {
+    ozaki_slice_kernel<false><<<sa, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, ea, L.m_emb, g.K, L.k_emb, L.m_pad,
+                                                   L.exp_a_pad, L.k_pad, L.H, g.a_kfast, 0, 0, L.slices, ap);
+    ozaki_slice_kernel<false><<<sb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, eb, g.N, g.K, L.k_emb, L.n_pad,
+                                                   L.n_pad, L.k_pad, L.H, g.b_kfast, 1, 0, L.slices, bp);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ozaki_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ws, int kb0, int kb1,
+                              cudaStream_t st) {
+  const int8_t* ap = static_cast<const int8_t*>(ws);
+  const int8_t* bp = ap + (size_t)L.slices * L.H * L.m_pad * L.k_pad;
+  const int* ea = reinterpret_cast<const int*>(bp + (size_t)L.slices * L.H * L.n_pad * L.k_pad);
+  const int* eb = ea + L.H * L.exp_a_pad;
+  if ((int64_t)L.slices * L.H * (L.m_pad > L.n_pad ? L.m_pad : L.n_pad) >= (int64_t)1 << 31)
+    return cudaErrorInvalidValue;
+  if (L.H > 65535) return cudaErrorInvalidConfiguration;
+  if (L.cplx) return gemm_dispatch<true>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+  return gemm_dispatch<false>(g, L, ap, bp, ea, eb, kb0, kb1, st);
+}
+
+}  // namespace dev
+}  // namespace tprims

@@ -87,8 +87,7 @@ struct TileGather {
 // the running total (round-to-nearest FADD), which keeps the FP32 rounding
 // error of a deep K near u * (sqrt(BK) + sqrt(K / BK)) instead of u * sqrt(K).
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1)
-simt_gemm_kernel(GemmArgs g) {
+__device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int PAD = 4;
   constexpr int SA = BM + PAD, SB = BN + PAD;
@@ -100,8 +99,7 @@ simt_gemm_kernel(GemmArgs g) {
   __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
 
   const int tid = threadIdx.x;
-  const int64_t h = blockIdx.z;
-  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+  const int64_t m0 = mtile * BM, n0 = ntile * BN;
 
   for (int i = tid; i < BM; i += NT) {
     const int64_t m = m0 + i;
@@ -240,7 +238,7 @@ __device__ inline void dmma_884(double& d0, double& d1, double a, double b) {
 
 // 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 8x8 DMMA tiles.
 template <bool CPLX, int WM, int WN, int BK>
-__global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
+__device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
   constexpr int BM = 2 * WM, BN = 2 * WN, NT = 128;
   constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
   constexpr int NPL = CPLX ? 2 : 1;
@@ -252,8 +250,7 @@ __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
   __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t h = blockIdx.z;
-  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+  const int64_t m0 = mtile * BM, n0 = ntile * BN;
   const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
 
   for (int i = tid; i < BM; i += NT) {
@@ -291,14 +288,18 @@ __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
   gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
+  if (nt > 1) {
+    ga.load_idx(g.s.a_k, BK, g.K, g.a_kfast, tid);
+    gb.load_idx(g.s.b_k, BK, g.K, g.b_kfast, tid);
+  }
   __syncthreads();
 
   const int fr = lane >> 2, fk = lane & 3;
   for (int64_t t = 0; t < nt; ++t) {
     const int buf = (int)(t & 1);
     if (t + 1 < nt) {
-      ga.load(Ab, am_s, g.s.a_k, m0, g.M, (t + 1) * BK, g.K, g.a_kfast, g.conj_a, tid);
-      gb.load(Bb, bn_s, g.s.b_k, n0, g.N, (t + 1) * BK, g.K, g.b_kfast, g.conj_b, tid);
+      ga.load(Ab, am_s, m0, g.M, g.a_kfast, g.conj_a, tid);
+      gb.load(Bb, bn_s, n0, g.N, g.b_kfast, g.conj_b, tid);
     }
 #pragma unroll
     for (int kq = 0; kq < BK / 4; ++kq) {
@@ -329,6 +330,10 @@ __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
     if (t + 1 < nt) {
       ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
       gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
+      if (t + 2 < nt) {
+        ga.load_idx(g.s.a_k, (t + 2) * BK, g.K, g.a_kfast, tid);
+        gb.load_idx(g.s.b_k, (t + 2) * BK, g.K, g.b_kfast, tid);
+      }
     }
     __syncthreads();
   }
@@ -350,6 +355,73 @@ __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
       }
   }
 }
+
+// One CTA per (batch, M tile, N tile).
+template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(GemmArgs g) {
+  simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, blockIdx.z, blockIdx.y, blockIdx.x);
+}
+
+template <bool CPLX, int WM, int WN, int BK>
+__global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
+  dmma_tile<CPLX, WM, WN, BK>(g, blockIdx.z, blockIdx.y, blockIdx.x);
+}
+
+// Persistent grouped kernel over a heterogeneous list (contract_batched): the
+// tiles of all items form one queue, in the order of `tile_start` (items
+// sorted by decreasing cost on the host, so the longest tiles go first); each
+// CTA claims the next tile with an atomic counter, copies the item's
+// arguments to shared memory and runs the same tile body as the one-item
+// kernels. Claiming never waits, so the kernel needs no bounded spin.
+template <class Tile, int NT>
+__global__ void __launch_bounds__(NT) grouped_kernel(const GroupItem* __restrict__ items,
+                                                     const int64_t* __restrict__ tile_start, int nitems,
+                                                     unsigned long long* counter) {
+  __shared__ __align__(16) GemmArgs sg;
+  __shared__ long long claimed;
+  __shared__ int item_s;
+  const int64_t total = tile_start[nitems];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      claimed = (long long)atomicAdd(counter, 1ull);
+      int lo = 0, hi = nitems - 1;  // the item whose tile range holds `claimed`
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= claimed) lo = mid; else hi = mid - 1;
+      }
+      item_s = lo;
+    }
+    __syncthreads();
+    const long long t = claimed;
+    if (t >= total) break;
+    const int it = item_s;
+    {
+      const int4* src = reinterpret_cast<const int4*>(&items[it].g);
+      int4* dst = reinterpret_cast<int4*>(&sg);
+      for (int w = threadIdx.x; w < (int)(sizeof(GemmArgs) / 16); w += NT) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int64_t local = t - tile_start[it];
+    const int64_t tn = items[it].tiles_n, tm = items[it].tiles_m;
+    Tile::run(sg, local / (tm * tn), (local / tn) % tm, local % tn);
+    __syncthreads();
+  }
+}
+
+template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
+struct SimtTileOp {
+  static constexpr int NT = (BM / TM) * (BN / TN);
+  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
+    simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
+  }
+};
+template <bool CPLX, int WM, int WN, int BK>
+struct DmmaTileOp {
+  static constexpr int NT = 128;
+  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
+    dmma_tile<CPLX, WM, WN, BK>(g, h, mt, nt);
+  }
+};
 
 template <int BM, int BN>
 dim3 grid_for(const GemmArgs& g) {
@@ -415,6 +487,66 @@ cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStre
       if (dtype != 3) return cudaErrorInvalidValue;
       dmma_gemm_kernel<true, 16, 16, 8><<<grid_for<32, 32>(g), 128, 0, st>>>(g);
       break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+void plain_tile_shape(int kernel, int* bm, int* bn) {
+  switch (kernel) {
+    case PLAIN_F32_SIMT_128x128: *bm = 128; *bn = 128; return;
+    case PLAIN_F32_SIMT_64x64: *bm = 64; *bn = 64; return;
+    case PLAIN_C32_SIMT_64x64: *bm = 64; *bn = 64; return;
+    case PLAIN_F64_DMMA_64x64: *bm = 64; *bn = 64; return;
+    case PLAIN_F64_DMMA_32x32: *bm = 32; *bn = 32; return;
+    case PLAIN_C64_DMMA_64x32: *bm = 64; *bn = 32; return;
+    case PLAIN_C64_DMMA_32x32: *bm = 32; *bn = 32; return;
+  }
+  *bm = *bn = 0;
+}
+
+cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
+                           unsigned long long* counter, int num_sms, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  if (nitems <= 0) return cudaSuccess;
+  switch (kernel) {
+    case PLAIN_F32_SIMT_128x128: {
+      using Op = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
+      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_F32_SIMT_64x64: {
+      using Op = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
+      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_C32_SIMT_64x64: {
+      using Op = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
+      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_F64_DMMA_64x64: {
+      using Op = DmmaTileOp<false, 32, 32, 16>;
+      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_F64_DMMA_32x32: {
+      using Op = DmmaTileOp<false, 16, 16, 16>;
+      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_C64_DMMA_64x32: {
+      using Op = DmmaTileOp<true, 32, 16, 8>;
+      grouped_kernel<Op, Op::NT><<<num_sms * 3, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
+    case PLAIN_C64_DMMA_32x32: {
+      using Op = DmmaTileOp<true, 16, 16, 8>;
+      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      break;
+    }
     default:
       return cudaErrorInvalidValue;
   }

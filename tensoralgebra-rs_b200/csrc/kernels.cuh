@@ -63,6 +63,22 @@ enum PlainKernel : int {
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).
 cudaError_t launch_output_pass(int dtype, const GemmArgs& g, cudaStream_t st);
 cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st);
+static_assert(sizeof(GemmArgs) % 16 == 0, "grouped kernels copy GemmArgs in 16-byte words");
+
+// One item of a grouped launch: its arguments and its tile grid.
+struct GroupItem {
+  GemmArgs g;
+  int64_t tiles_m, tiles_n;
+};
+// CTA tile of a plain kernel family.
+void plain_tile_shape(int kernel, int* bm, int* bn);
+// Persistent grouped launch over `nitems` items whose tiles are numbered by the
+// prefix `tile_start[0..nitems]` (device arrays); `counter` is reset here.
+cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
+                           unsigned long long* counter, int num_sms, cudaStream_t st);
+// Zero every element of a strided layout (origin = element of index 0).
+cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t* dims, const int64_t* strides,
+                             cudaStream_t st);
 const char* plain_kernel_name(int kernel);
 // The family the autotuner would pick for a shape (no launch).
 int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
@@ -87,6 +103,26 @@ cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const v
 // Bytes of packed workspace a split scheme needs.
 size_t split_workspace_bytes(const SplitLayout& L);
 SplitLayout split_layout(int scheme, int64_t M, int64_t N, int64_t K, int64_t H);
+
+// ---- Ozaki INT8 slices (f64 / c64 on tensor cores) -------------------------
+
+struct OzakiLayout {
+  int slices;      // S: 7-bit slices per operand; S(S+1)/2 slice products
+  int cplx;        // complex operands embedded as a real problem (2M rows, 2K depth)
+  int64_t m_emb;   // rows of the embedded A'
+  int64_t k_emb;   // depth of the embedded product
+  int64_t m_pad, n_pad, k_pad;
+  int64_t exp_a_pad;  // row stride of the A exponent array
+  int64_t H;
+  int kb_chunk;    // k-blocks per launch that keep INT32 accumulation exact
+};
+OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K, int64_t H);
+size_t ozaki_workspace_bytes(const OzakiLayout& L);
+// Exponent scan and slicing of A' and B' into the workspace.
+cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st);
+// Slice products over k-blocks [kb0, kb1) with the recombining epilogue.
+cudaError_t launch_ozaki_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ws, int kb0, int kb1,
+                              cudaStream_t st);
 
 }  // namespace dev
 }  // namespace tprims

@@ -157,7 +157,7 @@ double Problem::macs() const {
 Problem Problem::from_labels(DType dtype, const Operand& a, const Operand& b, CMode cmode, const Operand& c,
                              const Operand& d, const std::vector<int64_t>& la, const std::vector<int64_t>& lb,
                              bool has_c_labels, const std::vector<int64_t>& lc, const std::vector<int64_t>& ld,
-                             bool output_conj_c) {
+                             bool output_conj_c, bool d_is_operand_layout) {
   if ((cmode == CMode::Separate) != has_c_labels)
     throw Error(ERR_LABELS, "a separate C needs C labels, and only a separate C may carry them");
   Problem p;
@@ -167,6 +167,10 @@ Problem Problem::from_labels(DType dtype, const Operand& a, const Operand& b, CM
   p.d = d;
   p.cmode = cmode;
   p.c = (cmode == CMode::Separate) ? c : d;
+  p.la = la;
+  p.lb = lb;
+  p.lc = (cmode == CMode::Separate) ? lc : ld;
+  p.ld = ld;
   p.op_c_conj = (cmode == CMode::Separate) ? c.conj : (cmode == CMode::Output ? output_conj_c : false);
   p.c.conj = p.op_c_conj;
 
@@ -200,8 +204,15 @@ Problem Problem::from_labels(DType dtype, const Operand& a, const Operand& b, CM
   p.spans[SD] = span_of(dtype, d.layout);
 
   {
+    // The conservative sorted-stride test runs on the collapsed output modes
+    // (validate.rs:122). An adjoint output that is an input operand's own
+    // layout restricted to a diagonal (Plan::vjp) is injective whenever that
+    // layout is, which is what is checked for it instead.
     std::vector<std::pair<int64_t, int64_t>> axes;
-    for (auto& md : rd) axes.push_back({md.extent, md.stride});
+    if (d_is_operand_layout)
+      for (size_t i = 0; i < d.layout.rank(); ++i) axes.push_back({d.layout.dims[i], d.layout.strides[i]});
+    else
+      for (auto& md : rd) axes.push_back({md.extent, md.stride});
     if (!injective_modes(axes))
       throw Error(ERR_ALIASED, "D addresses an element more than once (zero or overlapping strides)");
   }

@@ -99,13 +99,16 @@ struct Problem {
   bool c_matches_d = true;
   bool k_empty = false;
   bool out_empty = false;
+  // The labels the problem was described with (synthetic ones for dot_general);
+  // the adjoint contractions of Plan::vjp are built from them.
+  std::vector<int64_t> la, lb, lc, ld;
 
   // Problem::from_labels (api/problem.rs:370). `lc` is used only for
   // CMode::Separate; `has_c_labels` says whether C labels were given at all.
   static Problem from_labels(DType dtype, const Operand& a, const Operand& b, CMode cmode, const Operand& c,
                              const Operand& d, const std::vector<int64_t>& la, const std::vector<int64_t>& lb,
                              bool has_c_labels, const std::vector<int64_t>& lc, const std::vector<int64_t>& ld,
-                             bool output_conj_c = false);
+                             bool output_conj_c = false, bool d_is_operand_layout = false);
 
   // Problem::from_dot_general (api/problem.rs:396) with DotGeneral::validate
   // (api/dot_general.rs:82). D must have extents [lhs_free, rhs_free, batch].

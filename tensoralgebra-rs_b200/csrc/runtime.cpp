@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <sstream>
+#include <vector>
 
 namespace tprims {
 
@@ -61,6 +62,10 @@ Executor::~Executor() {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  for (auto& kv : graphs) {
+    cudaGraphExecDestroy(kv.second.exec);
+    cudaFree(kv.second.buf);
+  }
   if (ws) cudaFree(ws);
   if (status) cudaFree(status);
   if (own_stream && stream) cudaStreamDestroy(stream);
@@ -166,7 +171,9 @@ std::string Product::report() const {
   std::string family = scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
                        : scheme == Scheme::Bf16x3 ? "sm100.f32.tcgen05.bf16x3.128x256x32"
                        : scheme == Scheme::Bf16x6 ? "sm100.f32.tcgen05.bf16x6.128x256x32"
-                                                  : "sm100.ozaki.int8";
+                                                  : std::string("sm100.") + dtype_name(problem.dtype) +
+                                                        ".tcgen05.ozaki-int8.s" + std::to_string(ozaki_slices) +
+                                                        ".128x64x64";
   o << "{\"algorithm\":\"packed\",\"dtype\":\"" << dtype_name(problem.dtype) << "\",\"m\":" << st.m
     << ",\"n\":" << st.n << ",\"k\":" << st.k << ",\"batch\":" << st.batch
     << ",\"is_pure_gemm\":" << (st.is_pure_gemm ? "true" : "false") << ",\"m_axes\":" << axes_json(st.m_axes)
@@ -269,11 +276,12 @@ void span_bytes(const Problem& p, int slot, int64_t* lo, size_t* bytes) {
   *bytes = (size_t)((sp.hi - sp.lo + 1) * sz);
 }
 
-bool dense(const Problem& p, int slot) {
-  const Span& sp = p.spans[slot];
-  const Operand& op = slot == SD ? p.d : p.c;
-  __int128 n = 1;
-  for (auto e : op.layout.dims) n *= e;
+// Whether the contraction writes every element of D's span (so a staged D
+// need not be copied in): the distinct output elements (M * N * batch after
+// repeated labels collapse) fill the span exactly.
+bool fully_written(const Product& pr) {
+  const Span& sp = pr.problem.spans[SD];
+  const __int128 n = (__int128)pr.packed.stats.m * pr.packed.stats.n * pr.packed.stats.batch;
   return n == sp.hi - sp.lo + 1;
 }
 
@@ -340,16 +348,47 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
       check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream), "tcgen05 contraction launch");
       return;
     }
-    case Scheme::OzakiInt8:
-      throw Error(ERR_UNSUPPORTED, "the Ozaki INT8 scheme is not available in this build");
+    case Scheme::OzakiInt8: {
+      const dev::OzakiLayout L =
+          dev::ozaki_layout(pr.ozaki_slices, dtype_complex(pr.problem.dtype), g.M, g.N, g.K, g.H);
+      if (dev::ozaki_workspace_bytes(L) > scratch_bytes) throw Error(ERR_INTERNAL, "Ozaki workspace too small");
+      char* ws = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
+      {
+        Timed t(ex, "ozaki_pack");
+        check_cuda(dev::launch_ozaki_pack(g, L, ws, ex.stream), "Ozaki slice pack");
+      }
+      const int nkb = (int)(L.k_pad / 64);
+      for (int kb0 = 0; kb0 < nkb; kb0 += L.kb_chunk) {
+        const int kb1 = std::min(nkb, kb0 + L.kb_chunk);
+        dev::GemmArgs gc = g;
+        if (kb0 > 0) {
+          // Later K chunks accumulate into D: beta = 1, C = D, op_C = op_D
+          // (the KC-slab rule of the reference's driver/tile.rs:331-350).
+          gc.C = g.D;
+          gc.s.c_m = g.s.d_m;
+          gc.s.c_n = g.s.d_n;
+          gc.s.h_c = g.s.h_d;
+          gc.e.beta_re = 1.0;
+          gc.e.beta_im = 0.0;
+          gc.e.beta_zero = 0;
+          gc.e.plain = 0;
+          gc.e.conj_c = g.e.conj_d;
+        }
+        Timed t(ex, "ozaki_gemm");
+        check_cuda(dev::launch_ozaki_gemm(gc, L, ws, kb0, kb1, ex.stream), "Ozaki INT8 contraction launch");
+      }
+      return;
+    }
   }
 }
 
 size_t scheme_scratch(const Product& pr) {
-  if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6) {
-    const auto& v = pr.view;
+  const auto& v = pr.view;
+  if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6)
     return dev::split_workspace_bytes(dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H));
-  }
+  if (pr.scheme == Scheme::OzakiInt8)
+    return dev::ozaki_workspace_bytes(
+        dev::ozaki_layout(pr.ozaki_slices, dtype_complex(pr.problem.dtype), v.M, v.N, v.K, v.H));
   return 0;
 }
 
@@ -416,6 +455,31 @@ void finish(Executor& ex) {
 
 namespace {
 
+// Kernel arguments of one item with device-resident operands. Orientation:
+// the kernels see A' and B', and the swap exchanges the operands.
+dev::GemmArgs build_args(Product& pr, Executor& ex, Scalar alpha, Scalar beta, bool c_read, const char* a_dev,
+                         const char* b_dev, const char* c_dev, char* d_dev) {
+  dev::GemmArgs g{};
+  g.s = pr.scatters(ex.device);
+  g.A = pr.view.swapped ? b_dev : a_dev;
+  g.B = pr.view.swapped ? a_dev : b_dev;
+  g.C = c_dev;
+  g.D = d_dev;
+  g.M = pr.view.M;
+  g.N = pr.view.N;
+  g.K = pr.view.K;
+  g.H = pr.view.H;
+  const bool cplx = dtype_complex(pr.problem.dtype);
+  g.conj_a = cplx && pr.view.conj_a;
+  g.conj_b = cplx && pr.view.conj_b;
+  g.a_kfast = pr.view.a_kfast;
+  g.b_kfast = pr.view.b_kfast;
+  g.d_mfast = pr.view.d_mfast;
+  g.e = make_epilogue(pr, alpha, beta, c_read);
+  g.status = ex.status;
+  return g;
+}
+
 // Enqueue one item; returns whether host copies were involved (the caller
 // must then drain the stream before returning to the host).
 bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
@@ -454,7 +518,7 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
     st[s].buf = ws + off;
     st[s].dev_origin = st[s].buf - st[s].lo_bytes;
     off += st[s].bytes;
-    const bool copy_in = s != SD || c_read || !dense(p, SD);
+    const bool copy_in = s != SD || c_read || !fully_written(pr);
     if (copy_in)
       check_cuda(cudaMemcpyAsync(st[s].buf, static_cast<const char*>(st[s].host) + st[s].lo_bytes, st[s].bytes,
                                  cudaMemcpyHostToDevice, ex.stream),
@@ -462,28 +526,9 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
   }
   char* scratch_ptr = ws + align_up(off, 256);
 
-  const dev::Scatters& sc = pr.scatters(ex.device);
-  dev::GemmArgs g{};
-  g.s = sc;
-  // Orientation: the kernels see A' and B'; the swap exchanges the operands.
-  const char* a_dev = st[SA].dev_origin;
-  const char* b_dev = st[SB].dev_origin;
-  g.A = pr.view.swapped ? b_dev : a_dev;
-  g.B = pr.view.swapped ? a_dev : b_dev;
-  g.C = c_read ? (in_place ? st[SD].dev_origin : st[SC].dev_origin) : nullptr;
-  g.D = st[SD].dev_origin;
-  g.M = pr.view.M;
-  g.N = pr.view.N;
-  g.K = pr.view.K;
-  g.H = pr.view.H;
-  const bool cplx = dtype_complex(p.dtype);
-  g.conj_a = cplx && pr.view.conj_a;
-  g.conj_b = cplx && pr.view.conj_b;
-  g.a_kfast = pr.view.a_kfast;
-  g.b_kfast = pr.view.b_kfast;
-  g.d_mfast = pr.view.d_mfast;
-  g.e = make_epilogue(pr, alpha, beta, c_read);
-  g.status = ex.status;
+  const dev::GemmArgs g = build_args(pr, ex, alpha, beta, c_read, st[SA].dev_origin, st[SB].dev_origin,
+                                     c_read ? (in_place ? st[SD].dev_origin : st[SC].dev_origin) : nullptr,
+                                     st[SD].dev_origin);
   launch_contraction(pr, ex, g, output_only, scratch_ptr, scratch);
 
   if (st[SD].staged)
@@ -505,21 +550,270 @@ void execute_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
   if (ex.sync || staged) finish(ex);
 }
 
+namespace {
+
+// Whether an item can join a grouped launch: plain scheme, a real contraction
+// (not the output-only pass), every operand already in device memory.
+bool groupable(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
+  const Problem& p = pr.problem;
+  if (pr.scheme != Scheme::Plain || p.out_empty || p.k_empty || alpha.is_zero()) return false;
+  if (pr.view.H > 65535) return false;
+  const bool c_read = it.c != nullptr && !beta.is_zero();
+  const void* ptrs[4] = {it.a, it.b, c_read ? it.c : nullptr, it.d};
+  for (const void* q : ptrs)
+    if (q && classify(q, ex.device) != Where::Device) return false;
+  return true;
+}
+
+uint64_t mix(uint64_t h, uint64_t v) {
+  h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+  return h;
+}
+
+// One grouped submission: descriptors for every groupable item, tiles in
+// decreasing-K order, one persistent launch per kernel family; captured in a
+// CUDA graph cached by the item list (plans, pointers and scalars), so a
+// repeated list replays with one graph launch.
+uint64_t list_key(int n, Product* const* plans, const Scalar* alpha, const Scalar* beta, const Item* items) {
+  uint64_t key = 1469598103934665603ull;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t f[7] = {(uint64_t)(uintptr_t)plans[i], (uint64_t)(uintptr_t)items[i].a,
+                           (uint64_t)(uintptr_t)items[i].b, (uint64_t)(uintptr_t)items[i].c,
+                           (uint64_t)(uintptr_t)items[i].d, 0, 0};
+    for (uint64_t v : f) key = mix(key, v);
+    double sc[4] = {alpha[i].re, alpha[i].im, beta[i].re, beta[i].im};
+    uint64_t bits[4];
+    std::memcpy(bits, sc, sizeof(bits));
+    for (uint64_t v : bits) key = mix(key, v);
+  }
+  return mix(key, (uint64_t)n);
+}
+
+// Builds, captures and caches the graph of the grouped items `idx`; the
+// entry also remembers the items that run individually (`single`).
+Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<int>& idx,
+                                 const std::vector<int>& single, Product* const* plans, const Scalar* alpha,
+                                 const Scalar* beta, const Item* items) {
+  // Families: each item takes the kernel the autotuner picks for its shape.
+  std::map<int, std::vector<int>> fam;
+  for (int i : idx) {
+    Product& pr = *plans[i];
+    const int k = pr.kernel_pin ? pr.kernel_pin
+                                : dev::choose_plain_kernel((int)pr.problem.dtype, pr.view.M, pr.view.N, pr.view.K,
+                                                           pr.view.H, ex.num_sms);
+    fam[k].push_back(i);
+  }
+  Executor::Graph gr;
+  gr.single = single;
+  std::vector<std::pair<int, std::pair<size_t, size_t>>> launches;  // family, item offset, count
+  std::vector<dev::GroupItem> host_items;
+  std::vector<int64_t> host_starts;
+  for (auto& kv : fam) {
+    std::vector<int>& list = kv.second;
+    std::stable_sort(list.begin(), list.end(),
+                     [&](int a, int b) { return plans[a]->view.K > plans[b]->view.K; });
+    int bm = 0, bn = 0;
+    dev::plain_tile_shape(kv.first, &bm, &bn);
+    const size_t item0 = host_items.size(), start0 = host_starts.size();
+    int64_t acc = 0;
+    for (int i : list) {
+      Product& pr = *plans[i];
+      const bool c_read = items[i].c != nullptr && !beta[i].is_zero();
+      dev::GroupItem gi{};
+      gi.g = build_args(pr, ex, alpha[i], beta[i], c_read, static_cast<const char*>(items[i].a),
+                        static_cast<const char*>(items[i].b),
+                        c_read ? static_cast<const char*>(items[i].c) : nullptr, static_cast<char*>(items[i].d));
+      gi.tiles_m = (pr.view.M + bm - 1) / bm;
+      gi.tiles_n = (pr.view.N + bn - 1) / bn;
+      host_items.push_back(gi);
+      host_starts.push_back(acc);
+      acc += gi.tiles_m * gi.tiles_n * pr.view.H;
+    }
+    host_starts.push_back(acc);
+    launches.push_back({kv.first, {item0, start0}});
+  }
+  const size_t items_bytes = host_items.size() * sizeof(dev::GroupItem);
+  const size_t starts_bytes = host_starts.size() * sizeof(int64_t);
+  check_cuda(cudaMalloc(&gr.buf, items_bytes + starts_bytes + 256 * (launches.size() + 1)), "cudaMalloc(groups)");
+  char* base = static_cast<char*>(gr.buf);
+  check_cuda(cudaMemcpy(base, host_items.data(), items_bytes, cudaMemcpyHostToDevice), "group descriptors");
+  char* starts = base + align_up(items_bytes, 256);
+  check_cuda(cudaMemcpy(starts, host_starts.data(), starts_bytes, cudaMemcpyHostToDevice), "group tile starts");
+  char* counters = starts + align_up(starts_bytes, 256);
+  check_cuda(cudaStreamBeginCapture(ex.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  cudaError_t cap = cudaSuccess;
+  for (size_t l = 0; l < launches.size() && cap == cudaSuccess; ++l) {
+    const int family = launches[l].first;
+    const size_t item0 = launches[l].second.first, start0 = launches[l].second.second;
+    const int count = (int)((l + 1 < launches.size() ? launches[l + 1].second.first : host_items.size()) - item0);
+    cap = dev::launch_grouped(family, reinterpret_cast<dev::GroupItem*>(base) + item0,
+                              reinterpret_cast<int64_t*>(starts) + start0, count,
+                              reinterpret_cast<unsigned long long*>(counters + 256 * l), ex.num_sms, ex.stream);
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t end = cudaStreamEndCapture(ex.stream, &graph);
+  if (cap != cudaSuccess || end != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(gr.buf);
+    check_cuda(cap != cudaSuccess ? cap : end, "grouped launch capture");
+  }
+  cudaError_t inst = cudaGraphInstantiate(&gr.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) {
+    cudaFree(gr.buf);
+    check_cuda(inst, "cudaGraphInstantiate");
+  }
+  gr.last_use = ++ex.graph_clock;
+  // Bounded cache: evict the least recently used graph.
+  if (ex.graphs.size() >= 16) {
+    auto victim = ex.graphs.begin();
+    for (auto it = ex.graphs.begin(); it != ex.graphs.end(); ++it)
+      if (it->second.last_use < victim->second.last_use) victim = it;
+    check_cuda(cudaStreamSynchronize(ex.stream), "cudaStreamSynchronize");
+    cudaGraphExecDestroy(victim->second.exec);
+    cudaFree(victim->second.buf);
+    ex.graphs.erase(victim);
+  }
+  return ex.graphs.emplace(key, gr).first->second;
+}
+
+}  // namespace
+
 void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
                    const Item* items) {
   std::lock_guard<std::mutex> lk(ex.mu);
   DeviceGuard g(ex.device);
+  const uint64_t key = ex.grouping ? list_key(n, plans, alpha, beta, items) : 0;
+  auto hit = ex.grouping ? ex.graphs.find(key) : ex.graphs.end();
+  Executor::Graph* gr = nullptr;
+  std::vector<int> single;
+  if (hit != ex.graphs.end()) {
+    gr = &hit->second;
+    single = gr->single;
+  } else {
+    std::vector<int> grouped;
+    for (int i = 0; i < n; ++i)
+      (ex.grouping && groupable(*plans[i], ex, alpha[i], beta[i], items[i]) ? grouped : single).push_back(i);
+    if (grouped.size() < 2) {
+      single.insert(single.end(), grouped.begin(), grouped.end());
+      grouped.clear();
+    } else {
+      gr = &capture_grouped(ex, key, grouped, single, plans, alpha, beta, items);
+    }
+  }
   bool staged = false;
-  for (int i = 0; i < n; ++i) {
+  if (gr) {
+    Timed t(ex, "grouped");
+    gr->last_use = ++ex.graph_clock;
+    check_cuda(cudaGraphLaunch(gr->exec, ex.stream), "cudaGraphLaunch");
+  }
+  for (size_t j = 0; j < single.size(); ++j) {
+    const int i = single[j];
     staged |= enqueue_item(*plans[i], ex, alpha[i], beta[i], items[i]);
     // A staged item's workspace is reused by the next item: drain between.
-    if (staged && i + 1 < n) finish(ex);
+    if (staged && j + 1 < single.size()) finish(ex);
   }
   if (ex.sync || staged) finish(ex);
 }
 
-void execute_vjp(Product&, Executor&, Scalar, const void*, const void*, const void*, void*, void*) {
-  throw Error(ERR_UNSUPPORTED, "Plan::vjp is not available in this build");
+namespace {
+
+bool has_repeat(const std::vector<int64_t>& labels) {
+  for (size_t i = 0; i < labels.size(); ++i)
+    for (size_t j = i + 1; j < labels.size(); ++j)
+      if (labels[i] == labels[j]) return true;
+  return false;
+}
+
+// Zero every element of `op`'s layout at `origin` (device or host memory).
+void zero_layout(Executor& ex, DType dt, const Operand& op, void* origin) {
+  const Layout& l = op.layout;
+  const size_t elem = dtype_size(dt);
+  __int128 n = 1, lo = 0, hi = 0;
+  for (size_t i = 0; i < l.rank(); ++i) {
+    n *= l.dims[i];
+    const __int128 reach = (__int128)(l.dims[i] - 1) * l.strides[i];
+    if (reach < 0) lo += reach; else hi += reach;
+  }
+  if (n <= 0) return;
+  const bool dense = n == hi - lo + 1;
+  if (classify(origin, ex.device) == Where::Device) {
+    char* base = static_cast<char*>(origin);
+    if (dense)
+      check_cuda(cudaMemsetAsync(base + (int64_t)lo * (int64_t)elem, 0, (size_t)n * elem, ex.stream), "zero fill");
+    else
+      check_cuda(dev::launch_fill_zero(elem, origin, (int)l.rank(), l.dims.data(), l.strides.data(), ex.stream),
+                 "zero fill launch");
+    return;
+  }
+  // Host memory: the staged copy of this operand is taken after this fill.
+  char* base = static_cast<char*>(origin);
+  if (dense) {
+    std::memset(base + (int64_t)lo * (int64_t)elem, 0, (size_t)n * elem);
+    return;
+  }
+  std::vector<int64_t> idx(l.rank(), 0);
+  for (__int128 t = 0; t < n; ++t) {
+    int64_t off = 0;
+    for (size_t a = 0; a < l.rank(); ++a) off += idx[a] * l.strides[a];
+    std::memset(base + off * (int64_t)elem, 0, elem);
+    for (size_t a = 0; a < l.rank(); ++a) {
+      if (++idx[a] < l.dims[a]) break;
+      idx[a] = 0;
+    }
+  }
+}
+
+}  // namespace
+
+// Plan::vjp. With P = op_A(A), Q = op_B(B) and D = op_D(alpha P Q + ...), the
+// cotangents follow the conjugate-Wirtinger convention (a real loss L, dX =
+// dL/d conj(X)): grad_P = conj(alpha) op_D(dD) conj(Q), grad_Q = conj(alpha)
+// conj(P) op_D(dD), and grad_A = op_A(grad_P), grad_B = op_B(grad_Q). Each is
+// one contraction of the existing kernels over the original labels: dA takes
+// A's labels as its output labels, so a repeated label of A writes the
+// diagonal (the rest of dA is zeroed first).
+void execute_vjp(Product& p, Executor& ex, Scalar alpha, const void* A, const void* B, const void* dD, void* dA,
+                 void* dB) {
+  const Problem& pb = p.problem;
+  const bool ca = pb.a.conj, cb = pb.b.conj, cd = pb.d.conj;
+  const bool cplx = dtype_complex(pb.dtype);
+  {
+    std::lock_guard<std::mutex> lk(p.mu);
+    if (dA && !p.adj_a) {
+      Operand x = pb.d, y = pb.b, out = pb.a;
+      x.conj = cd != ca;
+      y.conj = !(cb != ca);
+      out.conj = false;
+      p.adj_a.reset(new Product(Problem::from_labels(pb.dtype, x, y, CMode::Absent, out, out, pb.ld, pb.lb, false, {},
+                                                     pb.la, false, true)));
+    }
+    if (dB && !p.adj_b) {
+      Operand x = pb.a, y = pb.d, out = pb.b;
+      x.conj = !(ca != cb);
+      y.conj = cd != cb;
+      out.conj = false;
+      p.adj_b.reset(new Product(Problem::from_labels(pb.dtype, x, y, CMode::Absent, out, out, pb.la, pb.ld, false, {},
+                                                     pb.lb, false, true)));
+    }
+  }
+  if (dA) validate_item(*p.adj_a, Item{dD, B, nullptr, dA}, true);
+  if (dB) validate_item(*p.adj_b, Item{A, dD, nullptr, dB}, true);
+  std::lock_guard<std::mutex> lk(ex.mu);
+  DeviceGuard g(ex.device);
+  const Scalar conj_alpha{alpha.re, cplx ? -alpha.im : 0.0};
+  const Scalar zero{};
+  bool staged = false;
+  if (dA) {
+    if (has_repeat(pb.la)) zero_layout(ex, pb.dtype, pb.a, dA);
+    staged |= enqueue_item(*p.adj_a, ex, ca ? alpha : conj_alpha, zero, Item{dD, B, nullptr, dA});
+  }
+  if (dB) {
+    if (staged) finish(ex);  // the staged workspace is reused
+    if (has_repeat(pb.lb)) zero_layout(ex, pb.dtype, pb.b, dB);
+    staged |= enqueue_item(*p.adj_b, ex, cb ? alpha : conj_alpha, zero, Item{A, dD, nullptr, dB});
+  }
+  if (ex.sync || staged) finish(ex);
 }
 
 }  // namespace tprims

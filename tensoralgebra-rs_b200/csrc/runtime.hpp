@@ -52,6 +52,7 @@ struct Executor {
   bool own_stream = false;
   bool sync = true;
   bool profile = false;
+  bool grouping = true;
   KernelTimes times;
   size_t pool_size = 0, budget = 1;  // recorded for the pooled-executor extension
   void* ws = nullptr;
@@ -60,6 +61,15 @@ struct Executor {
   int num_sms = 148;
   std::mutex mu;
   std::atomic<int> inflight{0};
+  // CUDA graphs of grouped submissions, keyed by the item list.
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    void* buf = nullptr;  // descriptors, tile starts, claim counters
+    uint64_t last_use = 0;
+    std::vector<int> single;  // items of the list that run individually
+  };
+  std::map<uint64_t, Graph> graphs;
+  uint64_t graph_clock = 0;
 
   static Executor* create(int device, uintptr_t stream);
   ~Executor();
@@ -81,6 +91,8 @@ struct Product {
   int kernel_pin = 0;
   std::mutex mu;
   std::map<int, DeviceScatters> dev;  // per device
+  // Adjoint contractions of Plan::vjp, built on first use.
+  std::unique_ptr<Product> adj_a, adj_b;
 
   explicit Product(const Problem& p);
   ~Product();

@@ -67,6 +67,7 @@ ABI_SYMBOLS = [
     "tprims_b200_product_set_tile", "tprims_b200_product_report", "tprims_b200_product_from_dot_general",
     "tprims_b200_execute_product_dlpack", "tprims_b200_contract_batched", "tprims_b200_product_vjp",
     "tprims_b200_product_scatter", "tprims_b200_executor_set_profiling", "tprims_b200_executor_kernel_times",
+    "tprims_b200_executor_set_grouping",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -96,6 +97,7 @@ lib.tprims_b200_executor_stream.argtypes = [_ip, C.POINTER(C.c_size_t)]
 lib.tprims_b200_executor_set_sync.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_synchronize.argtypes = [_ip]
 lib.tprims_b200_executor_set_profiling.argtypes = [_ip, C.c_int]
+lib.tprims_b200_executor_set_grouping.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_kernel_times.argtypes = [_ip, C.c_char_p, C.c_size_t, C.c_int]
 lib.tprims_b200_executor_kernel_times.restype = C.c_size_t
 lib.tprims_tapp_executor_create_rayon.argtypes = [C.POINTER(_ip), C.c_size_t, _vp]
@@ -269,6 +271,10 @@ class Executor:
 
     def synchronize(self):
         check(lib.tprims_b200_executor_synchronize(self.h))
+
+    def set_grouping(self, on: bool):
+        """Grouped persistent launches (cached in CUDA graphs) for lists; off = one launch per item."""
+        check(lib.tprims_b200_executor_set_grouping(self.h, 1 if on else 0))
 
     def set_profiling(self, on: bool):
         """Record CUDA events around every kernel launch on this executor."""
@@ -526,6 +532,25 @@ class Item:
     beta: object = 0
     c: object = None
     _keep: list = field(default_factory=list)
+
+
+class PreparedBatch:
+    """A list of (plan, operands) frozen into the C item array once, for
+    repeated submission without rebuilding it (see ``contract_batched``)."""
+
+    def __init__(self, items: Sequence[Item]):
+        self.n = len(items)
+        self.arr = (BatchItem * max(self.n, 1))()
+        self._keep = []
+        for i, it in enumerate(items):
+            al = scalar_bytes(it.plan.dtype, it.alpha)
+            be = scalar_bytes(it.plan.dtype, it.beta)
+            self._keep += [al, be, it.plan]
+            self.arr[i] = BatchItem(it.plan.product.h, C.cast(al, _vp), ptr_of(it.a), ptr_of(it.b), C.cast(be, _vp),
+                                    ptr_of(it.c), ptr_of(it.d))
+
+    def run(self, exec_: Optional[Executor] = None):
+        check(lib.tprims_b200_contract_batched(exec_.h if exec_ else 0, self.n, self.arr))
 
 
 def contract_batched(items: Sequence[Item], exec_: Optional[Executor] = None):

@@ -1,0 +1,146 @@
+"""The Ozaki INT8 slice scheme (f64 / c64 on tcgen05 kind::i8) against the
+extended-precision label oracle, through the C ABI. Stated bound: relative
+Frobenius error <= 1e-12 with the default 7 slices."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import Op, make_product, oracle_ref, rnd, run
+
+pytestmark = pytest.mark.gpu
+
+OZ = 3  # TPRIMS_PREC_OZAKI_INT8
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available()
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ex(tp, torch_cuda):
+    e = tp.Executor()
+    yield e
+    e.close()
+
+
+def run_oz(tp, ex, torch, dt, A, B, C, D, alpha, beta, slices=0, device=True):
+    p = make_product(tp, dt, A, B, C, D)
+    p.set_precision(OZ, slices)
+    rep = p.report()
+    assert rep["scheme"] == "ozaki-int8"
+    st, got, _ = run(tp, ex, torch, dt, A, B, C, D, alpha, beta, device=device, precision=0, kernel=0)
+    return p, got
+
+
+def _run_prepared(tp, ex, torch, p, A, B, C, D, alpha, beta):
+    tens = {}
+
+    def dptr(o, b, key):
+        t = torch.from_numpy(b.copy()).cuda()
+        tens[key] = t
+        return t.data_ptr() + o.offset * b.itemsize
+
+    pa, pb, pd = dptr(A, A.buf, "a"), dptr(B, B.buf, "b"), dptr(D, D.buf, "d")
+    pc = None if C is None else (pd if C.buf is D.buf else dptr(C, C.buf, "c"))
+    st = p.execute(ex, alpha, pa, pb, beta, pc, pd)
+    torch.cuda.synchronize()
+    assert st == 0, tp.last_error()
+    return tens["d"].cpu().numpy()
+
+
+def oz(tp, ex, torch, dt, A, B, C, D, alpha, beta, slices=0):
+    p = make_product(tp, dt, A, B, C, D)
+    p.set_precision(OZ, slices)
+    return _run_prepared(tp, ex, torch, p, A, B, C, D, alpha, beta), p
+
+
+@pytest.mark.parametrize("dt", ["float64", "complex128"])
+def test_ozaki_ragged_batched_general_strides(tp, ex, torch_cuda, orc, dt):
+    rng = np.random.default_rng(41)
+    for (m, n, k, h) in [(1, 1, 1, 1), (7, 13, 5, 1), (130, 257, 70, 1), (65, 33, 129, 3)]:
+        A = Op(rnd(rng, dt, h * m * k), [h, k, m], [1, h, h * k], [9, 2, 0])  # k before m
+        B = Op(rnd(rng, dt, h * k * n), [h, n, k], [1, h * k, h], [9, 1, 2])
+        C = Op(rnd(rng, dt, h * m * n), [h, m, n], [1, h, h * m], [9, 0, 1])
+        d0 = np.zeros(h * m * n, dtype=dt)
+        D = Op(d0, [h, m, n], [1, h, h * m], [9, 0, 1])
+        al, be = (complex(0.5, -0.25), complex(-1.5, 0.5)) if dt == "complex128" else (0.75, -1.5)
+        want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
+        got, p = oz(tp, ex, torch_cuda, dt, A, B, C, D, al, be)
+        err = orc.rel_frobenius(got, want)
+        assert err <= 1e-12, (m, n, k, h, err, p.report()["family"])
+
+
+@pytest.mark.parametrize("mask", range(16))
+def test_ozaki_complex_every_conjugation(tp, ex, torch_cuda, orc, mask):
+    rng = np.random.default_rng(500 + mask)
+    dt = "complex128"
+    A = Op(rnd(rng, dt, 20 * 9), [20, 9], [1, 20], [0, 2], conj=bool(mask & 1))
+    B = Op(rnd(rng, dt, 9 * 11), [9, 11], [11, 1], [2, 1], conj=bool(mask & 2))
+    C = Op(rnd(rng, dt, 20 * 11), [20, 11], [1, 20], [0, 1], conj=bool(mask & 4))
+    d0 = np.zeros(220, dtype=dt)
+    D = Op(d0, [20, 11], [1, 20], [0, 1], conj=bool(mask & 8))
+    al, be = complex(1.25, -0.5), complex(0.75, 0.5)
+    want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
+    got, _ = oz(tp, ex, torch_cuda, dt, A, B, C, D, al, be)
+    assert orc.rel_frobenius(got, want) <= 1e-12
+
+
+def test_ozaki_c1_full_size(tp, ex, torch_cuda, orc):
+    rng = np.random.default_rng(20261203 + 1000 + 10)
+    e = 24
+    cm = [1, e, e * e, e ** 3]
+    A = Op(rng.uniform(-1, 1, e ** 4), [e] * 4, cm, [0, 4, 1, 5])
+    B = Op(rng.uniform(-1, 1, e ** 4), [e] * 4, cm, [5, 2, 4, 3])
+    C = Op(rng.uniform(-1, 1, e ** 4), [e] * 4, cm, [0, 1, 2, 3])
+    d0 = np.zeros(e ** 4)
+    D = Op(d0, [e] * 4, cm, [0, 1, 2, 3])
+    want = oracle_ref(orc, "float64", A, B, C, D, 1.0, 0.5, d0)
+    got, _ = oz(tp, ex, torch_cuda, "float64", A, B, C, D, 1.0, 0.5)
+    assert orc.rel_frobenius(got, want) <= 1e-12
+
+
+@pytest.mark.parametrize("dt", ["float64", "complex128"])
+def test_ozaki_deep_k_is_split_into_exact_chunks(tp, ex, torch_cuda, orc, dt):
+    # K = 40000 exceeds one INT32-exact chunk (about 19000 at 7 slices); later
+    # chunks accumulate into D with beta = 1 and op_C = op_D.
+    rng = np.random.default_rng(43)
+    m, n, k = 5, 6, 40000
+    A = Op(rnd(rng, dt, m * k), [m, k], [1, m], [0, 2])
+    B = Op(rnd(rng, dt, k * n), [k, n], [1, k], [2, 1])
+    C = Op(rnd(rng, dt, m * n), [m, n], [1, m], [0, 1])
+    d0 = np.zeros(m * n, dtype=dt)
+    D = Op(d0, [m, n], [1, m], [0, 1], conj=dt == "complex128")
+    want = oracle_ref(orc, dt, A, B, C, D, 1.0, 0.5, d0)
+    got, _ = oz(tp, ex, torch_cuda, dt, A, B, C, D, 1.0, 0.5)
+    assert orc.rel_frobenius(got, want) <= 1e-12
+
+
+def test_ozaki_error_falls_with_slices(tp, ex, torch_cuda, orc):
+    rng = np.random.default_rng(44)
+    m, n, k = 96, 80, 200
+    A = Op(rnd(rng, "float64", m * k), [m, k], [1, m], [0, 2])
+    B = Op(rnd(rng, "float64", k * n), [k, n], [1, k], [2, 1])
+    d0 = np.zeros(m * n)
+    D = Op(d0, [m, n], [1, m], [0, 1])
+    want = oracle_ref(orc, "float64", A, B, None, D, 1.0, 0.0, d0)
+    errs = []
+    for s in (4, 5, 6, 7, 8):
+        got, _ = oz(tp, ex, torch_cuda, "float64", A, B, None, D, 1.0, 0.0, slices=s)
+        errs.append(orc.rel_frobenius(got, want))
+    assert all(errs[i + 1] < errs[i] for i in range(3)), errs
+    assert errs[3] <= 1e-12 and errs[4] <= 1e-13, errs
+
+
+def test_ozaki_non_finite_rows_give_nan(tp, ex, torch_cuda, orc):
+    rng = np.random.default_rng(45)
+    a = rng.standard_normal(8 * 6)
+    a[3 + 8 * 2] = np.inf  # row 3 of A
+    A = Op(a, [8, 6], [1, 8], [0, 2])
+    B = Op(rng.standard_normal(6 * 5), [6, 5], [1, 6], [2, 1])
+    D = Op(np.zeros(40), [8, 5], [1, 8], [0, 1])
+    got, _ = oz(tp, ex, torch_cuda, "float64", A, B, None, D, 1.0, 0.0)
+    G = got.reshape(5, 8).T
+    assert np.all(np.isnan(G[3])) and np.all(np.isfinite(np.delete(G, 3, axis=0)))

@@ -183,8 +183,9 @@ extern "C" {
 
 /* Executor on CUDA device `device` (-1 = the current device). `stream` is a
    cudaStream_t passed as an integer; 0 makes the executor create its own
-   non-blocking stream. No reference counterpart: the reference's executors are
-   CPU thread pools (executor.rs:278-392). */
+   stream, a blocking one (ordered with work on the legacy default stream).
+   No reference counterpart: the reference's executors are CPU thread pools
+   (executor.rs:278-392). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_create(TAPP_executor* out, int device, uintptr_t stream);
 /* The executor's stream, as an integer cudaStream_t. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_stream(TAPP_executor exec, uintptr_t* stream);
@@ -200,6 +201,19 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_synchronize(TAPP_executor exe
    device memory run as one persistent grouped launch per kernel family,
    replayed from a cached CUDA graph; with 0 every item is its own launch. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on);
+/* Failure detection without a GPU fault. tprims_b200_executor_set_workspace_limit
+   caps the executor's workspace arena (0 = no cap): a call that needs more is
+   refused with TPRIMS_ERR_INTERNAL before anything runs (allocation-failure
+   injection). tprims_b200_executor_selftest_wait launches one kernel that waits
+   on a flag nothing sets and gives up after `limit_ns`; the executor reports
+   the recorded timeout as TPRIMS_ERR_INTERNAL and stays usable. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_workspace_limit(TAPP_executor exec, size_t bytes);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor exec, uint64_t limit_ns);
+/* Measured pipe peak for roofline denominators (diagnostics): which = 0 runs
+   the FP64 DMMA pipe (mma.sync m8n8k4), 1 the FP32 FFMA pipe, with
+   register-only operation chains on every SM; *tflops receives the best of a
+   few timed launches (CUDA events on the executor's stream). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int which, double* tflops);
 /* Per-kernel timing (diagnostics, off by default): with `on` != 0 the executor
    records CUDA events on its stream around every kernel launch. The totals
    are resolved whenever the stream is drained. */

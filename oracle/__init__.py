@@ -21,13 +21,22 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _cpu_has_avx2() -> bool:
+def _cpu_flags() -> str:
     try:
         with open("/proc/cpuinfo") as f:
-            txt = f.read()
-        return " avx2" in txt and " fma" in txt
+            return f.read()
     except OSError:
-        return False
+        return ""
+
+
+def _cpu_has_avx2() -> bool:
+    txt = _cpu_flags()
+    return " avx2" in txt and " fma" in txt
+
+
+def _cpu_has_avx512() -> bool:
+    txt = _cpu_flags()
+    return all(f" {f}" in txt for f in ("avx512f", "avx512dq", "avx512bw", "avx512vl", "avx512cd"))
 
 
 def build():
@@ -35,7 +44,8 @@ def build():
 
 
 def _load():
-    names = (["liboracle_v3.so"] if _cpu_has_avx2() else []) + ["liboracle_base.so"]
+    names = ((["liboracle_v4.so"] if _cpu_has_avx512() else []) + (["liboracle_v3.so"] if _cpu_has_avx2() else [])
+             + ["liboracle_base.so"])
     for n in names:
         p = os.path.join(_HERE, n)
         if os.path.exists(p):

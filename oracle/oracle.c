@@ -277,13 +277,21 @@ static i64vec pk_scatter(const pk_axis* ax, int n, int slot) {
    through this macro-free generic body using double/float switches. */
 typedef struct {
   int dtype, cplx, real_bytes;
+  int mr, nr; /* register tile of the micro-kernel */
   int64_t M, N, K, H;
   i64vec a_m, a_k, b_k, b_n, c_m, c_n, d_m, d_n, h_a, h_b, h_c, h_d;
   int conj_a, conj_b, conj_c, conj_d;
 } pk_plan;
 
-#define PK_MR 8
-#define PK_NR 6
+/* Register tiles: the reference's default x86 families (f64 24x8 and f32 48x8
+   AVX-512, crates/tprims-kernel/tests/snapshots/x86_64_manifest.txt) when this
+   file is built with AVX-512, a scalar 8x6 tile otherwise and for the planar
+   complex kernels. */
+#define PK_MR_MAX 48
+#define PK_NR_MAX 8
+#ifdef __AVX512F__
+#include <immintrin.h>
+#endif
 
 static double rd(const pk_plan* p, const void* base, int64_t off, int part) {
   switch (p->dtype) {
@@ -302,57 +310,124 @@ static void wr(const pk_plan* p, void* base, int64_t off, double re, double im) 
   }
 }
 
-/* The micro-kernel on packed panels. For f32 the accumulation runs in float
-   (as the reference's f32 kernels do), for f64 in double. Planar complex
-   follows planar_ukr's four real products. */
-static void ukr_f64(int kc, const double* a, const double* b, double* ab, int cplx) {
+/* The micro-kernel on packed panels: overwrite the mr x nr tile `ab`
+   (column-major, j * mr + i; planar complex adds the imaginary plane at
+   mr * nr) with the panel product. For f32 the accumulation runs in float, as
+   the reference's f32 kernels do; planar complex follows planar_ukr's four
+   real products (kernels/reference/scalar.rs:64-106). */
+#ifdef __AVX512F__
+static void ukr_f64_avx512(int kc, const double* a, const double* b, double* ab) {
+  __m512d c[3][8];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 8; ++j) c[i][j] = _mm512_setzero_pd();
+  for (int p = 0; p < kc; ++p) {
+    const __m512d a0 = _mm512_loadu_pd(a + 24 * p), a1 = _mm512_loadu_pd(a + 24 * p + 8),
+                  a2 = _mm512_loadu_pd(a + 24 * p + 16);
+    for (int j = 0; j < 8; ++j) {
+      const __m512d bj = _mm512_set1_pd(b[8 * p + j]);
+      c[0][j] = _mm512_fmadd_pd(a0, bj, c[0][j]);
+      c[1][j] = _mm512_fmadd_pd(a1, bj, c[1][j]);
+      c[2][j] = _mm512_fmadd_pd(a2, bj, c[2][j]);
+    }
+  }
+  for (int j = 0; j < 8; ++j)
+    for (int i = 0; i < 3; ++i) _mm512_storeu_pd(ab + 24 * j + 8 * i, c[i][j]);
+}
+static void ukr_f32_avx512(int kc, const float* a, const float* b, float* ab) {
+  __m512 c[3][8];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 8; ++j) c[i][j] = _mm512_setzero_ps();
+  for (int p = 0; p < kc; ++p) {
+    const __m512 a0 = _mm512_loadu_ps(a + 48 * p), a1 = _mm512_loadu_ps(a + 48 * p + 16),
+                 a2 = _mm512_loadu_ps(a + 48 * p + 32);
+    for (int j = 0; j < 8; ++j) {
+      const __m512 bj = _mm512_set1_ps(b[8 * p + j]);
+      c[0][j] = _mm512_fmadd_ps(a0, bj, c[0][j]);
+      c[1][j] = _mm512_fmadd_ps(a1, bj, c[1][j]);
+      c[2][j] = _mm512_fmadd_ps(a2, bj, c[2][j]);
+    }
+  }
+  for (int j = 0; j < 8; ++j)
+    for (int i = 0; i < 3; ++i) _mm512_storeu_ps(ab + 48 * j + 16 * i, c[i][j]);
+}
+#endif
+
+static void ukr_f64(int kc, const double* a, const double* b, double* ab, int cplx, int mr, int nr) {
+#ifdef __AVX512F__
+  if (!cplx && mr == 24 && nr == 8) {
+    ukr_f64_avx512(kc, a, b, ab);
+    return;
+  }
+#endif
   if (!cplx) {
-    double acc[PK_NR][PK_MR] = {{0}};
+    double acc[PK_NR_MAX][PK_MR_MAX];
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) acc[j][i] = 0;
     for (int p = 0; p < kc; ++p)
-      for (int j = 0; j < PK_NR; ++j) {
-        const double bv = b[p * PK_NR + j];
-        for (int i = 0; i < PK_MR; ++i) acc[j][i] += a[p * PK_MR + i] * bv;
+      for (int j = 0; j < nr; ++j) {
+        const double bv = b[p * nr + j];
+        for (int i = 0; i < mr; ++i) acc[j][i] += a[p * mr + i] * bv;
       }
-    memcpy(ab, acc, sizeof(acc));
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) ab[j * mr + i] = acc[j][i];
   } else {
-    double re[PK_NR][PK_MR] = {{0}}, im[PK_NR][PK_MR] = {{0}};
+    double re[PK_NR_MAX][PK_MR_MAX], im[PK_NR_MAX][PK_MR_MAX];
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) re[j][i] = im[j][i] = 0;
     for (int p = 0; p < kc; ++p) {
-      const double *ar = a + p * 2 * PK_MR, *ai = ar + PK_MR, *br = b + p * 2 * PK_NR, *bi = br + PK_NR;
-      for (int j = 0; j < PK_NR; ++j)
-        for (int i = 0; i < PK_MR; ++i) {
+      const double *ar = a + p * 2 * mr, *ai = ar + mr, *br = b + p * 2 * nr, *bi = br + nr;
+      for (int j = 0; j < nr; ++j)
+        for (int i = 0; i < mr; ++i) {
           re[j][i] += ar[i] * br[j];
           re[j][i] += -(ai[i] * bi[j]);
           im[j][i] += ar[i] * bi[j];
           im[j][i] += ai[i] * br[j];
         }
     }
-    memcpy(ab, re, sizeof(re));
-    memcpy(ab + PK_MR * PK_NR, im, sizeof(im));
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) {
+        ab[j * mr + i] = re[j][i];
+        ab[mr * nr + j * mr + i] = im[j][i];
+      }
   }
 }
-static void ukr_f32(int kc, const float* a, const float* b, float* ab, int cplx) {
+static void ukr_f32(int kc, const float* a, const float* b, float* ab, int cplx, int mr, int nr) {
+#ifdef __AVX512F__
+  if (!cplx && mr == 48 && nr == 8) {
+    ukr_f32_avx512(kc, a, b, ab);
+    return;
+  }
+#endif
   if (!cplx) {
-    float acc[PK_NR][PK_MR] = {{0}};
+    float acc[PK_NR_MAX][PK_MR_MAX];
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) acc[j][i] = 0;
     for (int p = 0; p < kc; ++p)
-      for (int j = 0; j < PK_NR; ++j) {
-        const float bv = b[p * PK_NR + j];
-        for (int i = 0; i < PK_MR; ++i) acc[j][i] += a[p * PK_MR + i] * bv;
+      for (int j = 0; j < nr; ++j) {
+        const float bv = b[p * nr + j];
+        for (int i = 0; i < mr; ++i) acc[j][i] += a[p * mr + i] * bv;
       }
-    memcpy(ab, acc, sizeof(acc));
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) ab[j * mr + i] = acc[j][i];
   } else {
-    float re[PK_NR][PK_MR] = {{0}}, im[PK_NR][PK_MR] = {{0}};
+    float re[PK_NR_MAX][PK_MR_MAX], im[PK_NR_MAX][PK_MR_MAX];
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) re[j][i] = im[j][i] = 0;
     for (int p = 0; p < kc; ++p) {
-      const float *ar = a + p * 2 * PK_MR, *ai = ar + PK_MR, *br = b + p * 2 * PK_NR, *bi = br + PK_NR;
-      for (int j = 0; j < PK_NR; ++j)
-        for (int i = 0; i < PK_MR; ++i) {
+      const float *ar = a + p * 2 * mr, *ai = ar + mr, *br = b + p * 2 * nr, *bi = br + nr;
+      for (int j = 0; j < nr; ++j)
+        for (int i = 0; i < mr; ++i) {
           re[j][i] += ar[i] * br[j];
           re[j][i] += -(ai[i] * bi[j]);
           im[j][i] += ar[i] * bi[j];
           im[j][i] += ai[i] * br[j];
         }
     }
-    memcpy(ab, re, sizeof(re));
-    memcpy(ab + PK_MR * PK_NR, im, sizeof(im));
+    for (int j = 0; j < nr; ++j)
+      for (int i = 0; i < mr; ++i) {
+        ab[j * mr + i] = re[j][i];
+        ab[mr * nr + j * mr + i] = im[j][i];
+      }
   }
 }
 
@@ -370,11 +445,11 @@ static void pk_writeback(const pk_plan* p, const void* ab, int mrem, int nrem, i
     for (int i = 0; i < mrem; ++i) {
       double tr, ti = 0;
       if (p->real_bytes == 4) {
-        tr = ((const float*)ab)[j * PK_MR + i];
-        if (cp) ti = ((const float*)ab)[PK_MR * PK_NR + j * PK_MR + i];
+        tr = ((const float*)ab)[j * p->mr + i];
+        if (cp) ti = ((const float*)ab)[p->mr * p->nr + j * p->mr + i];
       } else {
-        tr = ((const double*)ab)[j * PK_MR + i];
-        if (cp) ti = ((const double*)ab)[PK_MR * PK_NR + j * PK_MR + i];
+        tr = ((const double*)ab)[j * p->mr + i];
+        if (cp) ti = ((const double*)ab)[p->mr * p->nr + j * p->mr + i];
       }
       const int64_t doff = p->h_d.v[h] + p->d_m.v[i0 + i] + p->d_n.v[j0 + j];
       double vr, vi;
@@ -452,6 +527,17 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
   p.dtype = dtype;
   p.cplx = is_cplx(dtype);
   p.real_bytes = (dtype == OR_F32 || dtype == OR_C32) ? 4 : 8;
+  p.mr = 8;
+  p.nr = 6;
+#ifdef __AVX512F__
+  if (dtype == OR_F64) {
+    p.mr = 24;
+    p.nr = 8;
+  } else if (dtype == OR_F32) {
+    p.mr = 48;
+    p.nr = 8;
+  }
+#endif
   p.a_m = pk_scatter(am, nm, 0);
   p.a_k = pk_scatter(ak, nk, 0);
   p.b_k = pk_scatter(ak, nk, 1);
@@ -502,15 +588,16 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
   const int64_t kc = p.real_bytes == 4 ? 384 : 256;
   int64_t mc = (512 * 1024) / (kc * planes * p.real_bytes);
   int64_t nc = (3 * 1024 * 1024) / (kc * planes * p.real_bytes);
-  mc = mc / PK_MR * PK_MR;
-  nc = nc / PK_NR * PK_NR;
-  if (mc < PK_MR) mc = PK_MR;
-  if (nc < PK_NR) nc = PK_NR;
+  const int MR = p.mr, NR = p.nr;
+  mc = mc / MR * MR;
+  nc = nc / NR * NR;
+  if (mc < MR) mc = MR;
+  if (nc < NR) nc = NR;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
   const size_t rb = (size_t)p.real_bytes;
-  char* bpanel = (char*)malloc((size_t)(nc + PK_NR) * kc * planes * rb);
+  char* bpanel = (char*)malloc((size_t)(nc + NR) * kc * planes * rb);
   if (!bpanel) {
     pk_free(&p);
     return 3;
@@ -519,15 +606,15 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
     const int64_t ha = p.h_a.v[h], hb = p.h_b.v[h];
     for (int64_t jc = 0; jc < p.N; jc += nc) {
       const int64_t ncur = (p.N - jc < nc) ? p.N - jc : nc;
-      const int64_t nsl = (ncur + PK_NR - 1) / PK_NR;
+      const int64_t nsl = (ncur + NR - 1) / NR;
       for (int64_t pc = 0; pc < p.K; pc += kc) {
         const int64_t kcur = (p.K - pc < kc) ? p.K - pc : kc;
         /* pack B: slivers of NR columns, per k: NR reals (x planes) */
 #pragma omp parallel for schedule(static)
         for (int64_t s = 0; s < nsl; ++s) {
           for (int64_t q = 0; q < kcur; ++q)
-            for (int j = 0; j < PK_NR; ++j) {
-              const int64_t col = jc + s * PK_NR + j;
+            for (int j = 0; j < NR; ++j) {
+              const int64_t col = jc + s * NR + j;
               double vr = 0, vi = 0;
               if (col < p.N) {
                 const int64_t off = hb + p.b_k.v[pc + q] + p.b_n.v[col];
@@ -535,13 +622,13 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
                 vi = cp ? rd(&p, B->data, off, 1) : 0;
                 if (p.conj_b) vi = -vi;
               }
-              const size_t idx = (size_t)(s * kcur + q) * planes * PK_NR;
+              const size_t idx = (size_t)(s * kcur + q) * planes * NR;
               if (rb == 4) {
                 ((float*)bpanel)[idx + j] = (float)vr;
-                if (cp) ((float*)bpanel)[idx + PK_NR + j] = (float)vi;
+                if (cp) ((float*)bpanel)[idx + NR + j] = (float)vi;
               } else {
                 ((double*)bpanel)[idx + j] = vr;
-                if (cp) ((double*)bpanel)[idx + PK_NR + j] = vi;
+                if (cp) ((double*)bpanel)[idx + NR + j] = vi;
               }
             }
         }
@@ -557,18 +644,18 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
         const int first = pc == 0;
 #pragma omp parallel
         {
-          char* apanel = (char*)malloc((size_t)(mc + PK_MR) * kc * planes * rb);
-          double abbuf[2 * PK_MR * PK_NR];
+          char* apanel = (char*)malloc((size_t)(mc + MR) * kc * planes * rb);
+          double abbuf[2 * PK_MR_MAX * PK_NR_MAX];
 #pragma omp for schedule(static) collapse(2)
           for (int64_t ib = 0; ib < nic; ++ib)
             for (int64_t gi = 0; gi < groups; ++gi) {
               const int64_t ic = ib * mc;
               const int64_t mcur = (p.M - ic < mc) ? p.M - ic : mc;
-              const int64_t msl = (mcur + PK_MR - 1) / PK_MR;
+              const int64_t msl = (mcur + MR - 1) / MR;
               for (int64_t s = 0; s < msl; ++s)
                 for (int64_t q = 0; q < kcur; ++q)
-                  for (int i = 0; i < PK_MR; ++i) {
-                    const int64_t row = ic + s * PK_MR + i;
+                  for (int i = 0; i < MR; ++i) {
+                    const int64_t row = ic + s * MR + i;
                     double vr = 0, vi = 0;
                     if (row < p.M) {
                       const int64_t off = ha + p.a_m.v[row] + p.a_k.v[pc + q];
@@ -576,26 +663,26 @@ int oracle_packed_contract(int dtype, const double* alpha, const or_operand* A, 
                       vi = cp ? rd(&p, A->data, off, 1) : 0;
                       if (p.conj_a) vi = -vi;
                     }
-                    const size_t idx = (size_t)(s * kcur + q) * planes * PK_MR;
+                    const size_t idx = (size_t)(s * kcur + q) * planes * MR;
                     if (rb == 4) {
                       ((float*)apanel)[idx + i] = (float)vr;
-                      if (cp) ((float*)apanel)[idx + PK_MR + i] = (float)vi;
+                      if (cp) ((float*)apanel)[idx + MR + i] = (float)vi;
                     } else {
                       ((double*)apanel)[idx + i] = vr;
-                      if (cp) ((double*)apanel)[idx + PK_MR + i] = vi;
+                      if (cp) ((double*)apanel)[idx + MR + i] = vi;
                     }
                   }
               const int64_t s0 = nsl * gi / groups, s1 = nsl * (gi + 1) / groups;
               for (int64_t jr = s0; jr < s1; ++jr)
                 for (int64_t ir = 0; ir < msl; ++ir) {
-                  const size_t aoff = (size_t)ir * kcur * planes * PK_MR, boff = (size_t)jr * kcur * planes * PK_NR;
+                  const size_t aoff = (size_t)ir * kcur * planes * MR, boff = (size_t)jr * kcur * planes * NR;
                   if (rb == 4)
-                    ukr_f32((int)kcur, (float*)apanel + aoff, (float*)bpanel + boff, (float*)abbuf, cp);
+                    ukr_f32((int)kcur, (float*)apanel + aoff, (float*)bpanel + boff, (float*)abbuf, cp, MR, NR);
                   else
-                    ukr_f64((int)kcur, (double*)apanel + aoff, (double*)bpanel + boff, abbuf, cp);
-                  const int64_t i0 = ic + ir * PK_MR, j0 = jc + jr * PK_NR;
-                  const int mrem = (int)((p.M - i0 < PK_MR) ? p.M - i0 : PK_MR);
-                  const int nrem = (int)((p.N - j0 < PK_NR) ? p.N - j0 : PK_NR);
+                    ukr_f64((int)kcur, (double*)apanel + aoff, (double*)bpanel + boff, abbuf, cp, MR, NR);
+                  const int64_t i0 = ic + ir * MR, j0 = jc + jr * NR;
+                  const int mrem = (int)((p.M - i0 < MR) ? p.M - i0 : MR);
+                  const int nrem = (int)((p.N - j0 < NR) ? p.N - j0 : NR);
                   pk_writeback(&p, abbuf, mrem, nrem, i0, j0, h, alpha, beta, first, beta_zero, Cd, Dd);
                 }
             }

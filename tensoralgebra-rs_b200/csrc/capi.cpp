@@ -6,6 +6,7 @@
 // error-to-status table are those of status.rs:13-43 and abi.rs:97-113.
 // Every entry point catches all C++ exceptions: nothing unwinds across the C
 // boundary, and the message of the last failure is kept per thread.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -683,7 +684,7 @@ extern "C" size_t tprims_b200_executor_kernel_times(TAPP_executor exec, char* bu
         int prev = -1;
         cudaGetDevice(&prev);
         cudaSetDevice(ex.device);
-        check_cuda(cudaStreamSynchronize(ex.stream), "kernel execution");
+        drain(ex);
         ex.times.resolve();
         s = kernel_times_json(ex, reset != 0);
         if (prev >= 0) cudaSetDevice(prev);
@@ -702,5 +703,71 @@ extern "C" TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int 
     Executor& ex = resolve_exec(exec)->get();
     std::lock_guard<std::mutex> lk(ex.mu);
     ex.grouping = on != 0;
+  });
+}
+
+extern "C" TAPP_error tprims_b200_executor_set_workspace_limit(TAPP_executor exec, size_t bytes) {
+  return ffi([&] {
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    ex.ws_limit = bytes == 0 ? SIZE_MAX : bytes;
+  });
+}
+
+extern "C" TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor exec, uint64_t limit_ns) {
+  return ffi([&] {
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ex.device);
+    struct Restore {
+      int d;
+      ~Restore() {
+        if (d >= 0) cudaSetDevice(d);
+      }
+    } restore{prev};
+    // The flag is a zeroed word of the status allocation that nothing writes.
+    unsigned* flag = ex.status + 32;
+    check_cuda(cudaMemsetAsync(flag, 0, sizeof(unsigned), ex.stream), "selftest flag");
+    check_cuda(dev::launch_wait_selftest(flag, ex.status, limit_ns, ex.stream), "selftest launch");
+    finish(ex);
+  });
+}
+
+extern "C" TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int which, double* tflops) {
+  return ffi([&] {
+    if (!tflops) null_arg("tflops out-parameter");
+    if (which != 0 && which != 1) throw Error(ERR_INVALID_ARGUMENT, "probe must be 0 (FP64 DMMA) or 1 (FP32 FFMA)");
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ex.device);
+    struct Restore {
+      int d;
+      ~Restore() {
+        if (d >= 0) cudaSetDevice(d);
+      }
+    } restore{prev};
+    void* sink = ex.workspace(4096);
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    const int blocks = ex.num_sms * (which == 0 ? 8 : 8);
+    const int iters = which == 0 ? 4096 : 65536;
+    double best = 0, flops = 0;
+    for (int rep = 0; rep < 5; ++rep) {
+      check_cuda(cudaEventRecord(e0, ex.stream), "cudaEventRecord");
+      check_cuda(dev::launch_probe(which, sink, blocks, iters, ex.stream, &flops), "probe launch");
+      check_cuda(cudaEventRecord(e1, ex.stream), "cudaEventRecord");
+      check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float ms = 0;
+      check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = best;
   });
 }

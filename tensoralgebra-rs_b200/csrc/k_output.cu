@@ -61,6 +61,73 @@ cudaError_t launch_output_pass(int dtype, const GemmArgs& g, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Self-test of the bounded-wait path: one thread waits for a flag that nothing
+// sets, gives up after `limit_ns` of %globaltimer, records the timeout in the
+// status word and returns, exactly as the tensor-core kernels do when a
+// barrier phase never completes. No fault, no trap: the context stays usable.
+__global__ void bounded_wait_selftest_kernel(const volatile unsigned* flag, unsigned* status, uint64_t limit_ns) {
+  if (threadIdx.x != 0) return;
+  const uint64_t t0 = globaltimer_ns();
+  while (*flag == 0u) {
+    if (globaltimer_ns() - t0 > limit_ns) {
+      atomicOr(status, STATUS_WAIT_TIMEOUT);
+      return;
+    }
+  }
+}
+
+cudaError_t launch_wait_selftest(const unsigned* flag, unsigned* status, uint64_t limit_ns, cudaStream_t st) {
+  bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(flag, status, limit_ns);
+  return cudaGetLastError();
+}
+
+// Pipe-peak probes for roofline denominators: register-only chains of
+// independent operations, no memory traffic. FP64: mma.sync m8n8k4 (DMMA,
+// 512 flops per warp instruction); FP32: FFMA (2 flops per lane).
+__global__ void __launch_bounds__(128) probe_dmma_kernel(double* sink, int iters) {
+  double acc[8][2];
+  double a = 1.0 + threadIdx.x * 1e-9, b = 1.0 - threadIdx.x * 1e-9;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                   : "+d"(acc[i][0]), "+d"(acc[i][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += acc[i][0] + acc[i][1];
+  if (s == 12345.678) sink[threadIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) probe_ffma_kernel(float* sink, int iters) {
+  float acc[16];
+  const float a = 1.0f + threadIdx.x * 1e-7f, b = 0.999f;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) acc[i] = (float)i;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = fmaf(acc[i], b, a);
+  }
+  float s = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) s += acc[i];
+  if (s == 12345.678f) sink[threadIdx.x] = s;
+}
+
+cudaError_t launch_probe(int which, void* sink, int blocks, int iters, cudaStream_t st, double* flops) {
+  if (which == 0) {
+    probe_dmma_kernel<<<blocks, 128, 0, st>>>(static_cast<double*>(sink), iters);
+    *flops = (double)blocks * 4 /*warps*/ * iters * 8 * 512.0;
+  } else {
+    probe_ffma_kernel<<<blocks, 256, 0, st>>>(static_cast<float*>(sink), iters);
+    *flops = (double)blocks * 256 * iters * 16 * 2.0;
+  }
+  return cudaGetLastError();
+}
+
 // Zero every element a layout addresses (rank <= 16): the off-diagonal part of
 // a cotangent whose operand has a repeated label.
 struct FillLayout {

@@ -372,17 +372,24 @@ __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
 // sorted by decreasing cost on the host, so the longest tiles go first); each
 // CTA claims the next tile with an atomic counter, copies the item's
 // arguments to shared memory and runs the same tile body as the one-item
-// kernels. Claiming never waits, so the kernel needs no bounded spin.
+// kernels. Claiming never waits. The kernel checks itself: a claim loop longer
+// than the queue, a run past a %globaltimer limit, or an item / tile index out
+// of range sets STATUS_BAD_ARGUMENT (or STATUS_WAIT_TIMEOUT) in the status
+// word and ends the CTA.
 template <class Tile, int NT>
 __global__ void __launch_bounds__(NT) grouped_kernel(const GroupItem* __restrict__ items,
                                                      const int64_t* __restrict__ tile_start, int nitems,
-                                                     unsigned long long* counter) {
+                                                     unsigned long long* counter, unsigned* status) {
   __shared__ __align__(16) GemmArgs sg;
   __shared__ long long claimed;
   __shared__ int item_s;
+  __shared__ int stop;
   const int64_t total = tile_start[nitems];
-  for (;;) {
+  const uint64_t t_start = globaltimer_ns();
+  constexpr uint64_t LIMIT_NS = 60000000000ull;  // 60 s for one grouped launch
+  for (int64_t iter = 0;; ++iter) {
     if (threadIdx.x == 0) {
+      stop = 0;
       claimed = (long long)atomicAdd(counter, 1ull);
       int lo = 0, hi = nitems - 1;  // the item whose tile range holds `claimed`
       while (lo < hi) {
@@ -390,10 +397,21 @@ __global__ void __launch_bounds__(NT) grouped_kernel(const GroupItem* __restrict
         if (tile_start[mid] <= claimed) lo = mid; else hi = mid - 1;
       }
       item_s = lo;
+      if (claimed < total) {
+        const int64_t local = claimed - tile_start[lo];
+        const int64_t nt = items[lo].tiles_m * items[lo].tiles_n * items[lo].g.H;
+        if (lo < 0 || lo >= nitems || local < 0 || local >= nt || iter > total) {
+          atomicOr(status, STATUS_BAD_ARGUMENT);
+          stop = 1;
+        } else if (globaltimer_ns() - t_start > LIMIT_NS) {
+          atomicOr(status, STATUS_WAIT_TIMEOUT);
+          stop = 1;
+        }
+      }
     }
     __syncthreads();
     const long long t = claimed;
-    if (t >= total) break;
+    if (t >= total || stop) break;
     const int it = item_s;
     {
       const int4* src = reinterpret_cast<const int4*>(&items[it].g);
@@ -506,45 +524,83 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
   *bm = *bn = 0;
 }
 
+// Loads the family's grouped kernel (module loading is lazy) so that the first
+// launch inside a stream capture does not have to.
+cudaError_t prepare_grouped(int kernel) {
+  cudaFuncAttributes fa;
+  switch (kernel) {
+    case PLAIN_F32_SIMT_128x128: {
+      using Op = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_F32_SIMT_64x64: {
+      using Op = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_C32_SIMT_64x64: {
+      using Op = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_F64_DMMA_64x64: {
+      using Op = DmmaTileOp<false, 32, 32, 16>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_F64_DMMA_32x32: {
+      using Op = DmmaTileOp<false, 16, 16, 16>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_C64_DMMA_64x32: {
+      using Op = DmmaTileOp<true, 32, 16, 8>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    case PLAIN_C64_DMMA_32x32: {
+      using Op = DmmaTileOp<true, 16, 16, 8>;
+      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
+    }
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
-                           unsigned long long* counter, int num_sms, cudaStream_t st) {
+                           unsigned long long* counter, unsigned* status, int num_sms, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   if (nitems <= 0) return cudaSuccess;
   switch (kernel) {
     case PLAIN_F32_SIMT_128x128: {
       using Op = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_F32_SIMT_64x64: {
       using Op = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_C32_SIMT_64x64: {
       using Op = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
-      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_F64_DMMA_64x64: {
       using Op = DmmaTileOp<false, 32, 32, 16>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_F64_DMMA_32x32: {
       using Op = DmmaTileOp<false, 16, 16, 16>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_C64_DMMA_64x32: {
       using Op = DmmaTileOp<true, 32, 16, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 3, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms * 3, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     case PLAIN_C64_DMMA_32x32: {
       using Op = DmmaTileOp<true, 16, 16, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter);
+      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
       break;
     }
     default:

@@ -74,8 +74,13 @@ struct GroupItem {
 void plain_tile_shape(int kernel, int* bm, int* bn);
 // Persistent grouped launch over `nitems` items whose tiles are numbered by the
 // prefix `tile_start[0..nitems]` (device arrays); `counter` is reset here.
+cudaError_t prepare_grouped(int kernel);
 cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
-                           unsigned long long* counter, int num_sms, cudaStream_t st);
+                           unsigned long long* counter, unsigned* status, int num_sms, cudaStream_t st);
+// Register-only pipe probes (0: FP64 DMMA, 1: FP32 FFMA); *flops = work launched.
+cudaError_t launch_probe(int which, void* sink, int blocks, int iters, cudaStream_t st, double* flops);
+// Bounded wait on a flag that stays zero: sets STATUS_WAIT_TIMEOUT after limit_ns.
+cudaError_t launch_wait_selftest(const unsigned* flag, unsigned* status, uint64_t limit_ns, cudaStream_t st);
 // Zero every element of a strided layout (origin = element of index 0).
 cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t* dims, const int64_t* strides,
                              cudaStream_t st);

@@ -2,6 +2,9 @@
 #include "runtime.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <sstream>
@@ -46,13 +49,17 @@ Executor* Executor::create(int device, uintptr_t stream) {
   ex->device = device;
   DeviceGuard g(device);
   if (stream == 0) {
-    check_cuda(cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // A blocking stream: ordered after work on the legacy default stream (where
+    // a caller such as torch writes the operands by default) and before work
+    // issued there afterwards, so no explicit synchronisation is needed around a call.
+    check_cuda(cudaStreamCreateWithFlags(&ex->stream, cudaStreamDefault), "cudaStreamCreate");
     ex->own_stream = true;
   } else {
     ex->stream = reinterpret_cast<cudaStream_t>(stream);
   }
   check_cuda(cudaMalloc(&ex->status, 256), "cudaMalloc(status)");
-  check_cuda(cudaMemset(ex->status, 0, 256), "cudaMemset(status)");
+  check_cuda(cudaMemsetAsync(ex->status, 0, 256, ex->stream), "cudaMemset(status)");
+  check_cuda(cudaStreamSynchronize(ex->stream), "cudaStreamSynchronize");
   check_cuda(cudaDeviceGetAttribute(&ex->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
   return ex.release();
 }
@@ -69,11 +76,15 @@ Executor::~Executor() {
   if (ws) cudaFree(ws);
   if (status) cudaFree(status);
   if (own_stream && stream) cudaStreamDestroy(stream);
+  if (capture_stream) cudaStreamDestroy(capture_stream);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
 void* Executor::workspace(size_t bytes) {
   if (bytes <= ws_bytes) return ws;
+  if (bytes > ws_limit)
+    throw Error(ERR_INTERNAL, "workspace of " + std::to_string(bytes) + " bytes exceeds the executor's limit of " +
+                                  std::to_string(ws_limit) + " bytes");
   // Growing: earlier work on the stream may still use the old arena.
   check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
   if (ws) cudaFree(ws);
@@ -85,7 +96,11 @@ void* Executor::workspace(size_t bytes) {
   return ws;
 }
 
-Product::Product(const Problem& p) : problem(p) {
+namespace {
+std::atomic<uint64_t> g_product_uid{1};
+}
+
+Product::Product(const Problem& p) : problem(p), uid(g_product_uid.fetch_add(1)) {
   packed = PackedPlan::from_problem(p);
   view = orient(packed, packed.transposes_gemm(32));
 }
@@ -100,7 +115,7 @@ Product::~Product() {
   }
 }
 
-const dev::Scatters& Product::scatters(int device) {
+const dev::Scatters& Product::scatters(int device, cudaStream_t stream) {
   std::lock_guard<std::mutex> lk(mu);
   auto it = dev.find(device);
   if (it != dev.end()) return it->second.s;
@@ -116,8 +131,16 @@ const dev::Scatters& Product::scatters(int device) {
   }
   DeviceScatters ds;
   check_cuda(cudaMalloc(&ds.buf, host.size() * sizeof(int64_t)), "cudaMalloc(scatters)");
-  check_cuda(cudaMemcpy(ds.buf, host.data(), host.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
-             "cudaMemcpy(scatters)");
+  // A plain cudaMemcpy from pageable memory may return before its DMA lands,
+  // and it is ordered on the legacy stream, which a non-blocking stream does
+  // not wait for: copy on the caller's stream and wait for it, so that the
+  // vectors are complete for every stream that uses them afterwards.
+  cudaError_t e = cudaMemcpyAsync(ds.buf, host.data(), host.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    cudaFree(ds.buf);
+    check_cuda(e, "scatter vector upload");
+  }
   const int64_t* b = ds.buf;
   ds.s = dev::Scatters{b + offs[0], b + offs[1], b + offs[2],  b + offs[3],  b + offs[4],  b + offs[5],
                        b + offs[6], b + offs[7], b + offs[8], b + offs[9], b + offs[10], b + offs[11]};
@@ -440,13 +463,29 @@ std::string kernel_times_json(Executor& ex, bool reset) {
   return o.str();
 }
 
+// Drain the stream, giving up (with an error) after a deadline instead of
+// blocking forever on work that does not finish.
+void drain(Executor& ex) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t q = cudaStreamQuery(ex.stream);
+    if (q == cudaSuccess) return;
+    if (q != cudaErrorNotReady) check_cuda(q, "kernel execution");
+    if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(ex.drain_limit_s))
+      throw Error(ERR_INTERNAL, "the executor's stream did not drain within " + std::to_string(ex.drain_limit_s) +
+                                    " s");
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
 void finish(Executor& ex) {
-  check_cuda(cudaStreamSynchronize(ex.stream), "kernel execution");
+  drain(ex);
   if (!ex.times.pending.empty()) ex.times.resolve();
   unsigned word = 0;
   check_cuda(cudaMemcpy(&word, ex.status, sizeof(word), cudaMemcpyDeviceToHost), "status read");
   if (word != 0) {
-    cudaMemset(ex.status, 0, sizeof(unsigned));
+    cudaMemsetAsync(ex.status, 0, sizeof(unsigned), ex.stream);
+    cudaStreamSynchronize(ex.stream);
     if (word & dev::STATUS_WAIT_TIMEOUT)
       throw Error(ERR_INTERNAL, "a kernel gave up on a bounded wait (device status word " + std::to_string(word) + ")");
     throw Error(ERR_INTERNAL, "a kernel reported device status word " + std::to_string(word));
@@ -460,7 +499,7 @@ namespace {
 dev::GemmArgs build_args(Product& pr, Executor& ex, Scalar alpha, Scalar beta, bool c_read, const char* a_dev,
                          const char* b_dev, const char* c_dev, char* d_dev) {
   dev::GemmArgs g{};
-  g.s = pr.scatters(ex.device);
+  g.s = pr.scatters(ex.device, ex.stream);
   g.A = pr.view.swapped ? b_dev : a_dev;
   g.B = pr.view.swapped ? a_dev : b_dev;
   g.C = c_dev;
@@ -577,9 +616,13 @@ uint64_t mix(uint64_t h, uint64_t v) {
 uint64_t list_key(int n, Product* const* plans, const Scalar* alpha, const Scalar* beta, const Item* items) {
   uint64_t key = 1469598103934665603ull;
   for (int i = 0; i < n; ++i) {
-    const uint64_t f[7] = {(uint64_t)(uintptr_t)plans[i], (uint64_t)(uintptr_t)items[i].a,
-                           (uint64_t)(uintptr_t)items[i].b, (uint64_t)(uintptr_t)items[i].c,
-                           (uint64_t)(uintptr_t)items[i].d, 0, 0};
+    const uint64_t f[7] = {plans[i]->uid,
+                           (uint64_t)(uintptr_t)items[i].a,
+                           (uint64_t)(uintptr_t)items[i].b,
+                           (uint64_t)(uintptr_t)items[i].c,
+                           (uint64_t)(uintptr_t)items[i].d,
+                           (uint64_t)plans[i]->kernel_pin,
+                           ((uint64_t)plans[i]->scheme << 8) | (uint64_t)plans[i]->ozaki_slices};
     for (uint64_t v : f) key = mix(key, v);
     double sc[4] = {alpha[i].re, alpha[i].im, beta[i].re, beta[i].im};
     uint64_t bits[4];
@@ -634,13 +677,33 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
   }
   const size_t items_bytes = host_items.size() * sizeof(dev::GroupItem);
   const size_t starts_bytes = host_starts.size() * sizeof(int64_t);
-  check_cuda(cudaMalloc(&gr.buf, items_bytes + starts_bytes + 256 * (launches.size() + 1)), "cudaMalloc(groups)");
+  check_cuda(cudaMalloc(&gr.buf, align_up(items_bytes, 256) + align_up(starts_bytes, 256) + 256 * (launches.size() + 1)),
+             "cudaMalloc(groups)");
   char* base = static_cast<char*>(gr.buf);
-  check_cuda(cudaMemcpy(base, host_items.data(), items_bytes, cudaMemcpyHostToDevice), "group descriptors");
+  // Stream-ordered copies, complete before the capture (see Product::scatters).
   char* starts = base + align_up(items_bytes, 256);
-  check_cuda(cudaMemcpy(starts, host_starts.data(), starts_bytes, cudaMemcpyHostToDevice), "group tile starts");
+  cudaError_t up = cudaMemcpyAsync(base, host_items.data(), items_bytes, cudaMemcpyHostToDevice, ex.stream);
+  if (up == cudaSuccess)
+    up = cudaMemcpyAsync(starts, host_starts.data(), starts_bytes, cudaMemcpyHostToDevice, ex.stream);
+  if (up == cudaSuccess) up = cudaStreamSynchronize(ex.stream);
+  if (up != cudaSuccess) {
+    cudaFree(gr.buf);
+    check_cuda(up, "group descriptor upload");
+  }
   char* counters = starts + align_up(starts_bytes, 256);
-  check_cuda(cudaStreamBeginCapture(ex.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  for (auto& l : launches) {
+    const cudaError_t e = dev::prepare_grouped(l.first);
+    if (e != cudaSuccess) {
+      cudaFree(gr.buf);
+      check_cuda(e, "grouped kernel load");
+    }
+  }
+  // Capture on a private non-blocking stream (a capture on a stream that
+  // synchronises with the legacy stream would make other threads' legacy-stream
+  // work fail meanwhile); the graph is launched on the executor's stream.
+  if (!ex.capture_stream)
+    check_cuda(cudaStreamCreateWithFlags(&ex.capture_stream, cudaStreamNonBlocking), "cudaStreamCreate(capture)");
+  check_cuda(cudaStreamBeginCapture(ex.capture_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   cudaError_t cap = cudaSuccess;
   for (size_t l = 0; l < launches.size() && cap == cudaSuccess; ++l) {
     const int family = launches[l].first;
@@ -648,10 +711,11 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
     const int count = (int)((l + 1 < launches.size() ? launches[l + 1].second.first : host_items.size()) - item0);
     cap = dev::launch_grouped(family, reinterpret_cast<dev::GroupItem*>(base) + item0,
                               reinterpret_cast<int64_t*>(starts) + start0, count,
-                              reinterpret_cast<unsigned long long*>(counters + 256 * l), ex.num_sms, ex.stream);
+                              reinterpret_cast<unsigned long long*>(counters + 256 * l), ex.status, ex.num_sms,
+                              ex.capture_stream);
   }
   cudaGraph_t graph = nullptr;
-  cudaError_t end = cudaStreamEndCapture(ex.stream, &graph);
+  cudaError_t end = cudaStreamEndCapture(ex.capture_stream, &graph);
   if (cap != cudaSuccess || end != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
     cudaFree(gr.buf);
@@ -669,7 +733,7 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
     auto victim = ex.graphs.begin();
     for (auto it = ex.graphs.begin(); it != ex.graphs.end(); ++it)
       if (it->second.last_use < victim->second.last_use) victim = it;
-    check_cuda(cudaStreamSynchronize(ex.stream), "cudaStreamSynchronize");
+    drain(ex);
     cudaGraphExecDestroy(victim->second.exec);
     cudaFree(victim->second.buf);
     ex.graphs.erase(victim);

@@ -50,9 +50,12 @@ struct Executor {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t capture_stream = nullptr;  // grouped-graph captures only
   bool sync = true;
   bool profile = false;
   bool grouping = true;
+  size_t ws_limit = SIZE_MAX;  // cap of the workspace arena (allocation-failure injection)
+  int drain_limit_s = 300;     // bound of one wait for the stream to drain
   KernelTimes times;
   size_t pool_size = 0, budget = 1;  // recorded for the pooled-executor extension
   void* ws = nullptr;
@@ -89,6 +92,9 @@ struct Product {
   Scheme scheme = Scheme::Plain;
   int ozaki_slices = 0;
   int kernel_pin = 0;
+  // Unique over the process lifetime (never reused, unlike the address), so a
+  // cached grouped graph can never be replayed for a newer plan.
+  const uint64_t uid;
   std::mutex mu;
   std::map<int, DeviceScatters> dev;  // per device
   // Adjoint contractions of Plan::vjp, built on first use.
@@ -96,7 +102,9 @@ struct Product {
 
   explicit Product(const Problem& p);
   ~Product();
-  const dev::Scatters& scatters(int device);
+  // Device copy of the 12 scatter vectors, uploaded on first use on `stream`
+  // (which this call then drains once).
+  const dev::Scatters& scatters(int device, cudaStream_t stream);
   std::string report() const;
 };
 
@@ -132,8 +140,9 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
 void execute_vjp(Product& p, Executor& ex, Scalar alpha, const void* A, const void* B, const void* dD, void* dA,
                  void* dB);
 
-// Drain the stream and turn a non-zero device status word into an error.
+// Drain the stream (bounded) and turn a non-zero device status word into an error.
 void finish(Executor& ex);
+void drain(Executor& ex);
 
 // JSON of the executor's per-kernel totals ({"name": {"ms": .., "launches": ..}}).
 std::string kernel_times_json(Executor& ex, bool reset);

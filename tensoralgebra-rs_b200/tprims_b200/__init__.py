@@ -67,7 +67,8 @@ ABI_SYMBOLS = [
     "tprims_b200_product_set_tile", "tprims_b200_product_report", "tprims_b200_product_from_dot_general",
     "tprims_b200_execute_product_dlpack", "tprims_b200_contract_batched", "tprims_b200_product_vjp",
     "tprims_b200_product_scatter", "tprims_b200_executor_set_profiling", "tprims_b200_executor_kernel_times",
-    "tprims_b200_executor_set_grouping",
+    "tprims_b200_executor_set_grouping", "tprims_b200_executor_set_workspace_limit",
+    "tprims_b200_executor_selftest_wait", "tprims_b200_executor_probe_peak",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -98,6 +99,9 @@ lib.tprims_b200_executor_set_sync.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_synchronize.argtypes = [_ip]
 lib.tprims_b200_executor_set_profiling.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_set_grouping.argtypes = [_ip, C.c_int]
+lib.tprims_b200_executor_set_workspace_limit.argtypes = [_ip, C.c_size_t]
+lib.tprims_b200_executor_selftest_wait.argtypes = [_ip, C.c_uint64]
+lib.tprims_b200_executor_probe_peak.argtypes = [_ip, C.c_int, C.POINTER(C.c_double)]
 lib.tprims_b200_executor_kernel_times.argtypes = [_ip, C.c_char_p, C.c_size_t, C.c_int]
 lib.tprims_b200_executor_kernel_times.restype = C.c_size_t
 lib.tprims_tapp_executor_create_rayon.argtypes = [C.POINTER(_ip), C.c_size_t, _vp]
@@ -275,6 +279,20 @@ class Executor:
     def set_grouping(self, on: bool):
         """Grouped persistent launches (cached in CUDA graphs) for lists; off = one launch per item."""
         check(lib.tprims_b200_executor_set_grouping(self.h, 1 if on else 0))
+
+    def set_workspace_limit(self, nbytes: int):
+        """Cap the workspace arena (0 = no cap); larger requests are refused."""
+        check(lib.tprims_b200_executor_set_workspace_limit(self.h, int(nbytes)))
+
+    def selftest_wait(self, limit_ns: int) -> int:
+        """Run the bounded-wait self-test kernel; returns the status it produced."""
+        return lib.tprims_b200_executor_selftest_wait(self.h, int(limit_ns))
+
+    def probe_peak(self, which: int) -> float:
+        """Measured TFLOP/s of the FP64 DMMA (0) or FP32 FFMA (1) pipe on this device."""
+        v = C.c_double(0)
+        check(lib.tprims_b200_executor_probe_peak(self.h, int(which), C.byref(v)))
+        return v.value
 
     def set_profiling(self, on: bool):
         """Record CUDA events around every kernel launch on this executor."""

@@ -39,6 +39,7 @@ def test_grouped_list_matches_per_item_and_the_full_contraction(tp, torch_cuda, 
                 tp.OperandSpec(tp.LayoutSpec.col_major([ext[l] for l in ld])), la, lb, ld)
             lists[si].append(tp.Item(tp.Plan(prob), 1.0, t[xa].data_ptr(), t[xb].data_ptr(), t[xd].data_ptr()))
     prepared = [tp.PreparedBatch(l) for l in lists]
+    torch.cuda.synchronize()  # the inputs are written on torch's stream
 
     def run(grouping):
         ex.set_grouping(grouping)

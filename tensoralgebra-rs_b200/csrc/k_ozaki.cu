@@ -171,6 +171,95 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
   }
 }
 
+// Batch-innermost operands (the batch index has the smallest stride, as in a
+// [batch, k, row] tensor stored batch-first): the same scan and slicing with
+// the 32 lanes of a warp on 32 consecutive batch entries, so each warp load
+// is one contiguous run. Exponent scan: one thread per (batch entry, row),
+// looping over k; 32 batch entries x 8 rows per CTA.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
+                                                              const int64_t* k_scat, const int64_t* h_scat,
+                                                              int64_t nrows, int64_t K, int64_t rows_pad, int64_t H,
+                                                              int* __restrict__ out) {
+  const int hl = threadIdx.x & 31, rl = threadIdx.x >> 5;
+  const int64_t h = (int64_t)blockIdx.y * 32 + hl;
+  const int64_t r = (int64_t)blockIdx.x * 8 + rl;
+  if (r >= rows_pad || h >= H) return;
+  unsigned long long best = 0ull;
+  if (r < nrows) {
+    const double* base = X + (CPLX ? 2 : 1) * (h_scat[h] + rows_scat[r]);
+    for (int64_t k = 0; k < K; ++k) {
+      const double* e = base + (CPLX ? 2 : 1) * __ldg(k_scat + k);
+      double m = fabs(e[0]);
+      if (CPLX) m = fmax(m, fabs(e[1]));
+      if (!(m <= 1.79769313486231570e308)) m = __longlong_as_double(0x7ff0000000000000ll);  // inf or NaN
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+      if (bits > best) best = bits;
+    }
+  }
+  int e = 0;
+  if (best >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
+  else if (best != 0ull) frexp(__longlong_as_double((long long)best), &e);
+  out[h * rows_pad + r] = e;
+}
+
+// Slicing of one embedded row across 32 batch entries x 64 k: loads run along
+// the batch index, the K-major plane rows are written 4 bytes per thread.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
+                                                                const int64_t* k_scat, const int64_t* h_scat,
+                                                                const int* __restrict__ exps, int64_t nrows_emb,
+                                                                int64_t K, int64_t K_emb, int64_t rows_pad,
+                                                                int64_t exp_pad, int64_t k_pad, int64_t H, int which,
+                                                                int conj, int S, int8_t* __restrict__ out) {
+  __shared__ double tile[32][65];
+  const int tid = threadIdx.x;
+  const int64_t k0 = (int64_t)blockIdx.x * 64, r = blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
+  {
+    const int hl = tid & 31;
+    const int64_t h = h0 + hl;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int kk = (tid >> 5) + 8 * j;
+      const int64_t k = k0 + kk;
+      double v = 0.0;
+      if (h < H && r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, h_scat[h], r, k, K, which, conj);
+      tile[hl][kk] = v;
+    }
+  }
+  __syncthreads();
+  const int64_t plane = H * rows_pad * k_pad;
+  const int64_t er = (CPLX && which == 0) ? (r >> 1) : r;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int p = tid + 256 * j;
+    const int hl = p / 16, kq = (p % 16) * 4;
+    const int64_t h = h0 + hl;
+    if (h >= H) continue;
+    const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
+    double x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : ldexp(tile[hl][kq + q], -e);
+    int8_t* o = out + (h * rows_pad + r) * k_pad + k0 + kq;
+    for (int s = 0; s < S; ++s) {
+      char4 c;
+      signed char qv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        x[q] *= 128.0;
+        const double t = trunc(x[q]);
+        x[q] -= t;
+        qv[q] = (signed char)(int)t;
+      }
+      c.x = qv[0];
+      c.y = qv[1];
+      c.z = qv[2];
+      c.w = qv[3];
+      *reinterpret_cast<char4*>(o + s * plane) = c;
+    }
+  }
+}
+
 template <int S>
 struct OzCfg {
   static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A plane tile
@@ -179,15 +268,21 @@ struct OzCfg {
   static constexpr int STAGES = (S <= 6) ? 3 : 2;
   static constexpr int RING = STAGES * STAGE;
   static constexpr int SCAT = 2 * OZ_BN * 8 + OZ_BN * 4;  // d_n, c_n, column exponents
-  static constexpr int BAR = (2 * STAGES + 1) * 8 + 16;
+  static constexpr int BAR = (2 * STAGES + 2) * 8 + 16;
   static constexpr int SMEM = 1024 + RING + SCAT + BAR;
   static constexpr int TMEM_COLS = (S * OZ_BN <= 256) ? 256 : 512;
   static_assert(S * OZ_BN <= 512, "one INT32 accumulator per diagonal must fit in TMEM");
 };
 
-// One CTA per 128 x 64 tile of the embedded product over k-blocks
-// [kb0, kb1). Warp 0: TMA producer; warp 1: TMEM owner and MMA issuer;
-// warps 2-5: epilogue (TMEM lanes = tile rows).
+// Persistent: one CTA per SM walks the 128 x 64 tiles of the embedded product
+// (tile = blockIdx.x, blockIdx.x + gridDim.x, ...; n fastest, then m, then
+// batch), each over k-blocks [kb0, kb1). Warp 0: TMA producer, running ahead
+// across tile boundaries through the stage ring; warp 1: TMEM owner and MMA
+// issuer; warps 2-5: epilogue (TMEM lanes = tile rows). The epilogue drains
+// the S diagonal accumulators of a tile into FP64 registers, hands TMEM back
+// (tmem_empty) and then scales and stores while the MMAs of the next tile run.
+// Every mbarrier wait is bounded; a timeout sets STATUS_WAIT_TIMEOUT and the
+// role stops, so the kernel always ends.
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(192, 1)
 ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
@@ -197,18 +292,16 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* ring = smem;
-  int64_t* dn_s = reinterpret_cast<int64_t*>(smem + Cfg::RING);
-  int64_t* cn_s = dn_s + OZ_BN;
-  int* en_s = reinterpret_cast<int*>(cn_s + OZ_BN);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING + Cfg::SCAT);
   uint64_t* empty = full + Cfg::STAGES;
   uint64_t* accf = empty + Cfg::STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* tmem_empty = accf + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tmem_empty + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t h = blockIdx.z;
-  const int64_t m0 = (int64_t)blockIdx.y * OZ_BM, n0 = (int64_t)blockIdx.x * OZ_BN;
   const int nk = kb1 - kb0;
+  const int64_t tiles_n = n_pad / OZ_BN, tiles_m = m_pad / OZ_BM;
+  const int64_t ntiles = tiles_n * tiles_m * g.H;
 
   if (warp == 0 && lane == 0) {
     for (int i = 0; i < Cfg::STAGES; ++i) {
@@ -216,6 +309,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
       mbar_init(&empty[i], 1);
     }
     mbar_init(accf, 1);
+    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
     fence_barrier_init();
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
@@ -224,15 +318,6 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
     tmem_relinquish();
   }
-  if (warp >= 2) {
-    for (int i = tid - 64; i < OZ_BN; i += 128) {
-      const int64_t n = n0 + i;
-      const bool ok = n < g.N;
-      dn_s[i] = ok ? g.s.d_n[n] : 0;
-      cn_s[i] = ok ? g.s.c_n[n] : 0;
-      en_s[i] = exp_b[h * n_pad + n0 + i];
-    }
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -240,93 +325,127 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int i = 0; i < nk; ++i) {
-        const int st = i % Cfg::STAGES;
-        const uint32_t round = (uint32_t)(i / Cfg::STAGES);
-        if (!mbar_wait(&empty[st], (round & 1u) ^ 1u)) {
-          atomicOr(g.status, STATUS_WAIT_TIMEOUT);
-          break;
+      uint32_t it = 0;
+      bool alive = true;
+      for (int64_t tile = blockIdx.x; alive && tile < ntiles; tile += gridDim.x) {
+        const int64_t nt = tile % tiles_n, mt = (tile / tiles_n) % tiles_m, h = tile / (tiles_n * tiles_m);
+        for (int i = 0; i < nk; ++i, ++it) {
+          const int st = (int)(it % Cfg::STAGES);
+          const uint32_t round = it / Cfg::STAGES;
+          if (!mbar_wait(&empty[st], (round & 1u) ^ 1u)) {
+            atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+            alive = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
+          uint8_t* sbase = ring + st * Cfg::STAGE;
+          const int kx = (kb0 + i) * OZ_BK;
+#pragma unroll
+          for (int p = 0; p < S; ++p)
+            tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + mt * OZ_BM));
+#pragma unroll
+          for (int p = 0; p < S; ++p)
+            tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kx,
+                        (int)((p * g.H + h) * n_pad + nt * OZ_BN));
         }
-        mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
-        uint8_t* sbase = ring + st * Cfg::STAGE;
-        const int kx = (kb0 + i) * OZ_BK;
-#pragma unroll
-        for (int p = 0; p < S; ++p)
-          tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + m0));
-#pragma unroll
-        for (int p = 0; p < S; ++p)
-          tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kx, (int)((p * g.H + h) * n_pad + n0));
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t IDESC = idesc_i8(OZ_BM, OZ_BN);
-      for (int i = 0; i < nk; ++i) {
-        const int st = i % Cfg::STAGES;
-        const uint32_t round = (uint32_t)(i / Cfg::STAGES);
-        if (!mbar_wait(&full[st], round & 1u)) {
+      uint32_t it = 0, j = 0;
+      bool alive = true;
+      for (int64_t tile = blockIdx.x; alive && tile < ntiles; tile += gridDim.x, ++j) {
+        // The epilogue must have drained the previous tile's accumulators.
+        if (!mbar_wait(tmem_empty, (j & 1u) ^ 1u)) {
           atomicOr(g.status, STATUS_WAIT_TIMEOUT);
           break;
         }
         tc_fence_after();
-        const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
-#pragma unroll
-        for (int gd = 0; gd < S; ++gd) {
-#pragma unroll
-          for (int t = 0; t <= gd; ++t) {
-            const int u = gd - t;
-            const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
-            const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u * Cfg::B_TILE);
-#pragma unroll
-            for (int kk = 0; kk < OZ_BK / 32; ++kk)
-              umma_i8(tmem + (uint32_t)(gd * OZ_BN), ad + 2 * kk, bd + 2 * kk, IDESC,
-                      (i | t | kk) != 0 ? 1u : 0u);
+        for (int i = 0; i < nk; ++i, ++it) {
+          const int st = (int)(it % Cfg::STAGES);
+          const uint32_t round = it / Cfg::STAGES;
+          if (!mbar_wait(&full[st], round & 1u)) {
+            atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+            alive = false;
+            break;
           }
+          tc_fence_after();
+          const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+#pragma unroll
+          for (int gd = 0; gd < S; ++gd) {
+#pragma unroll
+            for (int t = 0; t <= gd; ++t) {
+              const int u = gd - t;
+              const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
+              const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u * Cfg::B_TILE);
+#pragma unroll
+              for (int kk = 0; kk < OZ_BK / 32; ++kk)
+                umma_i8(tmem + (uint32_t)(gd * OZ_BN), ad + 2 * kk, bd + 2 * kk, IDESC,
+                        (i | t | kk) != 0 ? 1u : 0u);
+            }
+          }
+          umma_commit(&empty[st]);
         }
-        umma_commit(&empty[st]);
+        if (alive) umma_commit(accf);
       }
-      umma_commit(accf);
     }
   } else {
-    const bool ok = mbar_wait(accf, 0);
-    if (!ok) atomicOr(g.status, STATUS_WAIT_TIMEOUT);
-    tc_fence_after();
     const int lane_base = 32 * (warp & 3);
     const uint32_t lane_addr = (uint32_t)lane_base << 16;
-    const int64_t me = m0 + lane_base + lane;  // row of the embedded product
-    const int64_t m = CPLX ? (me >> 1) : me;   // output row
-    const bool row_ok = ok && me < m_emb;
-    const int em = row_ok ? exp_a[h * exp_a_pad + m] : 0;
-    const int64_t dm = row_ok ? g.s.d_m[m] : 0;
-    const int64_t cm = (row_ok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
     using T = typename Elem<double, CPLX>::type;
-    const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]) + cm;
-    T* Db = static_cast<T*>(g.D) + g.s.h_d[h] + dm;
-#pragma unroll 1
-    for (int c = 0; c < OZ_BN / 16; ++c) {
-      double v[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = 0.0;
-#pragma unroll
-      for (int gd = S - 1; gd >= 0; --gd) {
-        uint32_t r[16];
-        tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + c * 16), r);
-        tmem_ld_wait();
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] += ldexp((double)(int)r[j], -7 * (gd + 2));
+    uint32_t j = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
+      const int64_t nt = tile % tiles_n, mt = (tile / tiles_n) % tiles_m, h = tile / (tiles_n * tiles_m);
+      const int64_t n0 = nt * OZ_BN;
+      if (!mbar_wait(accf, j & 1u)) {
+        atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+        break;
       }
+      tc_fence_after();
+      // Drain: the S diagonals, smallest weight first, into FP64 (each term
+      // is an exact power-of-two multiple of an INT32).
+      double v[OZ_BN];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int nn = c * 16 + j;
-        const int en = en_s[nn];
-        double x = (em == EXP_NONFINITE || en == EXP_NONFINITE) ? __longlong_as_double(0x7ff8000000000000ll)
-                                                                 : ldexp(v[j], em + en);
+      for (int c = 0; c < OZ_BN / 16; ++c) {
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) v[c * 16 + jj] = 0.0;
+#pragma unroll
+        for (int gd = S - 1; gd >= 0; --gd) {
+          uint32_t r[16];
+          tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + c * 16), r);
+          tmem_ld_wait();
+          const double w = ldexp(1.0, -7 * (gd + 2));
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) v[c * 16 + jj] += (double)(int)r[jj] * w;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_empty);
+
+      const int64_t me = mt * OZ_BM + lane_base + lane;  // row of the embedded product
+      const int64_t m = CPLX ? (me >> 1) : me;            // output row
+      const bool row_ok = me < m_emb;
+      const int em = row_ok ? __ldg(exp_a + h * exp_a_pad + m) : 0;
+      const int64_t dm = row_ok ? __ldg(g.s.d_m + m) : 0;
+      const int64_t cm = (row_ok && !g.e.beta_zero) ? __ldg(g.s.c_m + m) : 0;
+      const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : __ldg(g.s.h_c + h)) + cm;
+      T* Db = static_cast<T*>(g.D) + __ldg(g.s.h_d + h) + dm;
+#pragma unroll
+      for (int nn = 0; nn < OZ_BN; ++nn) {
+        const int64_t n = n0 + nn;
+        const bool col_ok = n < g.N;
+        const int en = __ldg(exp_b + h * n_pad + n);
+        const double x = (em == EXP_NONFINITE || en == EXP_NONFINITE) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                       : ldexp(v[nn], em + en);
+        const int64_t dn = col_ok ? __ldg(g.s.d_n + n) : 0;
+        const int64_t cn = (col_ok && !g.e.beta_zero) ? __ldg(g.s.c_n + n) : 0;
         if constexpr (CPLX) {
           const double other = __shfl_xor_sync(0xffffffffu, x, 1);
-          if (row_ok && (lane & 1) == 0 && n0 + nn < g.N)
-            epilogue_store<double, true>(g.e, x, other, Cb + cn_s[nn], Db + dn_s[nn]);
+          if (row_ok && (lane & 1) == 0 && col_ok) epilogue_store<double, true>(g.e, x, other, Cb + cn, Db + dn);
         } else {
-          if (row_ok && n0 + nn < g.N) epilogue_store<double, false>(g.e, x, 0.0, Cb + cn_s[nn], Db + dn_s[nn]);
+          if (row_ok && col_ok) epilogue_store<double, false>(g.e, x, 0.0, Cb + cn, Db + dn);
         }
       }
     }
@@ -352,7 +471,10 @@ cudaError_t run_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ap, co
   cudaError_t e =
       cudaFuncSetAttribute(ozaki_gemm_kernel<S, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)(L.n_pad / OZ_BN), (unsigned)(L.m_pad / OZ_BM), (unsigned)L.H);
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t ntiles = (L.n_pad / OZ_BN) * (L.m_pad / OZ_BM) * L.H;
+  const unsigned grid = (unsigned)(ntiles < sms ? ntiles : sms);
   ozaki_gemm_kernel<S, CPLX><<<grid, 192, Cfg::SMEM, st>>>(ma, mb, g, ea, eb, L.m_emb, L.m_pad, L.n_pad, L.exp_a_pad,
                                                            kb0, kb1);
   return cudaGetLastError();
@@ -398,6 +520,28 @@ size_t ozaki_workspace_bytes(const OzakiLayout& L) {
   return pa + pb + ex + 4 * 256;
 }
 
+// Exponent scan + slicing of one operand (rows = M for A', N for B'), with the
+// batch-innermost variants when the batch index has the smallest stride.
+template <bool CPLX>
+static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* k_s, const int64_t* h_s, int64_t nrows,
+                         int64_t nrows_emb, int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
+                         int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
+  if (hfast) {
+    ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)((exp_pad + 7) / 8), (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
+        X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);
+    ozaki_slice_hfast_kernel<CPLX>
+        <<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
+            X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, rows_pad, exp_pad, L.k_pad, L.H, which, conj, L.slices,
+            planes);
+  } else {
+    ozaki_exp_kernel<CPLX><<<dim3((unsigned)((nrows + 31) / 32), (unsigned)L.H), 256, 0, st>>>(
+        X, rows_s, k_s, h_s, nrows, K, exp_pad, kfast, exps);
+    ozaki_slice_kernel<CPLX><<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
+        X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, rows_pad, exp_pad, L.k_pad, L.H, kfast, which, conj,
+        L.slices, planes);
+  }
+}
+
 cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st) {
   int8_t* ap = static_cast<int8_t*>(ws);
   int8_t* bp = ap + (size_t)L.slices * L.H * L.m_pad * L.k_pad;
@@ -407,31 +551,16 @@ cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws,
   const double* A = static_cast<const double*>(g.A);
   const double* B = static_cast<const double*>(g.B);
   // Row exponents of A (per complex row) and column exponents of B.
-  {
-    dim3 ga((unsigned)((g.M + 31) / 32), (unsigned)L.H);
-    dim3 gb((unsigned)((g.N + 31) / 32), (unsigned)L.H);
-    if (L.cplx) {
-      ozaki_exp_kernel<true><<<ga, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L.exp_a_pad, g.a_kfast, ea);
-      ozaki_exp_kernel<true><<<gb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L.n_pad, g.b_kfast, eb);
-    } else {
-      ozaki_exp_kernel<false><<<ga, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L.exp_a_pad, g.a_kfast, ea);
-      ozaki_exp_kernel<false><<<gb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L.n_pad, g.b_kfast, eb);
-    }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
-  dim3 sa((unsigned)(L.k_pad / 64), (unsigned)(L.m_pad / 32), (unsigned)L.H);
-  dim3 sb((unsigned)(L.k_pad / 64), (unsigned)(L.n_pad / 32), (unsigned)L.H);
   if (L.cplx) {
-    ozaki_slice_kernel<true><<<sa, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, ea, L.m_emb, g.K, L.k_emb, L.m_pad,
-                                                  L.exp_a_pad, L.k_pad, L.H, g.a_kfast, 0, g.conj_a, L.slices, ap);
-    ozaki_slice_kernel<true><<<sb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, eb, g.N, g.K, L.k_emb, L.n_pad, L.n_pad,
-                                                  L.k_pad, L.H, g.b_kfast, 1, g.conj_b, L.slices, bp);
+    pack_operand<true>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, L.m_emb, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast, L.a_hfast,
+                       0, g.conj_a, ea, ap, st);
+    pack_operand<true>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1,
+                       g.conj_b, eb, bp, st);
   } else {
-    ozaki_slice_kernel<false><<<sa, 256, 0, st>>>(A, g.s.a_m, g.s.a_k, g.s.h_a, ea, L.m_emb, g.K, L.k_emb, L.m_pad,
-                                                   L.exp_a_pad, L.k_pad, L.H, g.a_kfast, 0, 0, L.slices, ap);
-    ozaki_slice_kernel<false><<<sb, 256, 0, st>>>(B, g.s.b_n, g.s.b_k, g.s.h_b, eb, g.N, g.K, L.k_emb, L.n_pad,
-                                                   L.n_pad, L.k_pad, L.H, g.b_kfast, 1, 0, L.slices, bp);
+    pack_operand<false>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, L.m_emb, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast,
+                        L.a_hfast, 0, 0, ea, ap, st);
+    pack_operand<false>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1, 0,
+                        eb, bp, st);
   }
   return cudaGetLastError();
 }

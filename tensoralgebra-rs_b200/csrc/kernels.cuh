@@ -120,6 +120,7 @@ struct OzakiLayout {
   int64_t exp_a_pad;  // row stride of the A exponent array
   int64_t H;
   int kb_chunk;    // k-blocks per launch that keep INT32 accumulation exact
+  int a_hfast = 0, b_hfast = 0;  // batch index has the smallest stride: batch-innermost packing
 };
 OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K, int64_t H);
 size_t ozaki_workspace_bytes(const OzakiLayout& L);

@@ -372,8 +372,14 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
       return;
     }
     case Scheme::OzakiInt8: {
-      const dev::OzakiLayout L =
-          dev::ozaki_layout(pr.ozaki_slices, dtype_complex(pr.problem.dtype), g.M, g.N, g.K, g.H);
+      dev::OzakiLayout L = dev::ozaki_layout(pr.ozaki_slices, dtype_complex(pr.problem.dtype), g.M, g.N, g.K, g.H);
+      // Batch-innermost packing when the batch index has the smallest stride.
+      const auto step = [](const std::vector<int64_t>& x) {
+        return x.size() > 1 ? std::llabs(x[1] - x[0]) : (long long)INT64_MAX;
+      };
+      const OrientedView& v = pr.view;
+      L.a_hfast = (v.H >= 32 && L.m_pad <= 65535 && step(v.h_a) < std::min(step(v.a_m), step(v.a_k))) ? 1 : 0;
+      L.b_hfast = (v.H >= 32 && L.n_pad <= 65535 && step(v.h_b) < std::min(step(v.b_n), step(v.b_k))) ? 1 : 0;
       if (dev::ozaki_workspace_bytes(L) > scratch_bytes) throw Error(ERR_INTERNAL, "Ozaki workspace too small");
       char* ws = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
       {

@@ -26,15 +26,6 @@ def ex(tp, torch_cuda):
     e.close()
 
 
-def run_oz(tp, ex, torch, dt, A, B, C, D, alpha, beta, slices=0, device=True):
-    p = make_product(tp, dt, A, B, C, D)
-    p.set_precision(OZ, slices)
-    rep = p.report()
-    assert rep["scheme"] == "ozaki-int8"
-    st, got, _ = run(tp, ex, torch, dt, A, B, C, D, alpha, beta, device=device, precision=0, kernel=0)
-    return p, got
-
-
 def _run_prepared(tp, ex, torch, p, A, B, C, D, alpha, beta):
     tens = {}
 
@@ -60,7 +51,9 @@ def oz(tp, ex, torch, dt, A, B, C, D, alpha, beta, slices=0):
 @pytest.mark.parametrize("dt", ["float64", "complex128"])
 def test_ozaki_ragged_batched_general_strides(tp, ex, torch_cuda, orc, dt):
     rng = np.random.default_rng(41)
-    for (m, n, k, h) in [(1, 1, 1, 1), (7, 13, 5, 1), (130, 257, 70, 1), (65, 33, 129, 3)]:
+    # h = 40: batch index innermost with at least 32 entries (the batch-innermost
+    # packing), not a multiple of 32.
+    for (m, n, k, h) in [(1, 1, 1, 1), (7, 13, 5, 1), (130, 257, 70, 1), (65, 33, 129, 3), (70, 45, 100, 40)]:
         A = Op(rnd(rng, dt, h * m * k), [h, k, m], [1, h, h * k], [9, 2, 0])  # k before m
         B = Op(rnd(rng, dt, h * k * n), [h, n, k], [1, h * k, h], [9, 1, 2])
         C = Op(rnd(rng, dt, h * m * n), [h, m, n], [1, h, h * m], [9, 0, 1])
@@ -144,3 +137,19 @@ def test_ozaki_non_finite_rows_give_nan(tp, ex, torch_cuda, orc):
     got, _ = oz(tp, ex, torch_cuda, "float64", A, B, None, D, 1.0, 0.0)
     G = got.reshape(5, 8).T
     assert np.all(np.isnan(G[3])) and np.all(np.isfinite(np.delete(G, 3, axis=0)))
+
+
+def test_ozaki_batch_innermost_conjugated_c3_layout(tp, ex, torch_cuda, orc):
+    """Config-3 layout at reduced size: D[b,i,j] = sum_k conj(A[b,k,i]) B[b,k,j],
+    c64, column-major in the listed order (batch stride 1 in every operand)."""
+    rng = np.random.default_rng(43)
+    dt, b, n = "complex128", 48, 96
+    ext = [b, n, n]
+    st = [1, b, b * n]
+    A = Op(rnd(rng, dt, b * n * n), ext, st, [0, 3, 1], conj=True)
+    B = Op(rnd(rng, dt, b * n * n), ext, st, [0, 3, 2])
+    d0 = np.zeros(b * n * n, dtype=dt)
+    D = Op(d0, ext, st, [0, 1, 2])
+    want = oracle_ref(orc, dt, A, B, None, D, 1.0, 0.0, d0)
+    got, p = oz(tp, ex, torch_cuda, dt, A, B, None, D, 1.0, 0.0)
+    assert orc.rel_frobenius(got, want) <= 1e-12, p.report()

@@ -295,6 +295,29 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_contract_batched(TAPP_executor exec, i
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_vjp(TAPP_tensor_product plan, TAPP_executor exec, const void* alpha,
                                                       const void* A, const void* B, const void* dD, void* dA, void* dB);
 
+/* Split-precision execution that allocates no device memory. No counterpart
+   in the reference. For callers that cannot call cudaMalloc: code running
+   inside a memory pool that another component owns (a framework's caching
+   allocator, a server that reserved the GPU's memory up front), or code that
+   must not let cudaMalloc / cudaFree synchronise the device. Same operands and
+   semantics as TAPP_execute_product, for an F32 plan set to
+   TPRIMS_PREC_BF16X3 or TPRIMS_PREC_BF16X6 (others: TPRIMS_ERR_UNSUPPORTED);
+   A, B, C and D must be in the current device's memory (else
+   TPRIMS_ERR_DEVICE). Runs on `stream` (a cudaStream_t as an integer; 0 = the
+   legacy default stream) of the current device and returns after that stream
+   has drained.
+   Its scratch is one fixed 64 MiB device array inside this library, held on
+   every GPU that loads the library until the process exits; a contraction
+   that needs more (about M = N = K = 2048 at bf16x6 fits) is refused with
+   TPRIMS_ERR_SHAPE before anything runs. The first call on a device looks
+   the array's address up (this may load the library's device code), so make
+   it before any stream capture on that device. All calls share the array:
+   calls that overlap on one GPU, from two streams or two threads, race on it
+   and give wrong results. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_execute_product_noalloc(TAPP_tensor_product plan, uintptr_t stream,
+                                                                  const void* alpha, const void* A, const void* B,
+                                                                  const void* beta, const void* C, void* D);
+
 #ifdef __cplusplus
 }
 #endif

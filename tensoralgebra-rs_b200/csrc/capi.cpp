@@ -771,3 +771,17 @@ extern "C" TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int wh
     *tflops = best;
   });
 }
+
+extern "C" TAPP_error tprims_b200_execute_product_noalloc(TAPP_tensor_product plan, uintptr_t stream,
+                                                         const void* alpha, const void* A, const void* B,
+                                                         const void* beta, const void* C, void* D) {
+  return ffi([&] {
+    Product& p = product_of(plan);
+    if (!alpha) null_arg("alpha");
+    if (!beta) null_arg("beta");
+    const Scalar al = read_scalar(p.problem.dtype, alpha), be = read_scalar(p.problem.dtype, beta);
+    const Item it{A, B, C, D};
+    validate_item(p, it, be.is_zero());
+    execute_split_noalloc(p, reinterpret_cast<cudaStream_t>(stream), al, be, it);
+  });
+}

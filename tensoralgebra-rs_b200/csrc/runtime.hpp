@@ -140,6 +140,10 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
 void execute_vjp(Product& p, Executor& ex, Scalar alpha, const void* A, const void* B, const void* dD, void* dA,
                  void* dB);
 
+// The split-precision path on the caller's stream with no device allocation:
+// scratch in a fixed device array (k_noalloc.cu). Synchronous on `stream`.
+void execute_split_noalloc(Product& p, cudaStream_t stream, Scalar alpha, Scalar beta, const Item& it);
+
 // Drain the stream (bounded) and turn a non-zero device status word into an error.
 void finish(Executor& ex);
 void drain(Executor& ex);

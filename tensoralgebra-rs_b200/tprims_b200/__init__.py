@@ -69,6 +69,7 @@ ABI_SYMBOLS = [
     "tprims_b200_product_scatter", "tprims_b200_executor_set_profiling", "tprims_b200_executor_kernel_times",
     "tprims_b200_executor_set_grouping", "tprims_b200_executor_set_workspace_limit",
     "tprims_b200_executor_selftest_wait", "tprims_b200_executor_probe_peak",
+    "tprims_b200_execute_product_noalloc",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -102,6 +103,7 @@ lib.tprims_b200_executor_set_grouping.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_set_workspace_limit.argtypes = [_ip, C.c_size_t]
 lib.tprims_b200_executor_selftest_wait.argtypes = [_ip, C.c_uint64]
 lib.tprims_b200_executor_probe_peak.argtypes = [_ip, C.c_int, C.POINTER(C.c_double)]
+lib.tprims_b200_execute_product_noalloc.argtypes = [_ip, C.c_size_t, _vp, _vp, _vp, _vp, _vp, _vp]
 lib.tprims_b200_executor_kernel_times.argtypes = [_ip, C.c_char_p, C.c_size_t, C.c_int]
 lib.tprims_b200_executor_kernel_times.restype = C.c_size_t
 lib.tprims_tapp_executor_create_rayon.argtypes = [C.POINTER(_ip), C.c_size_t, _vp]
@@ -391,6 +393,16 @@ class TensorProduct:
             self.h, exec_.h if exec_ else 0, C.byref(st) if status else None, al, ptr_of(a), ptr_of(b), be,
             ptr_of(c), ptr_of(d),
         )
+
+    def execute_noalloc(self, stream: int, alpha, a, b, beta, c, d) -> int:
+        """``tprims_b200_execute_product_noalloc``: the split-precision path with
+        its scratch in the library's fixed device array, for callers that cannot
+        allocate device memory. Device operands only; returns after ``stream``
+        has drained. Returns the status."""
+        al = scalar_bytes(self.dtype, alpha)
+        be = scalar_bytes(self.dtype, beta)
+        return lib.tprims_b200_execute_product_noalloc(self.h, int(stream), al, ptr_of(a), ptr_of(b), be,
+                                                       ptr_of(c), ptr_of(d))
 
     def execute_batched(self, exec_: Optional[Executor], alpha, As, Bs, beta, Cs, Ds) -> int:
         n = len(As)

@@ -327,7 +327,7 @@ def run_config(args, tp, torch, ex):
             p = product(tp.F64, specs)
             try:
                 if code:
-                    p.set_precision(code)
+                    p.set_precision(code, args.slices if code == 3 else 0)
             except tp.TprimsError as err:
                 out[scheme] = {"unavailable": err.message}
                 continue
@@ -356,7 +356,7 @@ def run_config(args, tp, torch, ex):
             p = product(tp.C64, specs, ops=(1, 0, 0, 0))
             try:
                 if code:
-                    p.set_precision(code)
+                    p.set_precision(code, args.slices if code == 3 else 0)
             except tp.TprimsError as err:
                 out[scheme] = {"unavailable": err.message}
                 continue
@@ -461,6 +461,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
+    ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5"],
                     help="c2 is the metric's workload; c1/c3/c5 print timing lines of the other configurations")
     args = ap.parse_args()
@@ -505,7 +506,7 @@ def main():
     for name, code in SCHEMES.items():
         p = tp.TensorProduct.create(h, (0, ia, LAB_A), (0, ib, LAB_B), (0, idd, LAB_D), (0, idd, LAB_D))
         if code:
-            p.set_precision(code)
+            p.set_precision(code, args.slices if code == 3 else 0)
         plans[name] = p
 
     def step(name):

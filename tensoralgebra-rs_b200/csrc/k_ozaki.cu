@@ -15,7 +15,8 @@
 //
 // Complex operands are embedded as one real problem of twice the rows and
 // twice the depth: A' row 2r = [Re A_r, -Im A_r], row 2r+1 = [Im A_r, Re A_r],
-// B' depth [Re B; Im B], so rows 2r and 2r+1 of the product are the real and
+// B' depth [Re B; Im B] (each depth half padded with zeros to a whole number
+// of 64-deep k-blocks), so rows 2r and 2r+1 of the product are the real and
 // imaginary parts of row r (the four real products of the planar method);
 // adjacent TMEM lanes hold them and the epilogue pairs them with a shuffle.
 //
@@ -44,24 +45,60 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
 }
 
 // One element of the (possibly complex-embedded) operand X' at (row, k).
-// which == 0: A' (rows = m); which == 1: B' (rows = n).
+// which == 0: A' (rows = m); which == 1: B' (rows = n). The complex depth is
+// two halves of Kh (K rounded up to a k-block): [0, K) real parts and
+// [Kh, Kh + K) imaginary parts, zero in between.
 template <bool CPLX>
 __device__ inline double embedded(const double* X, const int64_t* rows_scat, const int64_t* k_scat, int64_t hoff,
-                                  int64_t row, int64_t k, int64_t K, int which, int conj) {
+                                  int64_t row, int64_t k, int64_t K, int64_t Kh, int which, int conj) {
   if (!CPLX) return X[hoff + rows_scat[row] + k_scat[k]];
+  const bool second = k >= Kh;
+  const int64_t kk = second ? k - Kh : k;
+  if (kk >= K) return 0.0;
   if (which == 0) {
     const int64_t r = row >> 1;
-    const bool second = k >= K;
-    const int64_t kk = second ? k - K : k;
     const double* e = X + 2 * (hoff + rows_scat[r] + k_scat[kk]);
     const double re = e[0], im = conj ? -e[1] : e[1];
     if ((row & 1) == 0) return second ? -im : re;
     return second ? re : im;
   }
-  const bool second = k >= K;
-  const int64_t kk = second ? k - K : k;
   const double* e = X + 2 * (hoff + rows_scat[row] + k_scat[kk]);
   return second ? (conj ? -e[1] : e[1]) : e[0];
+}
+
+// The S signed 7-bit slices of four values of one row with exponent e
+// (|x| < 2^e), written as char4 into the S planes. T = trunc(x 2^(7S - e)) is
+// exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
+// of x, are the slices: the same digits as repeatedly multiplying the scaled
+// value by 128 and removing the integer part.
+__device__ inline void write_slices(const double (&x)[4], int e, int S, int8_t* o, int64_t plane) {
+  const int k = 7 * S - e;  // scale exponent; above 1023 only for rows below 2^-967
+  const bool two = k > 1023;
+  const double s1 = two ? ldexp(1.0, 1000) : ldexp(1.0, k);
+  const double s2 = two ? ldexp(1.0, k - 1000) : 1.0;
+  unsigned long long mag[4];
+  bool neg[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long t = (long long)((x[q] * s1) * s2);  // truncation toward zero
+    neg[q] = t < 0;
+    mag[q] = (unsigned long long)(neg[q] ? -t : t);
+  }
+  for (int sl = 0; sl < S; ++sl) {
+    const int sh = 7 * (S - 1 - sl);
+    signed char qv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int d = (int)((mag[q] >> sh) & 127ull);
+      qv[q] = (signed char)(neg[q] ? -d : d);
+    }
+    char4 c;
+    c.x = qv[0];
+    c.y = qv[1];
+    c.z = qv[2];
+    c.w = qv[3];
+    *reinterpret_cast<char4*>(o + sl * plane) = c;
+  }
 }
 
 // Per row (complex: per complex row) exponent e with max |x| < 2^e; a row with
@@ -117,7 +154,7 @@ template <bool CPLX>
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                           const int64_t* k_scat, const int64_t* h_scat,
                                                           const int* __restrict__ exps, int64_t nrows_emb,
-                                                          int64_t K, int64_t K_emb, int64_t rows_pad,
+                                                          int64_t K, int64_t K_emb, int64_t Kh, int64_t rows_pad,
                                                           int64_t exp_pad, int64_t k_pad, int64_t H, int kfast,
                                                           int which, int conj, int S, int8_t* __restrict__ out) {
   __shared__ double tile[32][65];
@@ -136,7 +173,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     }
     const int64_t r = r0 + rr, k = k0 + kk;
     double v = 0.0;
-    if (r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, hoff, r, k, K, which, conj);
+    if (r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, hoff, r, k, K, Kh, which, conj);
     tile[rr][kk] = v;
   }
   __syncthreads();
@@ -150,45 +187,30 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
     double x[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : ldexp(tile[rr][kq + q], -e);
-    int8_t* o = out + (h * rows_pad + r) * k_pad + k0 + kq;
-    for (int s = 0; s < S; ++s) {
-      char4 c;
-      signed char qv[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        x[q] *= 128.0;
-        const double t = trunc(x[q]);
-        x[q] -= t;
-        qv[q] = (signed char)(int)t;
-      }
-      c.x = qv[0];
-      c.y = qv[1];
-      c.z = qv[2];
-      c.w = qv[3];
-      *reinterpret_cast<char4*>(o + s * plane) = c;
-    }
+    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : tile[rr][kq + q];
+    write_slices(x, e, S, out + (h * rows_pad + r) * k_pad + k0 + kq, plane);
   }
 }
 
 // Batch-innermost operands (the batch index has the smallest stride, as in a
 // [batch, k, row] tensor stored batch-first): the same scan and slicing with
 // the 32 lanes of a warp on 32 consecutive batch entries, so each warp load
-// is one contiguous run. Exponent scan: one thread per (batch entry, row),
-// looping over k; 32 batch entries x 8 rows per CTA.
+// is one contiguous run.
 template <bool CPLX>
 __global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                               const int64_t* k_scat, const int64_t* h_scat,
                                                               int64_t nrows, int64_t K, int64_t rows_pad, int64_t H,
                                                               int* __restrict__ out) {
-  const int hl = threadIdx.x & 31, rl = threadIdx.x >> 5;
-  const int64_t h = (int64_t)blockIdx.y * 32 + hl;
-  const int64_t r = (int64_t)blockIdx.x * 8 + rl;
-  if (r >= rows_pad || h >= H) return;
+  // One CTA per (row, 32 batch entries); the 8 warps split k and combine in
+  // shared memory.
+  __shared__ unsigned long long red[8][32];
+  const int hl = threadIdx.x & 31, kp = threadIdx.x >> 5;
+  const int64_t r = blockIdx.x, h = (int64_t)blockIdx.y * 32 + hl;
   unsigned long long best = 0ull;
-  if (r < nrows) {
+  if (r < nrows && h < H) {
     const double* base = X + (CPLX ? 2 : 1) * (h_scat[h] + rows_scat[r]);
-    for (int64_t k = 0; k < K; ++k) {
+#pragma unroll 4
+    for (int64_t k = kp; k < K; k += 8) {
       const double* e = base + (CPLX ? 2 : 1) * __ldg(k_scat + k);
       double m = fabs(e[0]);
       if (CPLX) m = fmax(m, fabs(e[1]));
@@ -197,10 +219,16 @@ __global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __re
       if (bits > best) best = bits;
     }
   }
-  int e = 0;
-  if (best >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
-  else if (best != 0ull) frexp(__longlong_as_double((long long)best), &e);
-  out[h * rows_pad + r] = e;
+  red[kp][hl] = best;
+  __syncthreads();
+  if (kp == 0 && h < H && r < rows_pad) {
+#pragma unroll
+    for (int j = 1; j < 8; ++j) best = red[j][hl] > best ? red[j][hl] : best;
+    int e = 0;
+    if (best >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
+    else if (best != 0ull) frexp(__longlong_as_double((long long)best), &e);
+    out[h * rows_pad + r] = e;
+  }
 }
 
 // Slicing of one embedded row across 32 batch entries x 64 k: loads run along
@@ -209,7 +237,7 @@ template <bool CPLX>
 __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                                 const int64_t* k_scat, const int64_t* h_scat,
                                                                 const int* __restrict__ exps, int64_t nrows_emb,
-                                                                int64_t K, int64_t K_emb, int64_t rows_pad,
+                                                                int64_t K, int64_t K_emb, int64_t Kh, int64_t rows_pad,
                                                                 int64_t exp_pad, int64_t k_pad, int64_t H, int which,
                                                                 int conj, int S, int8_t* __restrict__ out) {
   __shared__ double tile[32][65];
@@ -223,7 +251,8 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __
       const int kk = (tid >> 5) + 8 * j;
       const int64_t k = k0 + kk;
       double v = 0.0;
-      if (h < H && r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, h_scat[h], r, k, K, which, conj);
+      if (h < H && r < nrows_emb && k < K_emb)
+        v = embedded<CPLX>(X, rows_scat, k_scat, h_scat[h], r, k, K, Kh, which, conj);
       tile[hl][kk] = v;
     }
   }
@@ -239,23 +268,67 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __
     const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
     double x[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : ldexp(tile[hl][kq + q], -e);
-    int8_t* o = out + (h * rows_pad + r) * k_pad + k0 + kq;
-    for (int s = 0; s < S; ++s) {
-      char4 c;
-      signed char qv[4];
+    for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : tile[hl][kq + q];
+    write_slices(x, e, S, out + (h * rows_pad + r) * k_pad + k0 + kq, plane);
+  }
+}
+
+// Complex batch-innermost slicing: one load of a complex element gives all of
+// its embedded values (A': rows 2r and 2r+1, both depth halves; B': row n,
+// both halves). One CTA per (complex row, 32 batch entries, 64 k).
+template <int WHICH>
+__global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
+    const double* __restrict__ X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
+    const int* __restrict__ exps, int64_t nrows, int64_t K, int64_t Kh, int64_t rows_pad, int64_t exp_pad,
+    int64_t k_pad, int64_t H, int conj, int S, int8_t* __restrict__ out) {
+  __shared__ double t_re[32][65], t_im[32][65];
+  const int tid = threadIdx.x;
+  const int64_t k0 = (int64_t)blockIdx.x * 64, r = blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
+  {
+    const int hl = tid & 31;
+    const int64_t h = h0 + hl;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        x[q] *= 128.0;
-        const double t = trunc(x[q]);
-        x[q] -= t;
-        qv[q] = (signed char)(int)t;
+    for (int j = 0; j < 8; ++j) {
+      const int kk = (tid >> 5) + 8 * j;
+      const int64_t k = k0 + kk;
+      double re = 0.0, im = 0.0;
+      if (h < H && r < nrows && k < K) {
+        const double* e = X + 2 * (h_scat[h] + rows_scat[r] + k_scat[k]);
+        re = e[0];
+        im = conj ? -e[1] : e[1];
       }
-      c.x = qv[0];
-      c.y = qv[1];
-      c.z = qv[2];
-      c.w = qv[3];
-      *reinterpret_cast<char4*>(o + s * plane) = c;
+      t_re[hl][kk] = re;
+      t_im[hl][kk] = im;
+    }
+  }
+  __syncthreads();
+  const int64_t plane = H * rows_pad * k_pad;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int p = tid + 256 * j;
+    const int hl = p / 16, kq = (p % 16) * 4;
+    const int64_t h = h0 + hl;
+    if (h >= H) continue;
+    const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
+    double re[4], im[4], nim[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool bad = e == EXP_NONFINITE;
+      re[q] = bad ? 0.0 : t_re[hl][kq + q];
+      im[q] = bad ? 0.0 : t_im[hl][kq + q];
+      nim[q] = -im[q];
+    }
+    if (WHICH == 0) {
+      int8_t* o0 = out + (h * rows_pad + 2 * r) * k_pad + k0 + kq;
+      int8_t* o1 = o0 + k_pad;
+      write_slices(re, e, S, o0, plane);
+      write_slices(nim, e, S, o0 + Kh, plane);
+      write_slices(im, e, S, o1, plane);
+      write_slices(re, e, S, o1 + Kh, plane);
+    } else {
+      int8_t* o0 = out + (h * rows_pad + r) * k_pad + k0 + kq;
+      write_slices(re, e, S, o0, plane);
+      write_slices(im, e, S, o0 + Kh, plane);
     }
   }
 }
@@ -278,13 +351,21 @@ struct OzCfg {
 // (tile = blockIdx.x, blockIdx.x + gridDim.x, ...; n fastest, then m, then
 // batch), each over k-blocks [kb0, kb1). Warp 0: TMA producer, running ahead
 // across tile boundaries through the stage ring; warp 1: TMEM owner and MMA
-// issuer; warps 2-5: epilogue (TMEM lanes = tile rows). The epilogue drains
-// the S diagonal accumulators of a tile into FP64 registers, hands TMEM back
-// (tmem_empty) and then scales and stores while the MMAs of the next tile run.
+// issuer; warps 2-9: epilogue, two warps per TMEM lane quarter (warp % 4),
+// one per 32-column half of the tile. The epilogue drains the S diagonal
+// accumulators of a tile into FP64 registers, hands TMEM back (tmem_empty) and
+// then scales and stores while the MMAs of the next tile run.
 // Every mbarrier wait is bounded; a timeout sets STATUS_WAIT_TIMEOUT and the
 // role stops, so the kernel always ends.
+constexpr int OZ_THREADS = 320;
+constexpr int OZ_EPI_WARPS = 8;
+constexpr int OZ_EPI_COLS = OZ_BN / 2;  // columns per epilogue warp
+
+// 2^e as a double for e in [-1022, 1023] (exact).
+__device__ inline double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
 template <int S, bool CPLX>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(OZ_THREADS, 1)
 ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
                   const int* __restrict__ exp_a, const int* __restrict__ exp_b, int64_t m_emb, int64_t m_pad,
                   int64_t n_pad, int64_t exp_a_pad, int kb0, int kb1) {
@@ -309,7 +390,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
       mbar_init(&empty[i], 1);
     }
     mbar_init(accf, 1);
-    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
+    mbar_init(tmem_empty, OZ_EPI_WARPS);  // one arrival per epilogue warp
     fence_barrier_init();
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
@@ -392,38 +473,20 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     }
   } else {
     const int lane_base = 32 * (warp & 3);
+    const int col0 = OZ_EPI_COLS * ((warp - 2) >> 2);  // this warp's column half
     const uint32_t lane_addr = (uint32_t)lane_base << 16;
     using T = typename Elem<double, CPLX>::type;
     uint32_t j = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
       const int64_t nt = tile % tiles_n, mt = (tile / tiles_n) % tiles_m, h = tile / (tiles_n * tiles_m);
-      const int64_t n0 = nt * OZ_BN;
-      if (!mbar_wait(accf, j & 1u)) {
-        atomicOr(g.status, STATUS_WAIT_TIMEOUT);
-        break;
-      }
-      tc_fence_after();
-      // Drain: the S diagonals, smallest weight first, into FP64 (each term
-      // is an exact power-of-two multiple of an INT32).
-      double v[OZ_BN];
-#pragma unroll
-      for (int c = 0; c < OZ_BN / 16; ++c) {
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) v[c * 16 + jj] = 0.0;
-#pragma unroll
-        for (int gd = S - 1; gd >= 0; --gd) {
-          uint32_t r[16];
-          tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + c * 16), r);
-          tmem_ld_wait();
-          const double w = ldexp(1.0, -7 * (gd + 2));
-#pragma unroll
-          for (int jj = 0; jj < 16; ++jj) v[c * 16 + jj] += (double)(int)r[jj] * w;
-        }
-      }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(tmem_empty);
-
+      const int64_t n0 = nt * OZ_BN + col0;
+      // Column data of the tile, one column per lane (broadcast by shuffles in
+      // the store loop), loaded before the accumulators are ready.
+      const int64_t n_l = n0 + lane;
+      const bool col_ok_l = n_l < g.N;
+      const int en_r = __ldg(exp_b + h * n_pad + n_l);
+      const int64_t dn_r = col_ok_l ? __ldg(g.s.d_n + n_l) : 0;
+      const int64_t cn_r = (col_ok_l && !g.e.beta_zero) ? __ldg(g.s.c_n + n_l) : 0;
       const int64_t me = mt * OZ_BM + lane_base + lane;  // row of the embedded product
       const int64_t m = CPLX ? (me >> 1) : me;            // output row
       const bool row_ok = me < m_emb;
@@ -432,15 +495,48 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
       const int64_t cm = (row_ok && !g.e.beta_zero) ? __ldg(g.s.c_m + m) : 0;
       const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : __ldg(g.s.h_c + h)) + cm;
       T* Db = static_cast<T*>(g.D) + __ldg(g.s.h_d + h) + dm;
+
+      if (!mbar_wait(accf, j & 1u)) {
+        atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+        break;
+      }
+      tc_fence_after();
+      // Drain: the S diagonals, smallest weight first, into FP64 (each term
+      // is an exact power-of-two multiple of an INT32); both 16-column loads
+      // of a diagonal are in flight together.
+      double v[OZ_EPI_COLS];
 #pragma unroll
-      for (int nn = 0; nn < OZ_BN; ++nn) {
+      for (int jj = 0; jj < OZ_EPI_COLS; ++jj) v[jj] = 0.0;
+#pragma unroll
+      for (int gd = S - 1; gd >= 0; --gd) {
+        uint32_t r[OZ_EPI_COLS / 16][16];
+#pragma unroll
+        for (int c = 0; c < OZ_EPI_COLS / 16; ++c)
+          tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + col0 + c * 16), r[c]);
+        tmem_ld_wait();
+        const double w = pow2(-7 * (gd + 2));
+#pragma unroll
+        for (int c = 0; c < OZ_EPI_COLS / 16; ++c)
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) v[c * 16 + jj] += (double)(int)r[c][jj] * w;
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_empty);
+
+      // x = v 2^(em + en), rounded once (as ldexp would).
+#pragma unroll
+      for (int nn = 0; nn < OZ_EPI_COLS; ++nn) {
         const int64_t n = n0 + nn;
         const bool col_ok = n < g.N;
-        const int en = __ldg(exp_b + h * n_pad + n);
-        const double x = (em == EXP_NONFINITE || en == EXP_NONFINITE) ? __longlong_as_double(0x7ff8000000000000ll)
-                                                                       : ldexp(v[nn], em + en);
-        const int64_t dn = col_ok ? __ldg(g.s.d_n + n) : 0;
-        const int64_t cn = (col_ok && !g.e.beta_zero) ? __ldg(g.s.c_n + n) : 0;
+        const int en = __shfl_sync(0xffffffffu, en_r, nn);
+        const int64_t dn = __shfl_sync(0xffffffffu, dn_r, nn);
+        const int64_t cn = __shfl_sync(0xffffffffu, cn_r, nn);
+        const int sc = em + en;
+        double x;
+        if (em == EXP_NONFINITE || en == EXP_NONFINITE) x = __longlong_as_double(0x7ff8000000000000ll);
+        else if (sc >= -1022 && sc <= 1023) x = v[nn] * pow2(sc);
+        else x = ldexp(v[nn], sc);
         if constexpr (CPLX) {
           const double other = __shfl_xor_sync(0xffffffffu, x, 1);
           if (row_ok && (lane & 1) == 0 && col_ok) epilogue_store<double, true>(g.e, x, other, Cb + cn, Db + dn);
@@ -475,7 +571,7 @@ cudaError_t run_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ap, co
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t ntiles = (L.n_pad / OZ_BN) * (L.m_pad / OZ_BM) * L.H;
   const unsigned grid = (unsigned)(ntiles < sms ? ntiles : sms);
-  ozaki_gemm_kernel<S, CPLX><<<grid, 192, Cfg::SMEM, st>>>(ma, mb, g, ea, eb, L.m_emb, L.m_pad, L.n_pad, L.exp_a_pad,
+  ozaki_gemm_kernel<S, CPLX><<<grid, OZ_THREADS, Cfg::SMEM, st>>>(ma, mb, g, ea, eb, L.m_emb, L.m_pad, L.n_pad, L.exp_a_pad,
                                                            kb0, kb1);
   return cudaGetLastError();
 }
@@ -500,7 +596,9 @@ OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K,
   L.slices = slices;
   L.cplx = cplx ? 1 : 0;
   L.m_emb = cplx ? 2 * M : M;
-  L.k_emb = cplx ? 2 * K : K;
+  // Complex depth: real parts in [0, K), imaginary parts in [k_half, k_half + K).
+  L.k_half = cplx ? (K + OZ_BK - 1) / OZ_BK * OZ_BK : K;
+  L.k_emb = cplx ? 2 * L.k_half : K;
   L.m_pad = (L.m_emb + OZ_BM - 1) / OZ_BM * OZ_BM;
   L.n_pad = (N + OZ_BN - 1) / OZ_BN * OZ_BN;
   L.k_pad = (L.k_emb + OZ_BK - 1) / OZ_BK * OZ_BK;
@@ -527,18 +625,30 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
                          int64_t nrows_emb, int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
                          int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
   if (hfast) {
-    ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)((exp_pad + 7) / 8), (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
+    ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);
-    ozaki_slice_hfast_kernel<CPLX>
-        <<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
-            X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, rows_pad, exp_pad, L.k_pad, L.H, which, conj, L.slices,
-            planes);
+    if (CPLX) {
+      // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
+      const dim3 grid((unsigned)(L.k_half / 64), (unsigned)(which == 0 ? rows_pad / 2 : rows_pad),
+                      (unsigned)((L.H + 31) / 32));
+      if (which == 0)
+        ozaki_slice_hfast_c64_kernel<0><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                               exp_pad, L.k_pad, L.H, conj, L.slices, planes);
+      else
+        ozaki_slice_hfast_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                               exp_pad, L.k_pad, L.H, conj, L.slices, planes);
+    } else {
+      ozaki_slice_hfast_kernel<CPLX>
+          <<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
+              X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, which,
+              conj, L.slices, planes);
+    }
   } else {
     ozaki_exp_kernel<CPLX><<<dim3((unsigned)((nrows + 31) / 32), (unsigned)L.H), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, kfast, exps);
     ozaki_slice_kernel<CPLX><<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
-        X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, rows_pad, exp_pad, L.k_pad, L.H, kfast, which, conj,
-        L.slices, planes);
+        X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, kfast, which,
+        conj, L.slices, planes);
   }
 }
 

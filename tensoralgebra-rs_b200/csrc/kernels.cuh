@@ -116,6 +116,7 @@ struct OzakiLayout {
   int cplx;        // complex operands embedded as a real problem (2M rows, 2K depth)
   int64_t m_emb;   // rows of the embedded A'
   int64_t k_emb;   // depth of the embedded product
+  int64_t k_half;  // complex: offset of the imaginary half of the depth (K rounded up to 64)
   int64_t m_pad, n_pad, k_pad;
   int64_t exp_a_pad;  // row stride of the A exponent array
   int64_t H;

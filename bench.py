@@ -309,6 +309,28 @@ def run_config(args, tp, torch, ex):
 
     cfg = args.config
     out = {"config": cfg, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "unit": "TFLOP/s"}
+    # Pipe peaks measured on this GPU (register-only probe kernels), and the
+    # INT8 tensor peak taken as twice the measured dense BF16 burst peak.
+    peaks, peak_src = measured_peaks()
+    pipe = {"fp64_dmma": ex.probe_peak(0), "fp32_ffma": ex.probe_peak(1),
+            "int8_tcgen05": 2.0 * peaks["bf16_tflops"]}
+    out["pipe_peaks_tflops"] = dict(pipe, source="probe kernels (fp64/fp32, measured here); int8 = 2 x " + peak_src)
+
+    def roofline(entry, kernel, pipe_flop_per_step, peak_name):
+        """Pipe fraction of the dominant kernel: executed pipe flops / its CUDA-event time / measured peak."""
+        kt = entry["kernels"].get(kernel)
+        if not kt:
+            return
+        k_ms = kt["ms"] / kt["launches"] * (kt["launches"] / args.steps)
+        entry["roofline"] = {"kernel": kernel, "pipe": peak_name, "achieved": pipe_flop_per_step / (k_ms * 1e-3) / 1e12,
+                             "peak": pipe[peak_name], "unit": "TFLOP/s",
+                             "frac": pipe_flop_per_step / (k_ms * 1e-3) / 1e12 / pipe[peak_name]}
+
+    def ozaki_products(entry):
+        fam = entry.get("family", "")
+        sl = int(fam.split(".s")[1].split(".")[0]) if ".s" in fam else 7
+        return sl * (sl + 1) // 2
+
     if cfg == "c1":
         e = 24
         cm = col_major([e] * 4)
@@ -336,6 +358,10 @@ def run_config(args, tp, torch, ex):
             out[scheme] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
                            "rel_err_vs_packed_oracle": oracle.rel_frobenius(D.cpu().numpy(), want),
                            "family": p.report()["family"]}
+            if code:
+                roofline(out[scheme], "ozaki_gemm", ozaki_products(out[scheme]) * flop, "int8_tcgen05")
+            else:
+                roofline(out[scheme], out[scheme]["family"], flop, "fp64_dmma")
     elif cfg == "c3":
         nb, n = 64, 384
         ext = [nb, n, n]
@@ -370,6 +396,12 @@ def run_config(args, tp, torch, ex):
                 den += abs(ref) ** 2
             out[scheme] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
                            "rel_err_sampled": (num / den) ** 0.5, "family": p.report()["family"]}
+            if code:
+                # Embedded real problem: 2M x N x 2K per batch entry, 2 flops per MAC.
+                emb = 2.0 * (2 * n) * n * (2 * n) * nb
+                roofline(out[scheme], "ozaki_gemm", ozaki_products(out[scheme]) * emb, "int8_tcgen05")
+            else:
+                roofline(out[scheme], out[scheme]["family"], flop, "fp64_dmma")
     elif cfg in ("c4", "c4c"):
         dt = "complex128" if cfg == "c4c" else "float64"
         tdt = tp.C64 if cfg == "c4c" else tp.F64
@@ -424,6 +456,7 @@ def run_config(args, tp, torch, ex):
             worst = max(worst, float(np.linalg.norm(got - want) / np.linalg.norm(want)))
         out["rel_err_sampled_items"] = worst
         out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
+        roofline(out["grouped"], "grouped", flop, "fp64_dmma")
     elif cfg == "c5":
         i, k, l = 512, 128, 256
         ea, eb, ed = [i, k, k, l], [l, i, k], [i, i]
@@ -447,6 +480,11 @@ def run_config(args, tp, torch, ex):
         out["plain"] = {"tflops": 3 * flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
                         "flops_counted": "forward + dA + dB, 3 x 2*i*j*k*l; the dA zero fill (17.2 GB) is extra",
                         "family": p.report()["family"]}
+        gemm_ms = sum(v["ms"] for n_, v in kt.items() if "dmma" in n_) / args.steps
+        out["plain"]["roofline"] = {"kernel": "dmma (forward + adjoints)", "pipe": "fp64_dmma",
+                                    "achieved": 3 * flop / (gemm_ms * 1e-3) / 1e12, "peak": pipe["fp64_dmma"],
+                                    "unit": "TFLOP/s",
+                                    "frac": 3 * flop / (gemm_ms * 1e-3) / 1e12 / pipe["fp64_dmma"]}
     print(json.dumps(out), flush=True)
 
 

@@ -87,7 +87,8 @@ struct TileGather {
 // the running total (round-to-nearest FADD), which keeps the FP32 rounding
 // error of a deep K near u * (sqrt(BK) + sqrt(K / BK)) instead of u * sqrt(K).
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
-__device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
+__device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                          int64_t split = 0) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int PAD = 4;
   constexpr int SA = BM + PAD, SB = BN + PAD;
@@ -134,14 +135,17 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
       if (CPLX) tot_im[i][j] = R(0);
     }
 
-  const int64_t nt = (g.K + BK - 1) / BK;
-  ga.load(Ab, am_s, g.s.a_k, m0, g.M, 0, g.K, g.a_kfast, g.conj_a, tid);
-  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
+  // This CTA's K range (the whole of K unless split).
+  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
+  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
+  const int64_t nt = (ke - kb + BK - 1) / BK;
+  ga.load(Ab, am_s, g.s.a_k, m0, g.M, kb, ke, g.a_kfast, g.conj_a, tid);
+  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, kb, ke, g.b_kfast, g.conj_b, tid);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
   if (nt > 1) {
-    ga.load_idx(g.s.a_k, BK, g.K, g.a_kfast, tid);
-    gb.load_idx(g.s.b_k, BK, g.K, g.b_kfast, tid);
+    ga.load_idx(g.s.a_k, kb + BK, ke, g.a_kfast, tid);
+    gb.load_idx(g.s.b_k, kb + BK, ke, g.b_kfast, tid);
   }
   __syncthreads();
 
@@ -205,8 +209,8 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
       ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
       gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
       if (t + 2 < nt) {
-        ga.load_idx(g.s.a_k, (t + 2) * BK, g.K, g.a_kfast, tid);
-        gb.load_idx(g.s.b_k, (t + 2) * BK, g.K, g.b_kfast, tid);
+        ga.load_idx(g.s.a_k, kb + (t + 2) * BK, ke, g.a_kfast, tid);
+        gb.load_idx(g.s.b_k, kb + (t + 2) * BK, ke, g.b_kfast, tid);
       }
     }
     __syncthreads();
@@ -222,7 +226,11 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
     for (int j = 0; j < TN; ++j) {
       const int cc = (j < HN) ? (ty * HN + j) : (BN / 2 + ty * HN + (j - HN));
       if (n0 + cc >= g.N) continue;
-      epilogue_store<R, CPLX>(g.e, tot_re[i][j], CPLX ? tot_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
+      if (g.partial)
+        Elem<R, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
+                             tot_re[i][j], CPLX ? tot_im[i][j] : R(0));
+      else
+        epilogue_store<R, CPLX>(g.e, tot_re[i][j], CPLX ? tot_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
                               Db + dm_s[rr] + dn_s[cc]);
     }
   }
@@ -238,7 +246,8 @@ __device__ inline void dmma_884(double& d0, double& d1, double a, double b) {
 
 // 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 8x8 DMMA tiles.
 template <bool CPLX, int WM, int WN, int BK>
-__device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
+__device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                          int64_t split = 0) {
   constexpr int BM = 2 * WM, BN = 2 * WN, NT = 128;
   constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
   constexpr int NPL = CPLX ? 2 : 1;
@@ -283,14 +292,17 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       if (CPLX) ci[i][j][0] = ci[i][j][1] = 0.0;
     }
 
-  const int64_t nt = (g.K + BK - 1) / BK;
-  ga.load(Ab, am_s, g.s.a_k, m0, g.M, 0, g.K, g.a_kfast, g.conj_a, tid);
-  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, 0, g.K, g.b_kfast, g.conj_b, tid);
+  // This CTA's K range (the whole of K unless split).
+  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
+  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
+  const int64_t nt = (ke - kb + BK - 1) / BK;
+  ga.load(Ab, am_s, g.s.a_k, m0, g.M, kb, ke, g.a_kfast, g.conj_a, tid);
+  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, kb, ke, g.b_kfast, g.conj_b, tid);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
   if (nt > 1) {
-    ga.load_idx(g.s.a_k, BK, g.K, g.a_kfast, tid);
-    gb.load_idx(g.s.b_k, BK, g.K, g.b_kfast, tid);
+    ga.load_idx(g.s.a_k, kb + BK, ke, g.a_kfast, tid);
+    gb.load_idx(g.s.b_k, kb + BK, ke, g.b_kfast, tid);
   }
   __syncthreads();
 
@@ -331,8 +343,8 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       ga.store(As[buf ^ 1][0], As[buf ^ 1][NPL - 1], SA, g.a_kfast, tid);
       gb.store(Bs[buf ^ 1][0], Bs[buf ^ 1][NPL - 1], SB, g.b_kfast, tid);
       if (t + 2 < nt) {
-        ga.load_idx(g.s.a_k, (t + 2) * BK, g.K, g.a_kfast, tid);
-        gb.load_idx(g.s.b_k, (t + 2) * BK, g.K, g.b_kfast, tid);
+        ga.load_idx(g.s.a_k, kb + (t + 2) * BK, ke, g.a_kfast, tid);
+        gb.load_idx(g.s.b_k, kb + (t + 2) * BK, ke, g.b_kfast, tid);
       }
     }
     __syncthreads();
@@ -350,7 +362,11 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       for (int q = 0; q < 2; ++q) {
         const int cc = wn0 + j * 8 + fk * 2 + q;
         if (n0 + cc >= g.N) continue;
-        epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
+        if (g.partial)
+          Elem<double, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
+                                    cr[i][j][q], CPLX ? ci[i][j][q] : 0.0);
+        else
+          epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
                                      Db + dm_s[rr] + dn_s[cc]);
       }
   }
@@ -359,12 +375,13 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
 // One CTA per (batch, M tile, N tile).
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(GemmArgs g) {
-  simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, blockIdx.z, blockIdx.y, blockIdx.x);
+  // blockIdx.z = split * H + h.
+  simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
 }
 
 template <bool CPLX, int WM, int WN, int BK>
 __global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
-  dmma_tile<CPLX, WM, WN, BK>(g, blockIdx.z, blockIdx.y, blockIdx.x);
+  dmma_tile<CPLX, WM, WN, BK>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
 }
 
 // Persistent grouped kernel over a heterogeneous list (contract_batched): the
@@ -443,7 +460,8 @@ struct DmmaTileOp {
 
 template <int BM, int BN>
 dim3 grid_for(const GemmArgs& g) {
-  return dim3((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM), (unsigned)g.H);
+  const int64_t splits = g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1;
+  return dim3((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM), (unsigned)(g.H * splits));
 }
 
 }  // namespace
@@ -473,9 +491,83 @@ int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, i
   return PLAIN_AUTO;
 }
 
+void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms, int* kernel,
+                         int* splits, int64_t* k_chunk) {
+  auto tiles = [&](int k) {
+    int bm = 0, bn = 0;
+    plain_tile_shape(k, &bm, &bn);
+    return ((M + bm - 1) / bm) * ((N + bn - 1) / bn) * H;
+  };
+  static const int large[4] = {PLAIN_F32_SIMT_128x128, PLAIN_F64_DMMA_64x64, PLAIN_C32_SIMT_64x64,
+                               PLAIN_C64_DMMA_64x32};
+  *splits = 1;
+  *k_chunk = 0;
+  const int64_t min_chunk = 512;  // K per split
+  const int k = pinned ? pinned : large[dtype & 3];
+  const int64_t t = tiles(k);
+  if (t < num_sms && K >= 2 * min_chunk) {
+    int64_t s = (2 * num_sms + t - 1) / t;
+    s = s < K / min_chunk ? s : K / min_chunk;
+    s = s < 64 ? s : 64;
+    while (s > 1 && H * s > 65535) --s;
+    if (s > 1) {
+      const int64_t chunk = ((K + s - 1) / s + 63) / 64 * 64;  // whole 64-deep blocks
+      *kernel = k;
+      *splits = (int)((K + chunk - 1) / chunk);
+      *k_chunk = chunk;
+      return;
+    }
+  }
+  *kernel = pinned ? pinned : choose_plain_kernel(dtype, M, N, K, H, num_sms);
+}
+
+namespace {
+
+// Split-K reduce: one thread per output element (m fastest), partials summed
+// in split order, then the alpha/beta/conjugation epilogue through the scatter.
+template <class R, bool CPLX>
+__global__ void __launch_bounds__(256) splitk_reduce_kernel(GemmArgs g, int splits) {
+  using T = typename Elem<R, CPLX>::type;
+  const int64_t total = g.H * g.M * g.N;
+  const T* P = static_cast<const T*>(g.partial);
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = idx % g.M, n = (idx / g.M) % g.N, h = idx / (g.M * g.N);
+    R sr = R(0), si = R(0);
+    for (int sp = 0; sp < splits; ++sp) {
+      R vr, vi;
+      Elem<R, CPLX>::load(P + ((sp * g.H + h) * g.N + n) * g.M + m, vr, vi);
+      sr += vr;
+      si += vi;
+    }
+    const T* c = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h] + g.s.c_m[m] + g.s.c_n[n]);
+    T* d = static_cast<T*>(g.D) + g.s.h_d[h] + g.s.d_m[m] + g.s.d_n[n];
+    epilogue_store<R, CPLX>(g.e, sr, si, c, d);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_splitk_reduce(int dtype, const GemmArgs& g, int splits, cudaStream_t st) {
+  const int64_t total = g.H * g.M * g.N;
+  if (total <= 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (total + 255) / 256;
+  const unsigned blocks = (unsigned)(want < (int64_t)sms * 16 ? want : (int64_t)sms * 16);
+  switch (dtype) {
+    case 0: splitk_reduce_kernel<float, false><<<blocks, 256, 0, st>>>(g, splits); break;
+    case 1: splitk_reduce_kernel<double, false><<<blocks, 256, 0, st>>>(g, splits); break;
+    case 2: splitk_reduce_kernel<float, true><<<blocks, 256, 0, st>>>(g, splits); break;
+    case 3: splitk_reduce_kernel<double, true><<<blocks, 256, 0, st>>>(g, splits); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.H <= 0) return cudaSuccess;
-  if (g.H > 65535) return cudaErrorInvalidConfiguration;
+  if (g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1) > 65535) return cudaErrorInvalidConfiguration;
   switch (kernel) {
     case PLAIN_F32_SIMT_128x128:
       if (dtype != 0) return cudaErrorInvalidValue;

@@ -46,6 +46,12 @@ struct GemmArgs {
   int a_kfast, b_kfast, d_mfast;
   Epilogue e;
   unsigned* status;
+  // Split-K: each K chunk of k_chunk (a multiple of the tile depth; 0 = all
+  // of K) is one CTA's range; with `partial` set, tiles write their raw
+  // accumulators to partial[((split * H + h) * N + n) * M + m] and a reduce
+  // pass applies the epilogue.
+  int64_t k_chunk;
+  void* partial;
 };
 
 // Kernel families of the plain (drop-in) path.
@@ -87,6 +93,13 @@ cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t*
 const char* plain_kernel_name(int kernel);
 // The family the autotuner would pick for a shape (no launch).
 int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
+// One-launch choice with split-K: the family (or `pinned`) and the number of
+// K chunks (1 = no split). Deep contractions with fewer large tiles than SMs
+// take the large tile and split K so that about two CTAs run per SM.
+void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms, int* kernel,
+                         int* splits, int64_t* k_chunk);
+// Sum of the split-K partials (fixed order) and the epilogue into D.
+cudaError_t launch_splitk_reduce(int dtype, const GemmArgs& g, int splits, cudaStream_t st);
 
 // ---- split precision (tensor cores) ----------------------------------------
 

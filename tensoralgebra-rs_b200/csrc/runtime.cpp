@@ -189,8 +189,10 @@ double stated_bound(DType t, Scheme s) {
 std::string Product::report() const {
   std::ostringstream o;
   const auto& st = packed.stats;
-  int kernel = kernel_pin ? kernel_pin
-                          : dev::choose_plain_kernel((int)problem.dtype, view.M, view.N, view.K, view.H, 148);
+  int kernel = 0, splits = 1;
+  int64_t chunk = 0;
+  dev::choose_plain_launch((int)problem.dtype, kernel_pin, view.M, view.N, view.K, view.H, 148, &kernel, &splits,
+                           &chunk);
   std::string family = scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
                        : scheme == Scheme::Bf16x3 ? "sm100.f32.tcgen05.bf16x3.128x256x32"
                        : scheme == Scheme::Bf16x6 ? "sm100.f32.tcgen05.bf16x6.128x256x32"
@@ -204,7 +206,8 @@ std::string Product::report() const {
     << ",\"h_axes\":" << axes_json(st.h_axes) << ",\"swapped\":" << (view.swapped ? "true" : "false")
     << ",\"a_kfast\":" << (view.a_kfast ? "true" : "false") << ",\"b_kfast\":" << (view.b_kfast ? "true" : "false")
     << ",\"d_mfast\":" << (view.d_mfast ? "true" : "false") << ",\"scheme\":\"" << scheme_name(scheme)
-    << "\",\"family\":\"" << family << "\",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)
+    << "\",\"family\":\"" << family << "\",\"split_k\":" << (scheme == Scheme::Plain ? splits : 1)
+    << ",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)
     << ",\"regular_rows\":" << regular_fraction(build_block_scatter(view.d_m, 32))
     << ",\"regular_cols\":" << regular_fraction(build_block_scatter(view.d_n, 32))
     << ",\"macs\":" << problem.macs() << "}";
@@ -351,7 +354,24 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
   }
   switch (pr.scheme) {
     case Scheme::Plain: {
-      int k = pr.kernel_pin ? pr.kernel_pin : dev::choose_plain_kernel(dt, g.M, g.N, g.K, g.H, ex.num_sms);
+      int k = 0, splits = 1;
+      int64_t chunk = 0;
+      dev::choose_plain_launch(dt, pr.kernel_pin, g.M, g.N, g.K, g.H, ex.num_sms, &k, &splits, &chunk);
+      if (splits > 1) {
+        // Split-K: partial tiles into the scratch, then the reduce + epilogue.
+        const size_t need = (size_t)splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype);
+        if (need + 256 > scratch_bytes) throw Error(ERR_INTERNAL, "split-K workspace too small");
+        dev::GemmArgs gs = g;
+        gs.k_chunk = chunk;
+        gs.partial = reinterpret_cast<void*>(align_up((uintptr_t)scratch, 256));
+        {
+          Timed t(ex, dev::plain_kernel_name(k));
+          check_cuda(dev::launch_plain_gemm(dt, k, gs, ex.stream), "plain contraction launch");
+        }
+        Timed t(ex, "splitk_reduce");
+        check_cuda(dev::launch_splitk_reduce(dt, gs, splits, ex.stream), "split-K reduce launch");
+        return;
+      }
       Timed t(ex, dev::plain_kernel_name(k));
       check_cuda(dev::launch_plain_gemm(dt, k, g, ex.stream), "plain contraction launch");
       return;
@@ -411,8 +431,14 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
   }
 }
 
-size_t scheme_scratch(const Product& pr) {
+size_t scheme_scratch(const Product& pr, int num_sms) {
   const auto& v = pr.view;
+  if (pr.scheme == Scheme::Plain) {
+    int k = 0, splits = 1;
+    int64_t chunk = 0;
+    dev::choose_plain_launch((int)pr.problem.dtype, pr.kernel_pin, v.M, v.N, v.K, v.H, num_sms, &k, &splits, &chunk);
+    return splits > 1 ? (size_t)splits * v.H * v.M * v.N * dtype_size(pr.problem.dtype) + 256 : 0;
+  }
   if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6)
     return dev::split_workspace_bytes(dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H));
   if (pr.scheme == Scheme::OzakiInt8)
@@ -554,7 +580,7 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
     span_bytes(p, s, &st[s].lo_bytes, &st[s].bytes);
     total = align_up(total, 256) + st[s].bytes;
   }
-  const size_t scratch = output_only ? 0 : scheme_scratch(pr);
+  const size_t scratch = output_only ? 0 : scheme_scratch(pr, ex.num_sms);
   char* ws = static_cast<char*>(ex.workspace(align_up(total, 256) + scratch + 512));
   size_t off = 0;
   for (int s = 0; s < 4; ++s) {

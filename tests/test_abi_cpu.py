@@ -240,3 +240,20 @@ def test_executor_handles_without_a_gpu(tp):
     assert (ps.value, bd.value) == (4, 2)
     assert tp.lib.TAPP_destroy_executor(h.value) == 0
     assert tp.lib.TAPP_destroy_executor(0) == 0
+
+
+def test_planner_splits_k_only_for_deep_contractions_with_few_tiles(tp):
+    """The launch choice (reported per plan, for 148 SMs): split-K when the
+    large-tile grid has fewer tiles than SMs and K is deep; never otherwise."""
+    def report(m, n, k, dt=1):
+        h = tp.Handle()
+        infos = [tp.TensorInfo(dt, [m, k], [1, m]), tp.TensorInfo(dt, [k, n], [1, k]),
+                 tp.TensorInfo(dt, [m, n], [1, m]), tp.TensorInfo(dt, [m, n], [1, m])]
+        p = tp.TensorProduct.create(h, (0, infos[0], [0, 2]), (0, infos[1], [2, 1]), (0, infos[2], [0, 1]),
+                                    (0, infos[3], [0, 1]))
+        return p.report()
+
+    deep = report(512, 512, 32768)
+    assert deep["split_k"] > 1 and "64x64" in deep["family"]
+    assert report(4096, 4096, 4096, dt=0)["split_k"] == 1  # enough tiles
+    assert report(64, 64, 512)["split_k"] == 1  # shallow

@@ -297,6 +297,30 @@ def test_c1_full_size_f64(tp, ex, torch_cuda, orc):
     assert orc.rel_frobenius(got, want) <= 1e-13
 
 
+# ----------------------------------------------------------------- split-K
+@pytest.mark.parametrize("dt", DTYPES)
+def test_split_k_on_deep_contractions_with_few_tiles(tp, ex, torch_cuda, orc, dt):
+    """Few output tiles and a deep K: the launch splits K across CTAs, writes
+    partial tiles and reduces them in a fixed order before the epilogue (the
+    KC-slab accumulation of the reference's driver, spread over SMs). Batch,
+    conjugation, beta and a permuted C layout all pass through the reduce."""
+    rng = np.random.default_rng(77)
+    m, n, k, h = {"float32": (100, 90, 4096, 1), "float64": (70, 65, 3000, 1),
+                  "complex64": (50, 60, 2500, 2), "complex128": (40, 33, 2100, 2)}[dt]
+    cplx = dt.startswith("complex")
+    A = Op(rnd(rng, dt, h * m * k), [k, m, h], [1, k, k * m], [2, 0, 9], conj=cplx)
+    B = Op(rnd(rng, dt, h * k * n), [h, n, k], [1, h, h * n], [9, 1, 2])
+    C = Op(rnd(rng, dt, h * m * n), [n, h, m], [1, n, n * h], [1, 9, 0])
+    d0 = rnd(rng, dt, h * m * n)
+    D = Op(d0, [m, n, h], [1, m, m * n], [0, 1, 9])
+    al, be = (complex(0.5, -1.0), complex(0.25, 0.75)) if cplx else (1.25, -0.5)
+    want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
+    st, got, p = run(tp, ex, torch_cuda, dt, A, B, C, D, al, be)
+    assert st == 0, tp.last_error()
+    assert p.report()["split_k"] > 1, p.report()
+    assert orc.rel_frobenius(got, want) <= plain_tol(dt), (dt, orc.rel_frobenius(got, want))
+
+
 # ----------------------------------------------------------------- split paths
 def _c2_layout(e):
     """Config 2 layout at extent e per mode: A[k1,m1,k2,m2] with a non-unit

@@ -379,8 +379,10 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(Gem
   simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
 }
 
+// Three CTAs per SM (at most 170 registers a thread): twelve warps to hide the
+// gather and shared-memory latency around the DMMA pipe.
 template <bool CPLX, int WM, int WN, int BK>
-__global__ void __launch_bounds__(128) dmma_gemm_kernel(GemmArgs g) {
+__global__ void __launch_bounds__(128, 3) dmma_gemm_kernel(GemmArgs g) {
   dmma_tile<CPLX, WM, WN, BK>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
 }
 
@@ -489,6 +491,24 @@ int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, i
     case 3: return tiles(64, 32) >= num_sms ? PLAIN_C64_DMMA_64x32 : PLAIN_C64_DMMA_32x32;
   }
   return PLAIN_AUTO;
+}
+
+int choose_grouped_kernel(int dtype, int64_t M, int64_t N) {
+  // In a grouped launch the list fills the GPU, so the tile is chosen for
+  // reuse and padding alone: the large tile unless it wastes much more of its
+  // area on padding than the small one.
+  static const int large[4] = {PLAIN_F32_SIMT_128x128, PLAIN_F64_DMMA_64x64, PLAIN_C32_SIMT_64x64,
+                               PLAIN_C64_DMMA_64x32};
+  static const int small[4] = {PLAIN_F32_SIMT_64x64, PLAIN_F64_DMMA_32x32, PLAIN_C32_SIMT_64x64,
+                               PLAIN_C64_DMMA_32x32};
+  auto util = [&](int k) {
+    int bm = 0, bn = 0;
+    plain_tile_shape(k, &bm, &bn);
+    const double padded = (double)((M + bm - 1) / bm * bm) * (double)((N + bn - 1) / bn * bn);
+    return (double)M * (double)N / padded;
+  };
+  const int L = large[dtype & 3], S = small[dtype & 3];
+  return util(L) >= 0.8 * util(S) ? L : S;
 }
 
 void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms, int* kernel,

@@ -93,6 +93,8 @@ cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t*
 const char* plain_kernel_name(int kernel);
 // The family the autotuner would pick for a shape (no launch).
 int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
+// Family of an item inside a grouped launch (the list fills the GPU).
+int choose_grouped_kernel(int dtype, int64_t M, int64_t N);
 // One-launch choice with split-K: the family (or `pinned`) and the number of
 // K chunks (1 = no split). Deep contractions with fewer large tiles than SMs
 // take the large tile and split K so that about two CTAs run per SM.

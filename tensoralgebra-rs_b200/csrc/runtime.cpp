@@ -669,13 +669,11 @@ uint64_t list_key(int n, Product* const* plans, const Scalar* alpha, const Scala
 Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<int>& idx,
                                  const std::vector<int>& single, Product* const* plans, const Scalar* alpha,
                                  const Scalar* beta, const Item* items) {
-  // Families: each item takes the kernel the autotuner picks for its shape.
+  // Families: each item takes the tile that suits its shape inside a full launch.
   std::map<int, std::vector<int>> fam;
   for (int i : idx) {
     Product& pr = *plans[i];
-    const int k = pr.kernel_pin ? pr.kernel_pin
-                                : dev::choose_plain_kernel((int)pr.problem.dtype, pr.view.M, pr.view.N, pr.view.K,
-                                                           pr.view.H, ex.num_sms);
+    const int k = pr.kernel_pin ? pr.kernel_pin : dev::choose_grouped_kernel((int)pr.problem.dtype, pr.view.M, pr.view.N);
     fam[k].push_back(i);
   }
   Executor::Graph gr;

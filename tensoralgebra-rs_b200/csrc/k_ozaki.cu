@@ -67,37 +67,52 @@ __device__ inline double embedded(const double* X, const int64_t* rows_scat, con
 }
 
 // The S signed 7-bit slices of four values of one row with exponent e
-// (|x| < 2^e), written as char4 into the S planes. T = trunc(x 2^(7S - e)) is
+// (|x| < 2^e), written as one 4-byte word per plane. T = trunc(x 2^(7S - e)) is
 // exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
 // of x, are the slices: the same digits as repeatedly multiplying the scaled
-// value by 128 and removing the integer part.
-__device__ inline void write_slices(const double (&x)[4], int e, int S, int8_t* o, int64_t plane) {
+// value by 128 and removing the integer part. Digits are cut from the 32-bit
+// halves of |T| (a funnel shift across the boundary), packed four to a word,
+// and negated bytewise where x < 0: for a byte b <= 127,
+// ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
+template <int S>
+__device__ inline void write_slices_t(const double (&x)[4], int e, int8_t* o, int64_t plane) {
   const int k = 7 * S - e;  // scale exponent; above 1023 only for rows below 2^-967
   const bool two = k > 1023;
   const double s1 = two ? ldexp(1.0, 1000) : ldexp(1.0, k);
   const double s2 = two ? ldexp(1.0, k - 1000) : 1.0;
-  unsigned long long mag[4];
-  bool neg[4];
+  uint32_t lo[4], hi[4], negmask = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const long long t = (long long)((x[q] * s1) * s2);  // truncation toward zero
-    neg[q] = t < 0;
-    mag[q] = (unsigned long long)(neg[q] ? -t : t);
+    const unsigned long long mag = (unsigned long long)(t < 0 ? -t : t);
+    lo[q] = (uint32_t)mag;
+    hi[q] = (uint32_t)(mag >> 32);
+    negmask |= (t < 0 ? 0xffu : 0u) << (8 * q);
   }
+#pragma unroll
   for (int sl = 0; sl < S; ++sl) {
     const int sh = 7 * (S - 1 - sl);
-    signed char qv[4];
+    uint32_t w = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int d = (int)((mag[q] >> sh) & 127ull);
-      qv[q] = (signed char)(neg[q] ? -d : d);
+      uint32_t d;
+      if (sh + 7 <= 32) d = lo[q] >> sh;
+      else if (sh >= 32) d = hi[q] >> (sh - 32);
+      else d = __funnelshift_r(lo[q], hi[q], sh);
+      w |= (d & 127u) << (8 * q);
     }
-    char4 c;
-    c.x = qv[0];
-    c.y = qv[1];
-    c.z = qv[2];
-    c.w = qv[3];
-    *reinterpret_cast<char4*>(o + sl * plane) = c;
+    const uint32_t nw = ((w ^ 0x7f7f7f7fu) + 0x01010101u) ^ 0x80808080u;
+    *reinterpret_cast<uint32_t*>(o + sl * plane) = (w & ~negmask) | (nw & negmask);
+  }
+}
+
+__device__ inline void write_slices(const double (&x)[4], int e, int S, int8_t* o, int64_t plane) {
+  switch (S) {
+    case 4: write_slices_t<4>(x, e, o, plane); break;
+    case 5: write_slices_t<5>(x, e, o, plane); break;
+    case 6: write_slices_t<6>(x, e, o, plane); break;
+    case 7: write_slices_t<7>(x, e, o, plane); break;
+    default: write_slices_t<8>(x, e, o, plane); break;
   }
 }
 

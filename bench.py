@@ -601,6 +601,8 @@ def main():
     traffic, traffic_src = profiled_traffic(dom_name) if dom_name else (None, None)
     launches = sum(v["launches"] for v in kt.values())
     kernel_launches = launches + (kt.get("split_pack", {}).get("launches", 0))  # split_pack covers 2 launches
+    if plans[head].report().get("tail_parts", 1) > 1:  # the GEMM family adds the tail reduce kernel
+        kernel_launches += kt.get(dom_name, {}).get("launches", 0)
 
     # The other schemes, shorter runs, for the comparison.
     others = {}

@@ -131,10 +131,17 @@ struct TcCfg {
 // registers with round-to-nearest adds. The cross terms, 2^-8 smaller, go to
 // a second ("corr") accumulator that lives for the whole K loop. TMEM columns:
 // main [0, BN), corr [BN, 2 BN).
+//
+// Tail split: the grid is 1-D; CTAs [0, whole) own one tile each over all of
+// K, and the last `tail` tiles (those that would run as a partly filled last
+// wave) are split into `parts` K ranges of whole CK chunks, one CTA each. A
+// tail CTA writes its FP32 sum to partial[(tail tile * parts + part) * TC_BM
+// * BN + col * TC_BM + row] and split_tail_reduce_kernel adds the parts in
+// order and applies the epilogue.
 template <int S, int BN, int CK>
 __global__ void __launch_bounds__(TcCfg<S, BN>::THREADS, 1)
 tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
-                    int64_t m_pad, int64_t n_pad, int64_t k_pad) {
+                    int64_t m_pad, int64_t n_pad, int64_t k_pad, int64_t whole, int parts, float* partial) {
   using Cfg = TcCfg<S, BN>;
   constexpr int CPT = Cfg::COLS_PER_THREAD;
   extern __shared__ uint8_t smem_raw[];
@@ -149,9 +156,22 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(main_empty + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t h = blockIdx.z;
-  const int64_t m0 = (int64_t)blockIdx.y * TC_BM, n0 = (int64_t)blockIdx.x * BN;
-  const int nk = (int)(k_pad / TC_BK);
+  const int64_t tiles_n = n_pad / BN, tiles_m = m_pad / TC_BM;
+  const int nk_all = (int)(k_pad / TC_BK);
+  int64_t tile = blockIdx.x;
+  int part = -1;  // -1: the whole K range
+  int kb_lo = 0, kb_hi = nk_all;
+  if ((int64_t)blockIdx.x >= whole) {
+    const int64_t j = (int64_t)blockIdx.x - whole;
+    tile = whole + j / parts;
+    part = (int)(j % parts);
+    const int per = ((nk_all + parts - 1) / parts + CK - 1) / CK * CK;  // whole chunks per part
+    kb_lo = part * per;
+    kb_hi = kb_lo + per < nk_all ? kb_lo + per : nk_all;
+  }
+  const int64_t h = tile / (tiles_n * tiles_m);
+  const int64_t m0 = ((tile / tiles_n) % tiles_m) * TC_BM, n0 = (tile % tiles_n) * BN;
+  const int nk = kb_hi - kb_lo;  // k-blocks of this CTA (>= 1)
   const int nchunks = (nk + CK - 1) / CK;
 
   if (warp == 0 && lane == 0) {
@@ -194,12 +214,13 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         }
         mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
         uint8_t* sbase = ring + st * Cfg::STAGE;
+        const int kx = (kb_lo + kb) * TC_BK;
 #pragma unroll
         for (int p = 0; p < S; ++p)
-          tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kb * TC_BK, (int)((p * g.H + h) * m_pad + m0));
+          tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + m0));
 #pragma unroll
         for (int p = 0; p < S; ++p)
-          tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kb * TC_BK,
+          tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kx,
                       (int)((p * g.H + h) * n_pad + n0));
       }
     }
@@ -277,13 +298,19 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     const int64_t cm = (mok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
     const float* Cb = static_cast<const float*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]) + cm;
     float* Db = static_cast<float*>(g.D) + g.s.h_d[h] + dm;
+    float* Pb = part >= 0 ? partial + ((tile - whole) * parts + part) * (int64_t)(TC_BM * BN) + lane_base + lane
+                          : nullptr;
     // The last main_full commit also covers every cross-term MMA.
 #pragma unroll
     for (int q = 0; q < CPT / 16; ++q) {
       uint32_t r[16];
       tmem_ld_32x32b_x16(tmem_corr + lane_addr + (uint32_t)(col0 + 16 * q), r);
       tmem_ld_wait();
-      if (mok) {
+      if (part >= 0) {
+        // Tail part: the raw FP32 sum, column-major in the tile (coalesced).
+#pragma unroll
+        for (int j = 0; j < 16; ++j) Pb[(col0 + 16 * q + j) * TC_BM] = run[16 * q + j] + __uint_as_float(r[j]);
+      } else if (mok) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int nn = col0 + 16 * q + j;
@@ -303,8 +330,58 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   }
 }
 
+// Tail tiles: add the parts in order, then the epilogue through the scatter.
+template <int BN>
+__global__ void __launch_bounds__(256) split_tail_reduce_kernel(GemmArgs g, const float* __restrict__ partial,
+                                                                int64_t whole, int parts, int64_t tail, int64_t m_pad,
+                                                                int64_t n_pad) {
+  const int64_t tiles_n = n_pad / BN, tiles_m = m_pad / TC_BM;
+  const int64_t total = tail * TC_BM * BN;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = idx / (TC_BM * BN), within = idx % (TC_BM * BN);
+    const int row = (int)(within % TC_BM), col = (int)(within / TC_BM);
+    const int64_t tile = whole + t;
+    const int64_t h = tile / (tiles_n * tiles_m);
+    const int64_t m = ((tile / tiles_n) % tiles_m) * TC_BM + row, n = (tile % tiles_n) * BN + col;
+    if (m >= g.M || n >= g.N) continue;
+    float v = 0.f;
+    for (int p = 0; p < parts; ++p) v += partial[(t * parts + p) * (int64_t)(TC_BM * BN) + within];
+    const float* c = static_cast<const float*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h] + g.s.c_m[m] + g.s.c_n[n]);
+    float* d = static_cast<float*>(g.D) + g.s.h_d[h] + g.s.d_m[m] + g.s.d_n[n];
+    epilogue_store<float, false>(g.e, v, 0.f, c, d);
+  }
+}
+
+// The tail split for a grid of `tiles` tiles on `sms` SMs (one CTA per SM):
+// the tiles of a partly filled last wave are split into `parts` K ranges when
+// that fills the wave better; parts = 1 means no split.
+struct TailSplit {
+  int64_t whole, tail;
+  int parts;
+};
+inline TailSplit tail_split(int64_t tiles, int sms, int nk, int ck) {
+  TailSplit t{tiles, 0, 1};
+  const int64_t rem = tiles % sms;
+  if (rem == 0 || tiles < sms) return t;  // full waves, or one partial wave of whole tiles
+  int parts = (int)(sms / rem);
+  parts = parts < 4 ? parts : 4;
+  // Each part keeps at least two CK chunks and the last part is not empty.
+  auto fits = [&](int p) {
+    const int per = ((nk + p - 1) / p + ck - 1) / ck * ck;
+    return nk >= p * 2 * ck && (p - 1) * per < nk;
+  };
+  while (parts > 1 && !fits(parts)) --parts;
+  if (parts < 2) return t;
+  t.whole = tiles - rem;
+  t.tail = rem;
+  t.parts = parts;
+  return t;
+}
+
 template <int S, int BN, int CK>
-cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, cudaStream_t st) {
+cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, float* tail_partial,
+                   cudaStream_t st) {
   using Cfg = TcCfg<S, BN>;
   CUtensorMap ma, mb;
   if (!make_map_2d(&ma, ap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, L.k_pad, (int64_t)S * L.H * L.m_pad, TC_BK, TC_BM))
@@ -315,8 +392,22 @@ cudaError_t run_tc(const GemmArgs& g, const SplitLayout& L, const void* ap, cons
   cudaError_t e =
       cudaFuncSetAttribute(tc_bf16_gemm_kernel<S, BN, CK>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)(L.n_pad / BN), (unsigned)(L.m_pad / TC_BM), (unsigned)L.H);
-  tc_bf16_gemm_kernel<S, BN, CK><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(ma, mb, g, L.m_pad, L.n_pad, L.k_pad);
+  const int64_t tiles = (L.n_pad / BN) * (L.m_pad / TC_BM) * L.H;
+  TailSplit ts{tiles, 0, 1};
+  if (tail_partial) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    ts = tail_split(tiles, sms, (int)(L.k_pad / TC_BK), CK);
+  }
+  const int64_t grid = ts.whole + ts.tail * ts.parts;
+  tc_bf16_gemm_kernel<S, BN, CK><<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM, st>>>(
+      ma, mb, g, L.m_pad, L.n_pad, L.k_pad, ts.whole, ts.parts, tail_partial);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || ts.tail == 0) return e;
+  const int64_t elems = ts.tail * TC_BM * BN;
+  const unsigned blocks = (unsigned)((elems + 255) / 256 < 4096 ? (elems + 255) / 256 : 4096);
+  split_tail_reduce_kernel<BN><<<blocks, 256, 0, st>>>(g, tail_partial, ts.whole, ts.parts, ts.tail, L.m_pad,
+                                                       L.n_pad);
   return cudaGetLastError();
 }
 
@@ -348,13 +439,25 @@ cudaError_t launch_split_pack_f32(const GemmArgs& g, int which, const SplitLayou
   return cudaGetLastError();
 }
 
+int split_tail_parts(const SplitLayout& L, int num_sms) {
+  const int64_t tiles = (L.n_pad / 256) * (L.m_pad / TC_BM) * L.H;
+  return tail_split(tiles, num_sms, (int)(L.k_pad / TC_BK), 4).parts;
+}
+
+size_t split_tail_bytes(const SplitLayout& L, int num_sms) {
+  // At most one wave of tail parts (tail * parts <= num_sms) of 128 x 256 FP32.
+  (void)L;
+  return (size_t)num_sms * TC_BM * 256 * sizeof(float) + 256;
+}
+
 cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const void* ap, const void* bp, int scheme,
-                                cudaStream_t st) {
+                                cudaStream_t st, void* tail_partial) {
   if ((int64_t)L.planes * L.H * (L.m_pad > L.n_pad ? L.m_pad : L.n_pad) >= (int64_t)1 << 31)
     return cudaErrorInvalidValue;
   if (L.H > 65535) return cudaErrorInvalidConfiguration;
-  if (scheme == 2) return run_tc<3, 256, 4>(g, L, ap, bp, st);
-  return run_tc<2, 256, 4>(g, L, ap, bp, st);
+  float* tp = static_cast<float*>(tail_partial);
+  if (scheme == 2) return run_tc<3, 256, 4>(g, L, ap, bp, tp, st);
+  return run_tc<2, 256, 4>(g, L, ap, bp, tp, st);
 }
 
 }  // namespace dev

@@ -118,8 +118,13 @@ cudaError_t launch_split_pack_f32(const GemmArgs& g, int which, const SplitLayou
                                   cudaStream_t st);
 // The tcgen05 GEMM over packed planes, with the scatter epilogue.
 // npairs/pairs: the list of (a_plane, b_plane) products accumulated.
+// With `tail_partial` (split_tail_bytes of device memory), the tiles of a
+// partly filled last wave are split along K and reduced by a second kernel.
 cudaError_t launch_tc_bf16_gemm(const GemmArgs& g, const SplitLayout& L, const void* a_planes, const void* b_planes,
-                                int scheme, cudaStream_t st);
+                                int scheme, cudaStream_t st, void* tail_partial = nullptr);
+size_t split_tail_bytes(const SplitLayout& L, int num_sms);
+// K parts of the tail tiles for `num_sms` SMs (1 = no tail split).
+int split_tail_parts(const SplitLayout& L, int num_sms);
 // Bytes of packed workspace a split scheme needs.
 size_t split_workspace_bytes(const SplitLayout& L);
 SplitLayout split_layout(int scheme, int64_t M, int64_t N, int64_t K, int64_t H);

@@ -207,6 +207,10 @@ std::string Product::report() const {
     << ",\"a_kfast\":" << (view.a_kfast ? "true" : "false") << ",\"b_kfast\":" << (view.b_kfast ? "true" : "false")
     << ",\"d_mfast\":" << (view.d_mfast ? "true" : "false") << ",\"scheme\":\"" << scheme_name(scheme)
     << "\",\"family\":\"" << family << "\",\"split_k\":" << (scheme == Scheme::Plain ? splits : 1)
+    << ",\"tail_parts\":"
+    << ((scheme == Scheme::Bf16x3 || scheme == Scheme::Bf16x6)
+            ? dev::split_tail_parts(dev::split_layout((int)scheme, view.M, view.N, view.K, view.H), 148)
+            : 1)
     << ",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)
     << ",\"regular_rows\":" << regular_fraction(build_block_scatter(view.d_m, 32))
     << ",\"regular_cols\":" << regular_fraction(build_block_scatter(view.d_n, 32))
@@ -379,16 +383,20 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
     case Scheme::Bf16x3:
     case Scheme::Bf16x6: {
       const dev::SplitLayout L = dev::split_layout((int)pr.scheme, g.M, g.N, g.K, g.H);
-      if (dev::split_workspace_bytes(L) > scratch_bytes) throw Error(ERR_INTERNAL, "split workspace too small");
+      const size_t planes_bytes = dev::split_workspace_bytes(L);
+      if (planes_bytes + dev::split_tail_bytes(L, ex.num_sms) > scratch_bytes)
+        throw Error(ERR_INTERNAL, "split workspace too small");
       char* ap = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
       char* bp = ap + (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
+      char* tail = reinterpret_cast<char*>(align_up((uintptr_t)(ap + planes_bytes), 256));
       {
         Timed t(ex, "split_pack");
         check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
         check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, ex.stream), "split pack B");
       }
       Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
-      check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream), "tcgen05 contraction launch");
+      check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream, tail),
+                 "tcgen05 contraction launch");
       return;
     }
     case Scheme::OzakiInt8: {
@@ -439,8 +447,10 @@ size_t scheme_scratch(const Product& pr, int num_sms) {
     dev::choose_plain_launch((int)pr.problem.dtype, pr.kernel_pin, v.M, v.N, v.K, v.H, num_sms, &k, &splits, &chunk);
     return splits > 1 ? (size_t)splits * v.H * v.M * v.N * dtype_size(pr.problem.dtype) + 256 : 0;
   }
-  if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6)
-    return dev::split_workspace_bytes(dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H));
+  if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6) {
+    const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
+    return dev::split_workspace_bytes(L) + dev::split_tail_bytes(L, num_sms) + 512;
+  }
   if (pr.scheme == Scheme::OzakiInt8)
     return dev::ozaki_workspace_bytes(
         dev::ozaki_layout(pr.ozaki_slices, dtype_complex(pr.problem.dtype), v.M, v.N, v.K, v.H));

@@ -392,6 +392,32 @@ def test_split_precision_full_c2_sampled(tp, ex, torch_cuda):
         assert (num / den) ** 0.5 <= bound, (scheme, (num / den) ** 0.5)
 
 
+@pytest.mark.parametrize("scheme,bound", [(1, 2e-5), (2, 1e-6)], ids=["bf16x3", "bf16x6"])
+def test_split_precision_tail_split_against_float64(tp, ex, torch_cuda, scheme, bound):
+    """160 output tiles on 148 SMs: the 12 tiles of the partial last wave run
+    as K halves whose FP32 sums are added by a reduce kernel before the
+    epilogue (alpha, beta, a transposed C). Checked at every element against
+    float64 products."""
+    torch = torch_cuda
+    rng = np.random.default_rng(91)
+    m, n, k = 2560, 2048, 1024
+    a = rng.standard_normal(m * k).astype(np.float32)  # A[k, m], k fastest
+    b = rng.standard_normal(k * n).astype(np.float32)  # B[k, n]
+    c = rng.standard_normal(m * n).astype(np.float32)  # C[n, m] (transposed)
+    A = Op(a, [k, m], [1, k], [2, 0])
+    B = Op(b, [k, n], [1, k], [2, 1])
+    C = Op(c, [n, m], [1, n], [1, 0])
+    D = Op(np.zeros(m * n, dtype=np.float32), [m, n], [1, m], [0, 1])
+    st, got, _ = run(tp, ex, torch, "float32", A, B, C, D, 0.75, -0.5, precision=scheme)
+    assert st == 0, tp.last_error()
+    a2 = a.reshape(m, k).astype(np.float64)  # [m, k]
+    b2 = b.reshape(n, k).astype(np.float64)  # [n, k]
+    want = 0.75 * a2 @ b2.T - 0.5 * c.reshape(m, n).astype(np.float64)  # C[n, m] stored n fastest
+    gotm = got.reshape(n, m).T  # D[m, n], m fastest
+    err = np.linalg.norm(gotm - want) / np.linalg.norm(want)
+    assert err <= bound, err
+
+
 # ------------------------------------------------------------ front ends, DLPack
 def test_dot_general_execute_into_and_accum(tp, ex, torch_cuda, orc):
     torch = torch_cuda

@@ -456,6 +456,27 @@ def run_config(args, tp, torch, ex):
             worst = max(worst, float(np.linalg.norm(got - want) / np.linalg.norm(want)))
         out["rel_err_sampled_items"] = worst
         out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
+        # Per binary step (grouped), and the mixed roofline of the list: each
+        # item-step bounded by max(flops / FP64 DMMA peak, bytes / HBM peak).
+        es, fm = (16, 8) if cfg == "c4c" else (8, 2)
+        per_step, t_roof = [], 0.0
+        for si, pb in enumerate(prepared):
+            ms_s, _ = timed(lambda: pb.run(ex), max(2, args.steps), 1)
+            f_s = by_s = tr_s = 0.0
+            for it in items:
+                a_, b_, s_, p_ = it["a"], it["b"], it["s"], it["p"]
+                macs, elems = ((a_ * s_ * b_ * p_ * a_, a_ * s_ * b_ + a_ * p_ * a_ + s_ * b_ * p_ * a_),
+                               (s_ * b_ * p_ * a_ * s_ * p_, s_ * b_ * p_ * a_ + s_ * p_ * s_ * p_ + b_ * a_ * s_ * p_),
+                               (b_ * a_ * s_ * p_ * b_, b_ * a_ * s_ * p_ + b_ * p_ * b_ + a_ * s_ * b_))[si]
+                f_s += fm * macs
+                by_s += es * elems
+                tr_s += max(fm * macs / (pipe["fp64_dmma"] * 1e12), es * elems / (peaks["hbm_gbs"] * 1e9))
+            t_roof += tr_s
+            per_step.append({"step": si + 1, "ms": ms_s, "tflops": f_s / (ms_s * 1e-3) / 1e12,
+                             "roofline_ms": tr_s * 1e3, "frac_of_roofline": tr_s * 1e3 / ms_s})
+        out["grouped"]["per_step"] = per_step
+        out["grouped"]["mixed_roofline"] = {"ms": t_roof * 1e3, "frac": t_roof * 1e3 / out["grouped"]["ms_per_step"],
+                                            "rule": "sum over item-steps of max(flops/FP64 DMMA peak, bytes/HBM)"}
         roofline(out["grouped"], "grouped", flop, "fp64_dmma")
     elif cfg == "c5":
         i, k, l = 512, 128, 256

@@ -238,20 +238,25 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
 
 // ---------------------------------------------------------------- FP64 DMMA
 
-__device__ inline void dmma_884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+// D (16 x 8) += A (16 x 8, row) B (8 x 8, col) in FP64. Fragments, with
+// g = lane / 4 and t = lane % 4: a[r] = A[g + 8 (r % 2)][t + 4 (r / 2)],
+// b[r] = B[t + 4 r][g], d[r] = D[g + 8 (r / 2)][2 t + r % 2].
+__device__ inline void dmma_1688(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};\n"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 8x8 DMMA tiles.
+// 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 16x8 DMMA tiles.
 template <bool CPLX, int WM, int WN, int BK>
 __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
                                           int64_t split = 0) {
   constexpr int BM = 2 * WM, BN = 2 * WN, NT = 128;
   constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
   constexpr int NPL = CPLX ? 2 : 1;
-  constexpr int TI = WM / 8, TJ = WN / 8;
+  constexpr int TI = WM / 16, TJ = WN / 8;
+  static_assert(WM % 16 == 0 && WN % 8 == 0 && BK % 8 == 0, "m16n8k8 fragments");
   using T = typename Elem<double, CPLX>::type;
 
   __shared__ __align__(16) double As[2][NPL][BK * SA];
@@ -283,14 +288,16 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
   TileGather<double, CPLX, BM, BK, NT> ga;
   TileGather<double, CPLX, BN, BK, NT> gb;
 
-  double cr[TI][TJ][2], ci[CPLX ? TI : 1][CPLX ? TJ : 1][2];
+  double cr[TI][TJ][4], ci[CPLX ? TI : 1][CPLX ? TJ : 1][4];
 #pragma unroll
   for (int i = 0; i < TI; ++i)
 #pragma unroll
-    for (int j = 0; j < TJ; ++j) {
-      cr[i][j][0] = cr[i][j][1] = 0.0;
-      if (CPLX) ci[i][j][0] = ci[i][j][1] = 0.0;
-    }
+    for (int j = 0; j < TJ; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        cr[i][j][q] = 0.0;
+        if (CPLX) ci[i][j][q] = 0.0;
+      }
 
   // This CTA's K range (the whole of K unless split).
   const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
@@ -314,28 +321,36 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       gb.load(Bb, bn_s, n0, g.N, g.b_kfast, g.conj_b, tid);
     }
 #pragma unroll
-    for (int kq = 0; kq < BK / 4; ++kq) {
-      const int krow = kq * 4 + fk;
-      double a_re[TI], b_re[TJ], a_im[CPLX ? TI : 1], b_im[CPLX ? TJ : 1];
+    for (int ks = 0; ks < BK / 8; ++ks) {
+      double a_re[TI][4], b_re[TJ][2], a_im[CPLX ? TI : 1][4], na_im[CPLX ? TI : 1][4], b_im[CPLX ? TJ : 1][2];
 #pragma unroll
-      for (int i = 0; i < TI; ++i) {
-        a_re[i] = As[buf][0][krow * SA + wm0 + i * 8 + fr];
-        if (CPLX) a_im[i] = As[buf][NPL - 1][krow * SA + wm0 + i * 8 + fr];
-      }
+      for (int i = 0; i < TI; ++i)
 #pragma unroll
-      for (int j = 0; j < TJ; ++j) {
-        b_re[j] = Bs[buf][0][krow * SB + wn0 + j * 8 + fr];
-        if (CPLX) b_im[j] = Bs[buf][NPL - 1][krow * SB + wn0 + j * 8 + fr];
-      }
+        for (int r = 0; r < 4; ++r) {
+          const int idx = (ks * 8 + fk + 4 * (r >> 1)) * SA + wm0 + i * 16 + fr + 8 * (r & 1);
+          a_re[i][r] = As[buf][0][idx];
+          if (CPLX) {
+            a_im[i][r] = As[buf][NPL - 1][idx];
+            na_im[i][r] = -a_im[i][r];
+          }
+        }
+#pragma unroll
+      for (int j = 0; j < TJ; ++j)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int idx = (ks * 8 + fk + 4 * r) * SB + wn0 + j * 8 + fr;
+          b_re[j][r] = Bs[buf][0][idx];
+          if (CPLX) b_im[j][r] = Bs[buf][NPL - 1][idx];
+        }
 #pragma unroll
       for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int j = 0; j < TJ; ++j) {
-          dmma_884(cr[i][j][0], cr[i][j][1], a_re[i], b_re[j]);
+          dmma_1688(cr[i][j], a_re[i], b_re[j]);
           if (CPLX) {
-            dmma_884(cr[i][j][0], cr[i][j][1], -a_im[i], b_im[j]);
-            dmma_884(ci[i][j][0], ci[i][j][1], a_re[i], b_im[j]);
-            dmma_884(ci[i][j][0], ci[i][j][1], a_im[i], b_re[j]);
+            dmma_1688(cr[i][j], na_im[i], b_im[j]);
+            dmma_1688(ci[i][j], a_re[i], b_im[j]);
+            dmma_1688(ci[i][j], a_im[i], b_re[j]);
           }
         }
     }
@@ -353,15 +368,14 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
   const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
   T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
 #pragma unroll
-  for (int i = 0; i < TI; ++i) {
-    const int rr = wm0 + i * 8 + fr;
-    if (m0 + rr >= g.M) continue;
+  for (int i = 0; i < TI; ++i)
 #pragma unroll
     for (int j = 0; j < TJ; ++j)
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int cc = wn0 + j * 8 + fk * 2 + q;
-        if (n0 + cc >= g.N) continue;
+      for (int q = 0; q < 4; ++q) {
+        const int rr = wm0 + i * 16 + fr + 8 * (q >> 1);
+        const int cc = wn0 + j * 8 + fk * 2 + (q & 1);
+        if (m0 + rr >= g.M || n0 + cc >= g.N) continue;
         if (g.partial)
           Elem<double, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
                                     cr[i][j][q], CPLX ? ci[i][j][q] : 0.0);
@@ -369,7 +383,6 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
           epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
                                      Db + dm_s[rr] + dn_s[cc]);
       }
-  }
 }
 
 // One CTA per (batch, M tile, N tile).

@@ -19,55 +19,76 @@ namespace dev {
 namespace {
 
 // Gather of one ROWS x BK tile (A': rows = m; B': rows = n) into registers,
-// then into planar shared memory laid out [k][row]. The k-scatter offsets of a
-// tile are fetched one tile ahead of its elements (load_idx), so an element
-// load never waits on the index load in front of it.
+// then into planar shared memory laid out [k][row]. Threads run along k when
+// k is the unit-stride index (kfast) and along the rows otherwise, so each
+// thread sees one fixed k (kfast) or one fixed row (otherwise) for all its
+// PER elements. Its offsets are therefore one fixed value plus one value per
+// element: kfast: the element's row offset (set once per tile, in var[]) plus
+// the stage's k offset (fixed); otherwise: the row offset (fixed, set once)
+// plus each element's k offset (var[], per stage). The k offsets of a stage
+// are fetched one stage ahead of its elements (load_idx), so an element load
+// never waits on the index load in front of it. INT64_MIN marks a row or k
+// outside the operand (the element reads as zero).
 template <class R, bool CPLX, int ROWS, int BK, int NT>
 struct TileGather {
   using T = typename Elem<R, CPLX>::type;
   static constexpr int PER = ROWS * BK / NT;
   static_assert(ROWS * BK % NT == 0, "tile must split evenly over threads");
+  static_assert(NT % BK == 0 && NT % ROWS == 0, "a thread keeps one k (kfast) or one row");
   R re[PER];
   R im[CPLX ? PER : 1];
-  int64_t koff[PER];  // k-scatter offsets of the tile whose elements load next
+  int64_t var[PER];  // kfast: row offsets; otherwise: k offsets of the next stage
+  int64_t fixed;     // kfast: k offset of the next stage; otherwise: the row offset
 
   __device__ static inline void coords(int idx, int kfast, int& kk, int& rr) {
     kk = kfast ? (idx % BK) : (idx / ROWS);
     rr = kfast ? (idx / BK) : (idx % ROWS);
   }
 
-  __device__ inline void load_idx(const int64_t* kscat, int64_t k0, int64_t K, int kfast, int tid) {
+  // Row offsets of this tile (rows_s: the tile's row scatter in shared memory).
+  __device__ inline void init(const int64_t* rows_s, int64_t row0, int64_t nrows, int kfast, int tid) {
+    if (kfast) {
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
+      for (int j = 0; j < PER; ++j) {
+        int kk, rr;
+        coords(tid + j * NT, 1, kk, rr);
+        var[j] = row0 + rr < nrows ? rows_s[rr] : INT64_MIN;
+      }
+    } else {
       int kk, rr;
-      coords(tid + j * NT, kfast, kk, rr);
-      const int64_t k = k0 + kk;
-      koff[j] = k < K ? __ldg(kscat + k) : INT64_MIN;
+      coords(tid, 0, kk, rr);
+      fixed = row0 + rr < nrows ? rows_s[rr] : INT64_MIN;
     }
   }
 
-  __device__ inline void load(const T* base, const int64_t* rows_s, int64_t row0, int64_t nrows, int kfast, int conj,
-                              int tid) {
+  __device__ inline void load_idx(const int64_t* kscat, int64_t k0, int64_t K, int kfast, int tid) {
+    if (kfast) {
+      int kk, rr;
+      coords(tid, 1, kk, rr);
+      const int64_t k = k0 + kk;
+      fixed = k < K ? __ldg(kscat + k) : INT64_MIN;
+    } else {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        int kk, rr;
+        coords(tid + j * NT, 0, kk, rr);
+        const int64_t k = k0 + kk;
+        var[j] = k < K ? __ldg(kscat + k) : INT64_MIN;
+      }
+    }
+  }
+
+  __device__ inline void load(const T* base, int conj) {
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-      int kk, rr;
-      coords(tid + j * NT, kfast, kk, rr);
-      const int64_t r = row0 + rr;
       R vr = R(0), vi = R(0);
-      if (r < nrows && koff[j] != INT64_MIN) {
-        Elem<R, CPLX>::load(base + rows_s[rr] + koff[j], vr, vi);
+      if (var[j] != INT64_MIN && fixed != INT64_MIN) {
+        Elem<R, CPLX>::load(base + var[j] + fixed, vr, vi);
         if (conj) vi = -vi;
       }
       re[j] = vr;
       if (CPLX) im[j] = vi;
     }
-  }
-
-  // Index-and-load in one step (used where latency hiding is not the issue).
-  __device__ inline void load(const T* base, const int64_t* rows_s, const int64_t* kscat, int64_t row0,
-                              int64_t nrows, int64_t k0, int64_t K, int kfast, int conj, int tid) {
-    load_idx(kscat, k0, K, kfast, tid);
-    load(base, rows_s, row0, nrows, kfast, conj, tid);
   }
 
   __device__ inline void store(R* s_re, R* s_im, int stride, int kfast, int tid) const {
@@ -139,8 +160,12 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
   const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
   const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
   const int64_t nt = (ke - kb + BK - 1) / BK;
-  ga.load(Ab, am_s, g.s.a_k, m0, g.M, kb, ke, g.a_kfast, g.conj_a, tid);
-  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, kb, ke, g.b_kfast, g.conj_b, tid);
+  ga.init(am_s, m0, g.M, g.a_kfast, tid);
+  gb.init(bn_s, n0, g.N, g.b_kfast, tid);
+  ga.load_idx(g.s.a_k, kb, ke, g.a_kfast, tid);
+  gb.load_idx(g.s.b_k, kb, ke, g.b_kfast, tid);
+  ga.load(Ab, g.conj_a);
+  gb.load(Bb, g.conj_b);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
   if (nt > 1) {
@@ -152,8 +177,8 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
   for (int64_t t = 0; t < nt; ++t) {
     const int buf = (int)(t & 1);
     if (t + 1 < nt) {
-      ga.load(Ab, am_s, m0, g.M, g.a_kfast, g.conj_a, tid);
-      gb.load(Bb, bn_s, n0, g.N, g.b_kfast, g.conj_b, tid);
+      ga.load(Ab, g.conj_a);
+      gb.load(Bb, g.conj_b);
     }
     R acc_re[TM][TN], acc_im[CPLX ? TM : 1][CPLX ? TN : 1];
 #pragma unroll
@@ -303,8 +328,12 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
   const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
   const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
   const int64_t nt = (ke - kb + BK - 1) / BK;
-  ga.load(Ab, am_s, g.s.a_k, m0, g.M, kb, ke, g.a_kfast, g.conj_a, tid);
-  gb.load(Bb, bn_s, g.s.b_k, n0, g.N, kb, ke, g.b_kfast, g.conj_b, tid);
+  ga.init(am_s, m0, g.M, g.a_kfast, tid);
+  gb.init(bn_s, n0, g.N, g.b_kfast, tid);
+  ga.load_idx(g.s.a_k, kb, ke, g.a_kfast, tid);
+  gb.load_idx(g.s.b_k, kb, ke, g.b_kfast, tid);
+  ga.load(Ab, g.conj_a);
+  gb.load(Bb, g.conj_b);
   ga.store(As[0][0], As[0][NPL - 1], SA, g.a_kfast, tid);
   gb.store(Bs[0][0], Bs[0][NPL - 1], SB, g.b_kfast, tid);
   if (nt > 1) {
@@ -317,8 +346,8 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
   for (int64_t t = 0; t < nt; ++t) {
     const int buf = (int)(t & 1);
     if (t + 1 < nt) {
-      ga.load(Ab, am_s, m0, g.M, g.a_kfast, g.conj_a, tid);
-      gb.load(Bb, bn_s, n0, g.N, g.b_kfast, g.conj_b, tid);
+      ga.load(Ab, g.conj_a);
+      gb.load(Bb, g.conj_b);
     }
 #pragma unroll
     for (int ks = 0; ks < BK / 8; ++ks) {
@@ -409,7 +438,7 @@ __global__ void __launch_bounds__(128, 3) dmma_gemm_kernel(GemmArgs g) {
 // of range sets STATUS_BAD_ARGUMENT (or STATUS_WAIT_TIMEOUT) in the status
 // word and ends the CTA.
 template <class Tile, int NT>
-__global__ void __launch_bounds__(NT) grouped_kernel(const GroupItem* __restrict__ items,
+__global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const GroupItem* __restrict__ items,
                                                      const int64_t* __restrict__ tile_start, int nitems,
                                                      unsigned long long* counter, unsigned* status) {
   __shared__ __align__(16) GemmArgs sg;
@@ -461,6 +490,7 @@ __global__ void __launch_bounds__(NT) grouped_kernel(const GroupItem* __restrict
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 struct SimtTileOp {
   static constexpr int NT = (BM / TM) * (BN / TN);
+  static constexpr int MIN_BLOCKS = 1;
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
     simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
   }
@@ -468,6 +498,9 @@ struct SimtTileOp {
 template <bool CPLX, int WM, int WN, int BK>
 struct DmmaTileOp {
   static constexpr int NT = 128;
+  // Three resident CTAs per SM as dmma_gemm_kernel, except the f64 64 x 64
+  // tile, whose grouped loop would spill at that register budget.
+  static constexpr int MIN_BLOCKS = (!CPLX && WM == 32) ? 2 : 3;
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
     dmma_tile<CPLX, WM, WN, BK>(g, h, mt, nt);
   }
@@ -649,41 +682,52 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
   *bm = *bn = 0;
 }
 
-// Loads the family's grouped kernel (module loading is lazy) so that the first
-// launch inside a stream capture does not have to.
+namespace {
+
+// Resident CTAs per SM of each grouped kernel (occupancy of the built code),
+// filled before any capture by prepare_grouped: the persistent grid must not
+// exceed what can be resident at once, or the CTAs beyond it start only when
+// others have drained the queue.
+int g_grouped_per_sm[8] = {};
+
+template <class Op>
+cudaError_t grouped_prepare_op(int kernel) {
+  int n = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_kernel<Op, Op::NT>, Op::NT, 0);
+  if (e != cudaSuccess) return e;
+  g_grouped_per_sm[kernel] = n > 0 ? n : 1;
+  return cudaSuccess;
+}
+
+template <class Op>
+void grouped_launch_op(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
+                       unsigned long long* counter, unsigned* status, int num_sms, cudaStream_t st) {
+  const int per_sm = g_grouped_per_sm[kernel] > 0 ? g_grouped_per_sm[kernel] : 1;
+  grouped_kernel<Op, Op::NT><<<num_sms * per_sm, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+}
+
+using GSimtF32L = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
+using GSimtF32S = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
+using GSimtC32 = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
+using GDmmaF64L = DmmaTileOp<false, 32, 32, 16>;
+using GDmmaF64S = DmmaTileOp<false, 16, 16, 16>;
+using GDmmaC64L = DmmaTileOp<true, 32, 16, 8>;
+using GDmmaC64S = DmmaTileOp<true, 16, 16, 8>;
+
+}  // namespace
+
+// Loads the family's grouped kernel (module loading is lazy) and records its
+// occupancy, so that the launch inside a stream capture needs neither.
 cudaError_t prepare_grouped(int kernel) {
-  cudaFuncAttributes fa;
   switch (kernel) {
-    case PLAIN_F32_SIMT_128x128: {
-      using Op = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_F32_SIMT_64x64: {
-      using Op = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_C32_SIMT_64x64: {
-      using Op = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_F64_DMMA_64x64: {
-      using Op = DmmaTileOp<false, 32, 32, 16>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_F64_DMMA_32x32: {
-      using Op = DmmaTileOp<false, 16, 16, 16>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_C64_DMMA_64x32: {
-      using Op = DmmaTileOp<true, 32, 16, 8>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    case PLAIN_C64_DMMA_32x32: {
-      using Op = DmmaTileOp<true, 16, 16, 8>;
-      return cudaFuncGetAttributes(&fa, grouped_kernel<Op, Op::NT>);
-    }
-    default:
-      return cudaErrorInvalidValue;
+    case PLAIN_F32_SIMT_128x128: return grouped_prepare_op<GSimtF32L>(kernel);
+    case PLAIN_F32_SIMT_64x64: return grouped_prepare_op<GSimtF32S>(kernel);
+    case PLAIN_C32_SIMT_64x64: return grouped_prepare_op<GSimtC32>(kernel);
+    case PLAIN_F64_DMMA_64x64: return grouped_prepare_op<GDmmaF64L>(kernel);
+    case PLAIN_F64_DMMA_32x32: return grouped_prepare_op<GDmmaF64S>(kernel);
+    case PLAIN_C64_DMMA_64x32: return grouped_prepare_op<GDmmaC64L>(kernel);
+    case PLAIN_C64_DMMA_32x32: return grouped_prepare_op<GDmmaC64S>(kernel);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -693,43 +737,28 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
   if (e != cudaSuccess) return e;
   if (nitems <= 0) return cudaSuccess;
   switch (kernel) {
-    case PLAIN_F32_SIMT_128x128: {
-      using Op = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_F32_SIMT_128x128:
+      grouped_launch_op<GSimtF32L>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_F32_SIMT_64x64: {
-      using Op = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_F32_SIMT_64x64:
+      grouped_launch_op<GSimtF32S>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_C32_SIMT_64x64: {
-      using Op = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
-      grouped_kernel<Op, Op::NT><<<num_sms, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_C32_SIMT_64x64:
+      grouped_launch_op<GSimtC32>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_F64_DMMA_64x64: {
-      using Op = DmmaTileOp<false, 32, 32, 16>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 2, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_F64_DMMA_64x64:
+      grouped_launch_op<GDmmaF64L>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_F64_DMMA_32x32: {
-      using Op = DmmaTileOp<false, 16, 16, 16>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_F64_DMMA_32x32:
+      grouped_launch_op<GDmmaF64S>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_C64_DMMA_64x32: {
-      using Op = DmmaTileOp<true, 32, 16, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 3, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_C64_DMMA_64x32:
+      grouped_launch_op<GDmmaC64L>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    case PLAIN_C64_DMMA_32x32: {
-      using Op = DmmaTileOp<true, 16, 16, 8>;
-      grouped_kernel<Op, Op::NT><<<num_sms * 4, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+    case PLAIN_C64_DMMA_32x32:
+      grouped_launch_op<GDmmaC64S>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
-    }
-    default:
-      return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }

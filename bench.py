@@ -273,6 +273,102 @@ def c4_flops(items, complex_):
     return f * (8.0 if complex_ else 2.0)
 
 
+CORPUS_DT = {"f32": (0, "float32"), "f64": (1, "float64"), "c32": (2, "complex64"), "c64": (3, "complex128")}
+
+
+def corpus_entries():
+    """The reference's dot_general benchmark corpus as shapes (tests/golden/corpus.json)."""
+    with open(os.path.join(REPO, "tests", "golden", "corpus.json")) as f:
+        return json.load(f)["entries"]
+
+
+def corpus_dims(e):
+    """Batch H, free M and N, contracted K, and the flop count of one entry."""
+    a, b = e["a"]["dims"], e["b"]["dims"]
+    prod = lambda xs: int(np.prod(xs)) if len(xs) else 1
+    H = prod([a[i] for i in e["lb"]])
+    K = prod([a[i] for i in e["lc"]])
+    M = prod([a[i] for i in range(len(a)) if i not in e["lc"] and i not in e["lb"]])
+    N = prod([b[i] for i in range(len(b)) if i not in e["rc"] and i not in e["rb"]])
+    return H, M, N, K, (8.0 if e["dtype"][0] == "c" else 2.0) * H * M * N * K
+
+
+def corpus_case(tp, torch, e, seed):
+    """Plan (Problem::from_dot_general) and seeded device operands of one entry.
+    Returns (plan, tensors, origin pointers); negative strides are placed so
+    that every addressed element lies inside its buffer."""
+    code, npdt = CORPUS_DT[e["dtype"]]
+    tdt = getattr(torch, npdt)
+    cplx = e["dtype"][0] == "c"
+    spec = lambda side, conj: tp.OperandSpec(tp.LayoutSpec(list(e[side]["dims"]), list(e[side]["strides"])), conj)
+    prob = tp.Problem.from_dot_general(code, spec("a", bool(e["conj"][0])), spec("b", bool(e["conj"][1])),
+                                       spec("c", False), tp.DotGeneral(e["lc"], e["rc"], e["lb"], e["rb"]))
+    plan = tp.Plan(prob)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    bufs, ptrs = {}, {}
+    for side in ("a", "b", "c"):
+        dims, st = e[side]["dims"], e[side]["strides"]
+        lo = sum((d - 1) * s for d, s in zip(dims, st) if s < 0 and d > 0)
+        hi = sum((d - 1) * s for d, s in zip(dims, st) if s > 0 and d > 0)
+        span = max(hi - lo + 1, 1)
+        if side == "c":
+            t = torch.zeros(span, dtype=tdt, device="cuda")
+        else:
+            real = torch.float32 if e["dtype"] in ("f32", "c32") else torch.float64
+            t = torch.rand(span, dtype=real, device="cuda", generator=gen) * 2 - 1
+            if cplx:
+                t = torch.complex(t, torch.rand(span, dtype=real, device="cuda", generator=gen) * 2 - 1)
+        bufs[side] = (t, -lo)
+        ptrs[side] = t.data_ptr() + (-lo) * t.element_size()
+    return plan, bufs, ptrs
+
+
+def corpus_sampled_error(torch, e, bufs, n_samples=64, seed=0):
+    """Relative Frobenius error of n sampled outputs against float64 (complex128)
+    sums over the contracted index set, computed on the device."""
+    a_d, b_d, c_d = e["a"]["dims"], e["b"]["dims"], e["c"]["dims"]
+    sa, sb, sc = e["a"]["strides"], e["b"]["strides"], e["c"]["strides"]
+    lfree = [i for i in range(len(a_d)) if i not in e["lc"] and i not in e["lb"]]
+    rfree = [i for i in range(len(b_d)) if i not in e["rc"] and i not in e["rb"]]
+    # Offsets of every contracted multi-index in A and B.
+    ca = np.zeros(1, dtype=np.int64)
+    cb = np.zeros(1, dtype=np.int64)
+    for la, rb_ in zip(e["lc"], e["rc"]):
+        rng_ = np.arange(a_d[la], dtype=np.int64)
+        ca = (ca[:, None] + rng_[None, :] * sa[la]).ravel()
+        cb = (cb[:, None] + rng_[None, :] * sb[rb_]).ravel()
+    g = np.random.default_rng(seed)
+    idx = [g.integers(0, max(d, 1), size=n_samples) for d in c_d]  # D = [lhs free, rhs free, batch]
+    nl, nr = len(lfree), len(rfree)
+    off_a = np.zeros(n_samples, dtype=np.int64)
+    off_b = np.zeros(n_samples, dtype=np.int64)
+    off_c = np.zeros(n_samples, dtype=np.int64)
+    for p, i in enumerate(lfree):
+        off_a += idx[p] * sa[i]
+    for p, i in enumerate(rfree):
+        off_b += idx[nl + p] * sb[i]
+    for p, (la, rb_) in enumerate(zip(e["lb"], e["rb"])):
+        off_a += idx[nl + nr + p] * sa[la]
+        off_b += idx[nl + nr + p] * sb[rb_]
+    for p in range(len(c_d)):
+        off_c += idx[p] * sc[p]
+    (A, za), (B, zb), (D, zc) = bufs["a"], bufs["b"], bufs["c"]
+    wide = torch.complex128 if e["dtype"][0] == "c" else torch.float64
+    ia = torch.from_numpy(off_a[:, None] + ca[None, :] + za).cuda()
+    ib = torch.from_numpy(off_b[:, None] + cb[None, :] + zb).cuda()
+    av = torch.take(A, ia).to(wide)
+    bv = torch.take(B, ib).to(wide)
+    if e["conj"][0]:
+        av = av.conj()
+    if e["conj"][1]:
+        bv = bv.conj()
+    ref = (av * bv).sum(dim=1)
+    got = torch.take(D, torch.from_numpy(off_c + zc).cuda()).to(wide)
+    den = torch.linalg.norm(ref).item()
+    num = torch.linalg.norm(got - ref).item()
+    return num / den if den > 0 else num
+
+
 def run_config(args, tp, torch, ex):
     """Timing lines for the other configurations (parity-test cases in the test
     suite): C1 (f64, extents 24, beta 0.5), C3 (c64 batched, conj(A), batch
@@ -309,6 +405,32 @@ def run_config(args, tp, torch, ex):
 
     cfg = args.config
     out = {"config": cfg, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "unit": "TFLOP/s"}
+    if cfg == "corpus":
+        # The reference's dot_general corpus replayed through Problem::from_dot_general
+        # and execute_into (plain precision), seeded inputs; each entry timed alone.
+        rows, tot_f, tot_t = [], 0.0, 0.0
+        for i, e in enumerate(corpus_entries()):
+            plan, bufs, ptrs = corpus_case(tp, torch, e, 20261203 + 7000 + i)
+            fn = lambda: plan.execute_into(ex, 1.0, ptrs["a"], ptrs["b"], ptrs["c"])
+            H, M, N, K, flop = corpus_dims(e)
+            reps = max(2, min(args.steps, int(2e11 // max(flop, 1.0))))
+            ms, _ = timed(fn, reps, 2)
+            err = corpus_sampled_error(torch, e, bufs, seed=i)
+            calls = int(e.get("calls", 1) or 1)
+            tot_f += calls * flop
+            tot_t += calls * ms * 1e-3
+            rows.append({"name": e["name"], "file": e["file"], "dtype": e["dtype"], "H": H, "M": M, "N": N, "K": K,
+                         "ms": ms, "tflops": flop / (ms * 1e-3) / 1e12, "rel_err_sampled": err,
+                         "family": plan.report()["family"], "split_k": plan.report().get("split_k", 1)})
+            del bufs, plan
+            torch.cuda.empty_cache()
+        out["workload"] = (f"{len(rows)} dot_general entries of the reference's benchmark corpus (tests/golden/"
+                           "corpus.json), plain precision, seeded uniform inputs")
+        out["call_weighted_tflops"] = tot_f / tot_t / 1e12
+        out["worst_rel_err"] = max(r["rel_err_sampled"] for r in rows)
+        out["entries"] = rows
+        print(json.dumps(out), flush=True)
+        return
     # Pipe peaks measured on this GPU (register-only probe kernels), and the
     # INT8 tensor peak taken as twice the measured dense BF16 burst peak.
     peaks, peak_src = measured_peaks()
@@ -521,7 +643,7 @@ def main():
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus"],
                     help="c2 is the metric's workload; c1/c3/c5 print timing lines of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -414,18 +414,42 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       }
 }
 
-// One CTA per (batch, M tile, N tile).
+// Tile t of a one-launch contraction: N tile fastest, then M tile, then
+// z = split * H + h. A 1-D grid (looping when there are more tiles than
+// CTAs), so neither the batch count nor the M tile count is limited to the
+// 65535 of a grid's y and z dimensions.
+__device__ __forceinline__ void tile_coords(int64_t t, int64_t tn, int64_t tm, int64_t& nt, int64_t& mt,
+                                            int64_t& z) {
+  nt = t % tn;
+  mt = (t / tn) % tm;
+  z = t / (tn * tm);
+}
+
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(GemmArgs g) {
-  // blockIdx.z = split * H + h.
-  simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
+  const int64_t tn = (g.N + BN - 1) / BN, tm = (g.M + BM - 1) / BM;
+  const int64_t total = tn * tm * g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1);
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int64_t nt, mt, z;
+    tile_coords(t, tn, tm, nt, mt, z);
+    simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, z % g.H, mt, nt, z / g.H);
+    __syncthreads();  // the next tile rewrites the shared scatter arrays
+  }
 }
 
 // Three CTAs per SM (at most 170 registers a thread): twelve warps to hide the
 // gather and shared-memory latency around the DMMA pipe.
 template <bool CPLX, int WM, int WN, int BK>
 __global__ void __launch_bounds__(128, 3) dmma_gemm_kernel(GemmArgs g) {
-  dmma_tile<CPLX, WM, WN, BK>(g, blockIdx.z % g.H, blockIdx.y, blockIdx.x, blockIdx.z / g.H);
+  constexpr int BM = 2 * WM, BN = 2 * WN;
+  const int64_t tn = (g.N + BN - 1) / BN, tm = (g.M + BM - 1) / BM;
+  const int64_t total = tn * tm * g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1);
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int64_t nt, mt, z;
+    tile_coords(t, tn, tm, nt, mt, z);
+    dmma_tile<CPLX, WM, WN, BK>(g, z % g.H, mt, nt, z / g.H);
+    __syncthreads();  // the next tile rewrites the shared scatter arrays
+  }
 }
 
 // Persistent grouped kernel over a heterogeneous list (contract_batched): the
@@ -509,7 +533,8 @@ struct DmmaTileOp {
 template <int BM, int BN>
 dim3 grid_for(const GemmArgs& g) {
   const int64_t splits = g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1;
-  return dim3((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM), (unsigned)(g.H * splits));
+  const int64_t total = ((g.N + BN - 1) / BN) * ((g.M + BM - 1) / BM) * g.H * splits;
+  return dim3((unsigned)(total < 0x7fffffff ? total : 0x7fffffff));
 }
 
 }  // namespace
@@ -575,7 +600,6 @@ void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K,
     int64_t s = (2 * num_sms + t - 1) / t;
     s = s < K / min_chunk ? s : K / min_chunk;
     s = s < 64 ? s : 64;
-    while (s > 1 && H * s > 65535) --s;
     if (s > 1) {
       const int64_t chunk = ((K + s - 1) / s + 63) / 64 * 64;  // whole 64-deep blocks
       *kernel = k;
@@ -633,7 +657,6 @@ cudaError_t launch_splitk_reduce(int dtype, const GemmArgs& g, int splits, cudaS
 
 cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.H <= 0) return cudaSuccess;
-  if (g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1) > 65535) return cudaErrorInvalidConfiguration;
   switch (kernel) {
     case PLAIN_F32_SIMT_128x128:
       if (dtype != 0) return cudaErrorInvalidValue;

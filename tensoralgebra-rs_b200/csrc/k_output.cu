@@ -6,6 +6,8 @@
 // (crates/tprims-kernel/src/pack/writeback.rs:495-550): beta == 0 writes zeros
 // without reading C. Memory-bound: one pass over D (and C), threads running
 // along whichever output index is unit-stride.
+#include <climits>
+
 #include "device_common.cuh"
 
 namespace tprims {
@@ -56,6 +58,63 @@ cudaError_t launch_output_pass(int dtype, const GemmArgs& g, cudaStream_t st) {
     case 1: output_pass_kernel<double, false><<<blocks, 256, 0, st>>>(g); break;
     case 2: output_pass_kernel<float, true><<<blocks, 256, 0, st>>>(g); break;
     case 3: output_pass_kernel<double, true><<<blocks, 256, 0, st>>>(g); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// Batches of tiny products (the all-batch / elementwise shapes: M N K <= 256,
+// e.g. a Hadamard product with M = N = K = 1): one thread per output element,
+// the batch index fastest (it is usually the unit-stride one), the K sum in
+// registers, then the epilogue. A batch scatter vector that is an arithmetic
+// sequence from 0 is replaced by its stride (INT64_MIN marks one that is not),
+// so the kernel reads only operand data. HBM-bound: A, B (and C) read once, D written once.
+template <class R, bool CPLX>
+__global__ void __launch_bounds__(256) tiny_batched_kernel(GemmArgs g, TinyStrides hs) {
+  using T = typename Elem<R, CPLX>::type;
+  const int64_t total = g.M * g.N * g.H;
+  const T* A = static_cast<const T*>(g.A);
+  const T* B = static_cast<const T*>(g.B);
+  const T* C = static_cast<const T*>(g.C);
+  T* D = static_cast<T*>(g.D);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t h = i % g.H, mn = i / g.H, m = mn % g.M, n = mn / g.M;
+    const int64_t ha = hs.a != INT64_MIN ? h * hs.a : g.s.h_a[h];
+    const int64_t hb = hs.b != INT64_MIN ? h * hs.b : g.s.h_b[h];
+    const int64_t hd = hs.d != INT64_MIN ? h * hs.d : g.s.h_d[h];
+    const T* ar = A + ha + g.s.a_m[m];
+    const T* bc = B + hb + g.s.b_n[n];
+    R sr = R(0), si = R(0);
+    for (int64_t k = 0; k < g.K; ++k) {
+      R xr, xi, yr, yi;
+      Elem<R, CPLX>::load(ar + g.s.a_k[k], xr, xi);
+      Elem<R, CPLX>::load(bc + g.s.b_k[k], yr, yi);
+      if (CPLX) {
+        if (g.conj_a) xi = -xi;
+        if (g.conj_b) yi = -yi;
+        sr = fma(xr, yr, sr);
+        sr = fma(-xi, yi, sr);
+        si = fma(xr, yi, si);
+        si = fma(xi, yr, si);
+      } else {
+        sr = fma(xr, yr, sr);
+      }
+    }
+    const T* c = C + (g.e.beta_zero ? 0 : (hs.c != INT64_MIN ? h * hs.c : g.s.h_c[h]) + g.s.c_m[m] + g.s.c_n[n]);
+    epilogue_store<R, CPLX>(g.e, sr, si, c, D + hd + g.s.d_m[m] + g.s.d_n[n]);
+  }
+}
+
+cudaError_t launch_tiny_batched(int dtype, const GemmArgs& g, const TinyStrides& hs, int num_sms, cudaStream_t st) {
+  const int64_t total = g.M * g.N * g.H;
+  if (total <= 0) return cudaSuccess;
+  const int64_t want = (total + 255) / 256;
+  const unsigned blocks = (unsigned)(want < (int64_t)num_sms * 16 ? want : (int64_t)num_sms * 16);
+  switch (dtype) {
+    case 0: tiny_batched_kernel<float, false><<<blocks, 256, 0, st>>>(g, hs); break;
+    case 1: tiny_batched_kernel<double, false><<<blocks, 256, 0, st>>>(g, hs); break;
+    case 2: tiny_batched_kernel<float, true><<<blocks, 256, 0, st>>>(g, hs); break;
+    case 3: tiny_batched_kernel<double, true><<<blocks, 256, 0, st>>>(g, hs); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -93,6 +93,18 @@ cudaError_t launch_fill_zero(size_t elem, void* origin, int rank, const int64_t*
 const char* plain_kernel_name(int kernel);
 // The family the autotuner would pick for a shape (no launch).
 int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
+// Batches of tiny products: per-operand batch strides when the batch scatter
+// vector is an arithmetic sequence from 0, else INT64_MIN (the vector is read).
+struct TinyStrides {
+  int64_t a, b, c, d;
+};
+// Whether a shape takes the tiny batched kernel (M N K <= 256 and a batch of
+// at least 64).
+inline bool use_tiny_batched(int64_t M, int64_t N, int64_t K, int64_t H) {
+  return M * N * K <= 256 && H >= 64;
+}
+cudaError_t launch_tiny_batched(int dtype, const GemmArgs& g, const TinyStrides& hs, int num_sms, cudaStream_t st);
+
 // Family of an item inside a grouped launch (the list fills the GPU).
 int choose_grouped_kernel(int dtype, int64_t M, int64_t N);
 // One-launch choice with split-K: the family (or `pinned`) and the number of

@@ -2,6 +2,7 @@
 #include "runtime.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <chrono>
 #include <thread>
@@ -100,9 +101,22 @@ namespace {
 std::atomic<uint64_t> g_product_uid{1};
 }
 
+namespace {
+// The stride of a scatter vector that is an arithmetic sequence from 0, else INT64_MIN.
+int64_t sequence_stride(const std::vector<int64_t>& v) {
+  if (v.empty() || v[0] != 0) return INT64_MIN;
+  const int64_t s = v.size() > 1 ? v[1] : 0;
+  for (size_t i = 1; i < v.size(); ++i)
+    if (v[i] != (int64_t)i * s) return INT64_MIN;
+  return s;
+}
+}  // namespace
+
 Product::Product(const Problem& p) : problem(p), uid(g_product_uid.fetch_add(1)) {
   packed = PackedPlan::from_problem(p);
   view = orient(packed, packed.transposes_gemm(32));
+  tiny_h = dev::TinyStrides{sequence_stride(view.h_a), sequence_stride(view.h_b), sequence_stride(view.h_c),
+                            sequence_stride(view.h_d)};
 }
 
 Product::~Product() {
@@ -193,7 +207,9 @@ std::string Product::report() const {
   int64_t chunk = 0;
   dev::choose_plain_launch((int)problem.dtype, kernel_pin, view.M, view.N, view.K, view.H, 148, &kernel, &splits,
                            &chunk);
-  std::string family = scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
+  const bool tiny = scheme == Scheme::Plain && !kernel_pin && dev::use_tiny_batched(view.M, view.N, view.K, view.H);
+  std::string family = tiny ? std::string("sm100.") + dtype_name(problem.dtype) + ".tiny-batched"
+                       : scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
                        : scheme == Scheme::Bf16x3 ? "sm100.f32.tcgen05.bf16x3.128x256x32"
                        : scheme == Scheme::Bf16x6 ? "sm100.f32.tcgen05.bf16x6.128x256x32"
                                                   : std::string("sm100.") + dtype_name(problem.dtype) +
@@ -206,7 +222,7 @@ std::string Product::report() const {
     << ",\"h_axes\":" << axes_json(st.h_axes) << ",\"swapped\":" << (view.swapped ? "true" : "false")
     << ",\"a_kfast\":" << (view.a_kfast ? "true" : "false") << ",\"b_kfast\":" << (view.b_kfast ? "true" : "false")
     << ",\"d_mfast\":" << (view.d_mfast ? "true" : "false") << ",\"scheme\":\"" << scheme_name(scheme)
-    << "\",\"family\":\"" << family << "\",\"split_k\":" << (scheme == Scheme::Plain ? splits : 1)
+    << "\",\"family\":\"" << family << "\",\"split_k\":" << (scheme == Scheme::Plain && !tiny ? splits : 1)
     << ",\"tail_parts\":"
     << ((scheme == Scheme::Bf16x3 || scheme == Scheme::Bf16x6)
             ? dev::split_tail_parts(dev::split_layout((int)scheme, view.M, view.N, view.K, view.H), 148)
@@ -358,6 +374,11 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
   }
   switch (pr.scheme) {
     case Scheme::Plain: {
+      if (!pr.kernel_pin && dev::use_tiny_batched(g.M, g.N, g.K, g.H)) {
+        Timed t(ex, "tiny_batched");
+        check_cuda(dev::launch_tiny_batched(dt, g, pr.tiny_h, ex.num_sms, ex.stream), "tiny batched launch");
+        return;
+      }
       int k = 0, splits = 1;
       int64_t chunk = 0;
       dev::choose_plain_launch(dt, pr.kernel_pin, g.M, g.N, g.K, g.H, ex.num_sms, &k, &splits, &chunk);
@@ -442,6 +463,7 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
 size_t scheme_scratch(const Product& pr, int num_sms) {
   const auto& v = pr.view;
   if (pr.scheme == Scheme::Plain) {
+    if (!pr.kernel_pin && dev::use_tiny_batched(v.M, v.N, v.K, v.H)) return 0;
     int k = 0, splits = 1;
     int64_t chunk = 0;
     dev::choose_plain_launch((int)pr.problem.dtype, pr.kernel_pin, v.M, v.N, v.K, v.H, num_sms, &k, &splits, &chunk);
@@ -639,6 +661,7 @@ bool groupable(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item&
   const Problem& p = pr.problem;
   if (pr.scheme != Scheme::Plain || p.out_empty || p.k_empty || alpha.is_zero()) return false;
   if (pr.view.H > 65535) return false;
+  if (!pr.kernel_pin && dev::use_tiny_batched(pr.view.M, pr.view.N, pr.view.K, pr.view.H)) return false;
   const bool c_read = it.c != nullptr && !beta.is_zero();
   const void* ptrs[4] = {it.a, it.b, c_read ? it.c : nullptr, it.d};
   for (const void* q : ptrs)

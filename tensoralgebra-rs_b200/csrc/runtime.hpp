@@ -92,6 +92,8 @@ struct Product {
   Scheme scheme = Scheme::Plain;
   int ozaki_slices = 0;
   int kernel_pin = 0;
+  // Batch strides of the oriented view for the tiny batched kernel.
+  dev::TinyStrides tiny_h{};
   // Unique over the process lifetime (never reused, unlike the address), so a
   // cached grouped graph can never be replayed for a newer plan.
   const uint64_t uid;

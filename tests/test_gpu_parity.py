@@ -297,6 +297,36 @@ def test_c1_full_size_f64(tp, ex, torch_cuda, orc):
     assert orc.rel_frobenius(got, want) <= 1e-13
 
 
+# ----------------------------------------------------------------- tiny batches
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("shape", [(1, 1, 1, (12, 11)), (2, 3, 5, (10, 9)), (4, 1, 16, (70,))],
+                         ids=["hadamard", "small", "vecmat"])
+def test_tiny_batched_products(tp, ex, torch_cuda, orc, dt, shape):
+    """Batches of tiny products (M N K <= 256) take the one-thread-per-output
+    kernel: batch axes folded or not (B's two batch axes are transposed, so
+    its batch scatter is not a sequence), conjugation, alpha, beta and C."""
+    m, n, k, hb = shape
+    rng = np.random.default_rng(55)
+    cplx = dt.startswith("complex")
+    h = int(np.prod(hb))
+    hl = list(range(10, 10 + len(hb)))
+    # A[batch..., m, k] batch-first; B[k, n, batch reversed]; C, D [m, n, batch...]
+    ea = list(hb) + [m, k]
+    A = Op(rnd(rng, dt, h * m * k), ea, layout(ea, rng, permute=False)[1], hl + [0, 2], conj=cplx)
+    eb = [k, n] + list(reversed(hb))
+    B = Op(rnd(rng, dt, h * k * n), eb, layout(eb, rng, permute=False)[1], [2, 1] + list(reversed(hl)))
+    ed = [m, n] + list(hb)
+    C = Op(rnd(rng, dt, h * m * n), ed, layout(ed, rng, permute=True)[1], [0, 1] + hl)
+    d0 = rnd(rng, dt, h * m * n)
+    D = Op(d0, ed, layout(ed, rng, permute=False)[1], [0, 1] + hl)
+    al, be = (complex(0.5, 0.25), complex(-1.0, 0.5)) if cplx else (1.5, -0.75)
+    want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
+    st, got, p = run(tp, ex, torch_cuda, dt, A, B, C, D, al, be)
+    assert st == 0, tp.last_error()
+    assert "tiny-batched" in p.report()["family"], p.report()
+    assert orc.rel_frobenius(got, want) <= plain_tol(dt)
+
+
 # ----------------------------------------------------------------- split-K
 @pytest.mark.parametrize("dt", DTYPES)
 def test_split_k_on_deep_contractions_with_few_tiles(tp, ex, torch_cuda, orc, dt):

@@ -263,6 +263,8 @@ __device__ __forceinline__ void simt_tile(const GemmArgs& g, int64_t h, int64_t 
 
 // ---------------------------------------------------------------- FP64 DMMA
 
+__device__ __forceinline__ uint32_t smem_addr_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
 // D (16 x 8) += A (16 x 8, row) B (8 x 8, col) in FP64. Fragments, with
 // g = lane / 4 and t = lane % 4: a[r] = A[g + 8 (r % 2)][t + 4 (r / 2)],
 // b[r] = B[t + 4 r][g], d[r] = D[g + 8 (r / 2)][2 t + r % 2].
@@ -273,9 +275,247 @@ __device__ inline void dmma_1688(double (&d)[4], const double (&a)[4], const dou
                : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// 4 warps in a 2x2 arrangement, each warp a WM x WN tile of 16x8 DMMA tiles.
+// Asynchronous gather of one ROWS x BK FP64 tile (planar for complex) into a
+// shared-memory stage: the same per-thread offsets as TileGather (one fixed
+// offset and one per element), but each element goes straight from global to
+// shared memory with cp.async (8 bytes; an element outside the operand is
+// zero-filled by a zero source size), so several stages can be in flight
+// without holding them in registers. Conjugation is applied when fragments
+// are read.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_addr_u32(smem)), "l"(gmem),
+               "r"(ok ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <bool CPLX, int ROWS, int BK, int NT>
+struct AsyncGather {
+  using T = typename Elem<double, CPLX>::type;
+  static constexpr int PER = ROWS * BK / NT;
+  static_assert(ROWS * BK % NT == 0 && NT % BK == 0 && NT % ROWS == 0, "one k or one row per thread");
+  int64_t var[PER];
+  int64_t fixed;
+
+  __device__ static inline void coords(int idx, int kfast, int& kk, int& rr) {
+    kk = kfast ? (idx % BK) : (idx / ROWS);
+    rr = kfast ? (idx / BK) : (idx % ROWS);
+  }
+  __device__ inline void init(const int64_t* rows_s, int64_t row0, int64_t nrows, int kfast, int tid) {
+    if (kfast) {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        int kk, rr;
+        coords(tid + j * NT, 1, kk, rr);
+        var[j] = row0 + rr < nrows ? rows_s[rr] : INT64_MIN;
+      }
+    } else {
+      int kk, rr;
+      coords(tid, 0, kk, rr);
+      fixed = row0 + rr < nrows ? rows_s[rr] : INT64_MIN;
+    }
+  }
+  __device__ inline void load_idx(const int64_t* kscat, int64_t k0, int64_t K, int kfast, int tid) {
+    if (kfast) {
+      int kk, rr;
+      coords(tid, 1, kk, rr);
+      const int64_t k = k0 + kk;
+      fixed = k < K ? __ldg(kscat + k) : INT64_MIN;
+    } else {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        int kk, rr;
+        coords(tid + j * NT, 0, kk, rr);
+        const int64_t k = k0 + kk;
+        var[j] = k < K ? __ldg(kscat + k) : INT64_MIN;
+      }
+    }
+  }
+  // Copies of this thread's elements of the stage whose offsets are loaded.
+  __device__ inline void issue(const T* base, double* s_re, double* s_im, int stride, int kfast, int tid) const {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      int kk, rr;
+      coords(tid + j * NT, kfast, kk, rr);
+      const bool ok = var[j] != INT64_MIN && fixed != INT64_MIN;
+      const T* src = ok ? base + var[j] + fixed : base;  // not read when !ok
+      const double* d = reinterpret_cast<const double*>(src);
+      cp_async8(s_re + kk * stride + rr, d, ok);
+      if (CPLX) cp_async8(s_im + kk * stride + rr, d + 1, ok);
+    }
+  }
+};
+
+// Shape of the DMMA stage ring (dynamic shared memory, see dmma_tile).
 template <bool CPLX, int WM, int WN, int BK>
-__device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+struct DmmaRing {
+  static constexpr int BM = 2 * WM, BN = 2 * WN;
+  static constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
+  static constexpr int NPL = CPLX ? 2 : 1;
+  static constexpr int STAGES = 4;
+  static constexpr int A_STAGE = NPL * BK * SA, B_STAGE = NPL * BK * SB;  // doubles
+  static constexpr int BYTES = STAGES * (A_STAGE + B_STAGE) * 8;
+};
+
+// Asynchronous variant (used for complex): 4 warps in a 2x2 arrangement, each
+// warp a WM x WN tile of 16x8 DMMA tiles, fed by a ring of STAGES
+// shared-memory stages (dynamic shared memory of DmmaRing::BYTES) filled with
+// cp.async.
+template <bool CPLX, int WM, int WN, int BK>
+__device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                          int64_t split = 0) {
+  using Ring = DmmaRing<CPLX, WM, WN, BK>;
+  constexpr int BM = Ring::BM, BN = Ring::BN, NT = 128;
+  constexpr int SA = Ring::SA, SB = Ring::SB;
+  constexpr int NPL = Ring::NPL;
+  constexpr int STAGES = Ring::STAGES;
+  constexpr int TI = WM / 16, TJ = WN / 8;
+  static_assert(WM % 16 == 0 && WN % 8 == 0 && BK % 8 == 0, "m16n8k8 fragments");
+  using T = typename Elem<double, CPLX>::type;
+
+  extern __shared__ __align__(16) double dmma_ring[];
+  double(*As)[NPL][BK * SA] = reinterpret_cast<double(*)[NPL][BK * SA]>(dmma_ring);
+  double(*Bs)[NPL][BK * SB] = reinterpret_cast<double(*)[NPL][BK * SB]>(dmma_ring + STAGES * Ring::A_STAGE);
+  __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t m0 = mtile * BM, n0 = ntile * BN;
+  const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
+
+  for (int i = tid; i < BM; i += NT) {
+    const int64_t m = m0 + i;
+    const bool ok = m < g.M;
+    am_s[i] = ok ? g.s.a_m[m] : 0;
+    dm_s[i] = ok ? g.s.d_m[m] : 0;
+    cm_s[i] = ok ? g.s.c_m[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int64_t n = n0 + i;
+    const bool ok = n < g.N;
+    bn_s[i] = ok ? g.s.b_n[n] : 0;
+    dn_s[i] = ok ? g.s.d_n[n] : 0;
+    cn_s[i] = ok ? g.s.c_n[n] : 0;
+  }
+  __syncthreads();
+
+  const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
+  const T* Bb = static_cast<const T*>(g.B) + g.s.h_b[h];
+  AsyncGather<CPLX, BM, BK, NT> ga;
+  AsyncGather<CPLX, BN, BK, NT> gb;
+
+  double cr[TI][TJ][4], ci[CPLX ? TI : 1][CPLX ? TJ : 1][4];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int j = 0; j < TJ; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        cr[i][j][q] = 0.0;
+        if (CPLX) ci[i][j][q] = 0.0;
+      }
+
+  // This CTA's K range (the whole of K unless split).
+  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
+  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
+  const int64_t nt = (ke - kb + BK - 1) / BK;
+  ga.init(am_s, m0, g.M, g.a_kfast, tid);
+  gb.init(bn_s, n0, g.N, g.b_kfast, tid);
+  // Prologue: stages 0 .. STAGES-2 in flight (one commit group each, empty
+  // groups past the end keep the count uniform).
+#pragma unroll
+  for (int sidx = 0; sidx < STAGES - 1; ++sidx) {
+    if (sidx < nt) {
+      ga.load_idx(g.s.a_k, kb + sidx * BK, ke, g.a_kfast, tid);
+      gb.load_idx(g.s.b_k, kb + sidx * BK, ke, g.b_kfast, tid);
+      ga.issue(Ab, As[sidx][0], As[sidx][NPL - 1], SA, g.a_kfast, tid);
+      gb.issue(Bb, Bs[sidx][0], Bs[sidx][NPL - 1], SB, g.b_kfast, tid);
+    }
+    cp_async_commit();
+  }
+
+  const double sa = g.conj_a ? -1.0 : 1.0, sb = g.conj_b ? -1.0 : 1.0;
+  const int fr = lane >> 2, fk = lane & 3;
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t tp = t + STAGES - 1;  // the stage issued in this iteration
+    if (tp < nt) {
+      ga.load_idx(g.s.a_k, kb + tp * BK, ke, g.a_kfast, tid);
+      gb.load_idx(g.s.b_k, kb + tp * BK, ke, g.b_kfast, tid);
+    }
+    cp_async_wait<STAGES - 2>();  // this thread's copies of stage t have landed
+    __syncthreads();              // everyone's have; and stage t-1's buffer is free
+    if (tp < nt) {
+      const int pb = (int)(tp % STAGES);
+      ga.issue(Ab, As[pb][0], As[pb][NPL - 1], SA, g.a_kfast, tid);
+      gb.issue(Bb, Bs[pb][0], Bs[pb][NPL - 1], SB, g.b_kfast, tid);
+    }
+    cp_async_commit();
+    const int buf = (int)(t % STAGES);
+#pragma unroll
+    for (int ks = 0; ks < BK / 8; ++ks) {
+      double a_re[TI][4], b_re[TJ][2], a_im[CPLX ? TI : 1][4], na_im[CPLX ? TI : 1][4], b_im[CPLX ? TJ : 1][2];
+#pragma unroll
+      for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int idx = (ks * 8 + fk + 4 * (r >> 1)) * SA + wm0 + i * 16 + fr + 8 * (r & 1);
+          a_re[i][r] = As[buf][0][idx];
+          if (CPLX) {
+            a_im[i][r] = sa * As[buf][NPL - 1][idx];
+            na_im[i][r] = -a_im[i][r];
+          }
+        }
+#pragma unroll
+      for (int j = 0; j < TJ; ++j)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int idx = (ks * 8 + fk + 4 * r) * SB + wn0 + j * 8 + fr;
+          b_re[j][r] = Bs[buf][0][idx];
+          if (CPLX) b_im[j][r] = sb * Bs[buf][NPL - 1][idx];
+        }
+#pragma unroll
+      for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) {
+          dmma_1688(cr[i][j], a_re[i], b_re[j]);
+          if (CPLX) {
+            dmma_1688(cr[i][j], na_im[i], b_im[j]);
+            dmma_1688(ci[i][j], a_re[i], b_im[j]);
+            dmma_1688(ci[i][j], a_im[i], b_re[j]);
+          }
+        }
+    }
+  }
+  cp_async_wait<0>();  // no copy may still target the ring when the next tile starts
+
+  const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
+  T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int j = 0; j < TJ; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int rr = wm0 + i * 16 + fr + 8 * (q >> 1);
+        const int cc = wn0 + j * 8 + fk * 2 + (q & 1);
+        if (m0 + rr >= g.M || n0 + cc >= g.N) continue;
+        if (g.partial)
+          Elem<double, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
+                                    cr[i][j][q], CPLX ? ci[i][j][q] : 0.0);
+        else
+          epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
+                                     Db + dm_s[rr] + dn_s[cc]);
+      }
+}
+
+// Register-staged variant (used for real f64): 4 warps in a 2x2 arrangement,
+// each warp a WM x WN tile of 16x8 DMMA tiles, two shared-memory stages, the
+// next stage's elements held in registers (TileGather).
+template <bool CPLX, int WM, int WN, int BK>
+__device__ __forceinline__ void dmma_tile_regs(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
                                           int64_t split = 0) {
   constexpr int BM = 2 * WM, BN = 2 * WN, NT = 128;
   constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
@@ -414,6 +654,23 @@ __device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t 
       }
 }
 
+// The DMMA tile body: measured on B200, the cp.async ring is faster for the
+// planar complex tiles and the register-staged path for real f64.
+template <bool CPLX, int WM, int WN, int BK>
+__device__ __forceinline__ void dmma_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                          int64_t split = 0) {
+  if constexpr (CPLX)
+    dmma_tile_async<CPLX, WM, WN, BK>(g, h, mtile, ntile, split);
+  else
+    dmma_tile_regs<CPLX, WM, WN, BK>(g, h, mtile, ntile, split);
+}
+
+// Dynamic shared memory of a DMMA tile body.
+template <bool CPLX, int WM, int WN, int BK>
+constexpr int dmma_dyn_smem() {
+  return CPLX ? DmmaRing<CPLX, WM, WN, BK>::BYTES : 0;
+}
+
 // Tile t of a one-launch contraction: N tile fastest, then M tile, then
 // z = split * H + h. A 1-D grid (looping when there are more tiles than
 // CTAs), so neither the batch count nor the M tile count is limited to the
@@ -514,6 +771,7 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
 template <class R, bool CPLX, int BM, int BN, int BK, int TM, int TN>
 struct SimtTileOp {
   static constexpr int NT = (BM / TM) * (BN / TN);
+  static constexpr int SMEM = 0;
   static constexpr int MIN_BLOCKS = 1;
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
     simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
@@ -522,6 +780,7 @@ struct SimtTileOp {
 template <bool CPLX, int WM, int WN, int BK>
 struct DmmaTileOp {
   static constexpr int NT = 128;
+  static constexpr int SMEM = dmma_dyn_smem<CPLX, WM, WN, BK>();
   // Three resident CTAs per SM as dmma_gemm_kernel, except the f64 64 x 64
   // tile, whose grouped loop would spill at that register budget.
   static constexpr int MIN_BLOCKS = (!CPLX && WM == 32) ? 2 : 3;
@@ -655,6 +914,20 @@ cudaError_t launch_splitk_reduce(int dtype, const GemmArgs& g, int splits, cudaS
   return cudaGetLastError();
 }
 
+namespace {
+template <bool CPLX, int WM, int WN, int BK>
+cudaError_t launch_dmma(const GemmArgs& g, cudaStream_t st) {
+  constexpr int bytes = dmma_dyn_smem<CPLX, WM, WN, BK>();
+  if (bytes > 0) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(dmma_gemm_kernel<CPLX, WM, WN, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  dmma_gemm_kernel<CPLX, WM, WN, BK><<<grid_for<2 * WM, 2 * WN>(g), 128, bytes, st>>>(g);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.H <= 0) return cudaSuccess;
   switch (kernel) {
@@ -672,20 +945,16 @@ cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStre
       break;
     case PLAIN_F64_DMMA_64x64:
       if (dtype != 1) return cudaErrorInvalidValue;
-      dmma_gemm_kernel<false, 32, 32, 16><<<grid_for<64, 64>(g), 128, 0, st>>>(g);
-      break;
+      return launch_dmma<false, 32, 32, 16>(g, st);
     case PLAIN_F64_DMMA_32x32:
       if (dtype != 1) return cudaErrorInvalidValue;
-      dmma_gemm_kernel<false, 16, 16, 16><<<grid_for<32, 32>(g), 128, 0, st>>>(g);
-      break;
+      return launch_dmma<false, 16, 16, 16>(g, st);
     case PLAIN_C64_DMMA_64x32:
       if (dtype != 3) return cudaErrorInvalidValue;
-      dmma_gemm_kernel<true, 32, 16, 8><<<grid_for<64, 32>(g), 128, 0, st>>>(g);
-      break;
+      return launch_dmma<true, 32, 16, 8>(g, st);
     case PLAIN_C64_DMMA_32x32:
       if (dtype != 3) return cudaErrorInvalidValue;
-      dmma_gemm_kernel<true, 16, 16, 8><<<grid_for<32, 32>(g), 128, 0, st>>>(g);
-      break;
+      return launch_dmma<true, 16, 16, 8>(g, st);
     default:
       return cudaErrorInvalidValue;
   }
@@ -715,8 +984,13 @@ int g_grouped_per_sm[8] = {};
 
 template <class Op>
 cudaError_t grouped_prepare_op(int kernel) {
+  if (Op::SMEM > 0) {
+    const cudaError_t a =
+        cudaFuncSetAttribute(grouped_kernel<Op, Op::NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Op::SMEM);
+    if (a != cudaSuccess) return a;
+  }
   int n = 0;
-  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_kernel<Op, Op::NT>, Op::NT, 0);
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_kernel<Op, Op::NT>, Op::NT, Op::SMEM);
   if (e != cudaSuccess) return e;
   g_grouped_per_sm[kernel] = n > 0 ? n : 1;
   return cudaSuccess;
@@ -726,7 +1000,7 @@ template <class Op>
 void grouped_launch_op(int kernel, const GroupItem* items, const int64_t* tile_start, int nitems,
                        unsigned long long* counter, unsigned* status, int num_sms, cudaStream_t st) {
   const int per_sm = g_grouped_per_sm[kernel] > 0 ? g_grouped_per_sm[kernel] : 1;
-  grouped_kernel<Op, Op::NT><<<num_sms * per_sm, Op::NT, 0, st>>>(items, tile_start, nitems, counter, status);
+  grouped_kernel<Op, Op::NT><<<num_sms * per_sm, Op::NT, Op::SMEM, st>>>(items, tile_start, nitems, counter, status);
 }
 
 using GSimtF32L = SimtTileOp<float, false, 128, 128, 16, 8, 8>;

@@ -779,13 +779,12 @@ struct SimtTileOp {
 };
 template <bool CPLX, int WM, int WN, int BK>
 struct DmmaTileOp {
+  // Grouped lists (many short-K tiles) take the cp.async ring for real f64 too.
   static constexpr int NT = 128;
-  static constexpr int SMEM = dmma_dyn_smem<CPLX, WM, WN, BK>();
-  // Three resident CTAs per SM as dmma_gemm_kernel, except the f64 64 x 64
-  // tile, whose grouped loop would spill at that register budget.
-  static constexpr int MIN_BLOCKS = (!CPLX && WM == 32) ? 2 : 3;
+  static constexpr int SMEM = DmmaRing<CPLX, WM, WN, BK>::BYTES;
+  static constexpr int MIN_BLOCKS = 3;
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
-    dmma_tile<CPLX, WM, WN, BK>(g, h, mt, nt);
+    dmma_tile_async<CPLX, WM, WN, BK>(g, h, mt, nt);
   }
 };
 

@@ -348,6 +348,70 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
   }
 }
 
+// Complex slicing for the general layouts (rows or k unit-stride): one load
+// of a complex element writes all of its embedded values, as in the
+// batch-innermost kernel above. One CTA per (32 complex rows, 64 k, batch
+// entry); threads run along k when k is the unit-stride index.
+template <int WHICH>
+__global__ void __launch_bounds__(256) ozaki_slice_c64_kernel(
+    const double* __restrict__ X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
+    const int* __restrict__ exps, int64_t nrows, int64_t K, int64_t Kh, int64_t rows_pad, int64_t exp_pad,
+    int64_t k_pad, int64_t H, int kfast, int conj, int S, int8_t* __restrict__ out) {
+  __shared__ double t_re[32][65], t_im[32][65];
+  const int tid = threadIdx.x;
+  const int64_t k0 = (int64_t)blockIdx.x * 64, r0 = (int64_t)blockIdx.y * 32, h = blockIdx.z;
+  const int64_t hoff = h_scat[h];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    int rr, kk;
+    if (kfast) {
+      rr = tid / 64 + 4 * j;
+      kk = tid % 64;
+    } else {
+      rr = tid % 32;
+      kk = tid / 32 + 8 * j;
+    }
+    const int64_t r = r0 + rr, k = k0 + kk;
+    double re = 0.0, im = 0.0;
+    if (r < nrows && k < K) {
+      const double* e = X + 2 * (hoff + rows_scat[r] + k_scat[k]);
+      re = e[0];
+      im = conj ? -e[1] : e[1];
+    }
+    t_re[rr][kk] = re;
+    t_im[rr][kk] = im;
+  }
+  __syncthreads();
+  const int64_t plane = H * rows_pad * k_pad;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int p = tid + 256 * j;
+    const int rr = p / 16, kq = (p % 16) * 4;
+    const int64_t r = r0 + rr;
+    const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
+    double re[4], im[4], nim[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool bad = e == EXP_NONFINITE;
+      re[q] = bad ? 0.0 : t_re[rr][kq + q];
+      im[q] = bad ? 0.0 : t_im[rr][kq + q];
+      nim[q] = -im[q];
+    }
+    if (WHICH == 0) {
+      int8_t* o0 = out + (h * rows_pad + 2 * r) * k_pad + k0 + kq;
+      int8_t* o1 = o0 + k_pad;
+      write_slices(re, e, S, o0, plane);
+      write_slices(nim, e, S, o0 + Kh, plane);
+      write_slices(im, e, S, o1, plane);
+      write_slices(re, e, S, o1 + Kh, plane);
+    } else {
+      int8_t* o0 = out + (h * rows_pad + r) * k_pad + k0 + kq;
+      write_slices(re, e, S, o0, plane);
+      write_slices(im, e, S, o0 + Kh, plane);
+    }
+  }
+}
+
 template <int S>
 struct OzCfg {
   static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A plane tile
@@ -642,7 +706,7 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
   if (hfast) {
     ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);
-    if (CPLX) {
+    if constexpr (CPLX) {
       // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
       const dim3 grid((unsigned)(L.k_half / 64), (unsigned)(which == 0 ? rows_pad / 2 : rows_pad),
                       (unsigned)((L.H + 31) / 32));
@@ -661,9 +725,22 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
   } else {
     ozaki_exp_kernel<CPLX><<<dim3((unsigned)((nrows + 31) / 32), (unsigned)L.H), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, kfast, exps);
-    ozaki_slice_kernel<CPLX><<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
-        X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, kfast, which,
-        conj, L.slices, planes);
+    if constexpr (CPLX) {
+      // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
+      const int64_t crows = which == 0 ? rows_pad / 2 : rows_pad;
+      const dim3 grid((unsigned)(L.k_half / 64), (unsigned)(crows / 32), (unsigned)L.H);
+      if (which == 0)
+        ozaki_slice_c64_kernel<0><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                         exp_pad, L.k_pad, L.H, kfast, conj, L.slices, planes);
+      else
+        ozaki_slice_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                         exp_pad, L.k_pad, L.H, kfast, conj, L.slices, planes);
+    } else {
+      ozaki_slice_kernel<CPLX>
+          <<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
+              X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, kfast,
+              which, conj, L.slices, planes);
+    }
   }
 }
 

@@ -535,10 +535,12 @@ void drain(Executor& ex) {
     const cudaError_t q = cudaStreamQuery(ex.stream);
     if (q == cudaSuccess) return;
     if (q != cudaErrorNotReady) check_cuda(q, "kernel execution");
-    if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(ex.drain_limit_s))
+    const auto waited = std::chrono::steady_clock::now() - t0;
+    if (waited > std::chrono::seconds(ex.drain_limit_s))
       throw Error(ERR_INTERNAL, "the executor's stream did not drain within " + std::to_string(ex.drain_limit_s) +
                                     " s");
-    std::this_thread::sleep_for(std::chrono::microseconds(20));
+    // Spin for the first 200 us (short synchronous calls), then poll gently.
+    if (waited > std::chrono::microseconds(200)) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
 }
 

@@ -66,6 +66,13 @@ __device__ inline double embedded(const double* X, const int64_t* rows_scat, con
   return second ? (conj ? -e[1] : e[1]) : e[0];
 }
 
+// Bytewise negation of four signed bytes each in [-127, 127]:
+// ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256, and (b ^ 0x7f) + 1 never exceeds 255,
+// so no carry crosses into the next byte.
+__device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
+  return ((w ^ 0x7f7f7f7fu) + 0x01010101u) ^ 0x80808080u;
+}
+
 // The S signed 7-bit slices of four values of one row with exponent e
 // (|x| < 2^e), written as one 4-byte word per plane. T = trunc(x 2^(7S - e)) is
 // exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
@@ -75,7 +82,7 @@ __device__ inline double embedded(const double* X, const int64_t* rows_scat, con
 // and negated bytewise where x < 0: for a byte b <= 127,
 // ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
 template <int S>
-__device__ inline void write_slices_t(const double (&x)[4], int e, int8_t* o, int64_t plane) {
+__device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[8]) {
   const int k = 7 * S - e;  // scale exponent; above 1023 only for rows below 2^-967
   const bool two = k > 1023;
   const double s1 = two ? ldexp(1.0, 1000) : ldexp(1.0, k);
@@ -101,8 +108,44 @@ __device__ inline void write_slices_t(const double (&x)[4], int e, int8_t* o, in
       else d = __funnelshift_r(lo[q], hi[q], sh);
       w |= (d & 127u) << (8 * q);
     }
-    const uint32_t nw = ((w ^ 0x7f7f7f7fu) + 0x01010101u) ^ 0x80808080u;
-    *reinterpret_cast<uint32_t*>(o + sl * plane) = (w & ~negmask) | (nw & negmask);
+    out[sl] = (w & ~negmask) | (neg_bytes(w) & negmask);
+  }
+}
+
+template <int S>
+__device__ inline void write_slices_t(const double (&x)[4], int e, int8_t* o, int64_t plane) {
+  uint32_t w[8];
+  slice_words<S>(x, e, w);
+#pragma unroll
+  for (int sl = 0; sl < S; ++sl) *reinterpret_cast<uint32_t*>(o + sl * plane) = w[sl];
+}
+
+// The four embedded copies of a complex quad of A' (rows 2r and 2r+1, both
+// depth halves: re, -im / im, re) from one digit pass per part: re is stored
+// twice and -im is the bytewise negation of im's slices.
+template <int S>
+__device__ inline void write_slices_a_t(const double (&re)[4], const double (&im)[4], int e, int8_t* o0, int8_t* o1,
+                                        int64_t kh, int64_t plane) {
+  uint32_t wr[8], wi[8];
+  slice_words<S>(re, e, wr);
+  slice_words<S>(im, e, wi);
+#pragma unroll
+  for (int sl = 0; sl < S; ++sl) {
+    *reinterpret_cast<uint32_t*>(o0 + sl * plane) = wr[sl];
+    *reinterpret_cast<uint32_t*>(o0 + kh + sl * plane) = neg_bytes(wi[sl]);
+    *reinterpret_cast<uint32_t*>(o1 + sl * plane) = wi[sl];
+    *reinterpret_cast<uint32_t*>(o1 + kh + sl * plane) = wr[sl];
+  }
+}
+
+__device__ inline void write_slices_a(const double (&re)[4], const double (&im)[4], int e, int S, int8_t* o0,
+                                      int8_t* o1, int64_t kh, int64_t plane) {
+  switch (S) {
+    case 4: write_slices_a_t<4>(re, im, e, o0, o1, kh, plane); break;
+    case 5: write_slices_a_t<5>(re, im, e, o0, o1, kh, plane); break;
+    case 6: write_slices_a_t<6>(re, im, e, o0, o1, kh, plane); break;
+    case 7: write_slices_a_t<7>(re, im, e, o0, o1, kh, plane); break;
+    default: write_slices_a_t<8>(re, im, e, o0, o1, kh, plane); break;
   }
 }
 
@@ -325,21 +368,16 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
     const int64_t h = h0 + hl;
     if (h >= H) continue;
     const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
-    double re[4], im[4], nim[4];
+    double re[4], im[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const bool bad = e == EXP_NONFINITE;
       re[q] = bad ? 0.0 : t_re[hl][kq + q];
       im[q] = bad ? 0.0 : t_im[hl][kq + q];
-      nim[q] = -im[q];
     }
     if (WHICH == 0) {
       int8_t* o0 = out + (h * rows_pad + 2 * r) * k_pad + k0 + kq;
-      int8_t* o1 = o0 + k_pad;
-      write_slices(re, e, S, o0, plane);
-      write_slices(nim, e, S, o0 + Kh, plane);
-      write_slices(im, e, S, o1, plane);
-      write_slices(re, e, S, o1 + Kh, plane);
+      write_slices_a(re, im, e, S, o0, o0 + k_pad, Kh, plane);
     } else {
       int8_t* o0 = out + (h * rows_pad + r) * k_pad + k0 + kq;
       write_slices(re, e, S, o0, plane);
@@ -389,21 +427,16 @@ __global__ void __launch_bounds__(256) ozaki_slice_c64_kernel(
     const int rr = p / 16, kq = (p % 16) * 4;
     const int64_t r = r0 + rr;
     const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
-    double re[4], im[4], nim[4];
+    double re[4], im[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const bool bad = e == EXP_NONFINITE;
       re[q] = bad ? 0.0 : t_re[rr][kq + q];
       im[q] = bad ? 0.0 : t_im[rr][kq + q];
-      nim[q] = -im[q];
     }
     if (WHICH == 0) {
       int8_t* o0 = out + (h * rows_pad + 2 * r) * k_pad + k0 + kq;
-      int8_t* o1 = o0 + k_pad;
-      write_slices(re, e, S, o0, plane);
-      write_slices(nim, e, S, o0 + Kh, plane);
-      write_slices(im, e, S, o1, plane);
-      write_slices(re, e, S, o1 + Kh, plane);
+      write_slices_a(re, im, e, S, o0, o0 + k_pad, Kh, plane);
     } else {
       int8_t* o0 = out + (h * rows_pad + r) * k_pad + k0 + kq;
       write_slices(re, e, S, o0, plane);

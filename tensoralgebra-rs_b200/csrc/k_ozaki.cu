@@ -44,28 +44,6 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// One element of the (possibly complex-embedded) operand X' at (row, k).
-// which == 0: A' (rows = m); which == 1: B' (rows = n). The complex depth is
-// two halves of Kh (K rounded up to a k-block): [0, K) real parts and
-// [Kh, Kh + K) imaginary parts, zero in between.
-template <bool CPLX>
-__device__ inline double embedded(const double* X, const int64_t* rows_scat, const int64_t* k_scat, int64_t hoff,
-                                  int64_t row, int64_t k, int64_t K, int64_t Kh, int which, int conj) {
-  if (!CPLX) return X[hoff + rows_scat[row] + k_scat[k]];
-  const bool second = k >= Kh;
-  const int64_t kk = second ? k - Kh : k;
-  if (kk >= K) return 0.0;
-  if (which == 0) {
-    const int64_t r = row >> 1;
-    const double* e = X + 2 * (hoff + rows_scat[r] + k_scat[kk]);
-    const double re = e[0], im = conj ? -e[1] : e[1];
-    if ((row & 1) == 0) return second ? -im : re;
-    return second ? re : im;
-  }
-  const double* e = X + 2 * (hoff + rows_scat[row] + k_scat[kk]);
-  return second ? (conj ? -e[1] : e[1]) : e[0];
-}
-
 // Bytewise negation of four signed bytes each in [-127, 127]:
 // ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256, and (b ^ 0x7f) + 1 never exceeds 255,
 // so no carry crosses into the next byte.
@@ -206,15 +184,14 @@ __global__ void __launch_bounds__(256) ozaki_exp_kernel(const double* __restrict
   }
 }
 
-// Gather + scale + slice of one 32-row x 64-k tile of the embedded operand,
-// written K-major into planes[S][H][rows_pad][k_pad] (INT8), zero-padded.
-template <bool CPLX>
+// Gather + scale + slice of one 32-row x 64-k tile of a real operand, written
+// K-major into planes[S][H][rows_pad][k_pad] (INT8), zero-padded. (Complex
+// operands use ozaki_slice_c64_kernel.)
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                           const int64_t* k_scat, const int64_t* h_scat,
-                                                          const int* __restrict__ exps, int64_t nrows_emb,
-                                                          int64_t K, int64_t K_emb, int64_t Kh, int64_t rows_pad,
-                                                          int64_t exp_pad, int64_t k_pad, int64_t H, int kfast,
-                                                          int which, int conj, int S, int8_t* __restrict__ out) {
+                                                          const int* __restrict__ exps, int64_t nrows, int64_t K,
+                                                          int64_t rows_pad, int64_t exp_pad, int64_t k_pad, int64_t H,
+                                                          int kfast, int S, int8_t* __restrict__ out) {
   __shared__ double tile[32][65];
   const int tid = threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 64, h = blockIdx.z;
@@ -230,9 +207,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
       kk = tid / 32 + 8 * j;
     }
     const int64_t r = r0 + rr, k = k0 + kk;
-    double v = 0.0;
-    if (r < nrows_emb && k < K_emb) v = embedded<CPLX>(X, rows_scat, k_scat, hoff, r, k, K, Kh, which, conj);
-    tile[rr][kk] = v;
+    tile[rr][kk] = (r < nrows && k < K) ? X[hoff + rows_scat[r] + k_scat[k]] : 0.0;
   }
   __syncthreads();
   const int64_t plane = H * rows_pad * k_pad;
@@ -241,8 +216,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const double* __restri
     const int p = tid + 256 * j;
     const int rr = p / 16, kq = (p % 16) * 4;
     const int64_t r = r0 + rr;
-    const int64_t er = (CPLX && which == 0) ? (r >> 1) : r;
-    const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
+    const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
     double x[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : tile[rr][kq + q];
@@ -289,15 +263,13 @@ __global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __re
   }
 }
 
-// Slicing of one embedded row across 32 batch entries x 64 k: loads run along
+// Slicing of one real row across 32 batch entries x 64 k: loads run along
 // the batch index, the K-major plane rows are written 4 bytes per thread.
-template <bool CPLX>
 __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                                 const int64_t* k_scat, const int64_t* h_scat,
-                                                                const int* __restrict__ exps, int64_t nrows_emb,
-                                                                int64_t K, int64_t K_emb, int64_t Kh, int64_t rows_pad,
-                                                                int64_t exp_pad, int64_t k_pad, int64_t H, int which,
-                                                                int conj, int S, int8_t* __restrict__ out) {
+                                                                const int* __restrict__ exps, int64_t nrows, int64_t K,
+                                                                int64_t rows_pad, int64_t exp_pad, int64_t k_pad,
+                                                                int64_t H, int S, int8_t* __restrict__ out) {
   __shared__ double tile[32][65];
   const int tid = threadIdx.x;
   const int64_t k0 = (int64_t)blockIdx.x * 64, r = blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
@@ -308,22 +280,18 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __
     for (int j = 0; j < 8; ++j) {
       const int kk = (tid >> 5) + 8 * j;
       const int64_t k = k0 + kk;
-      double v = 0.0;
-      if (h < H && r < nrows_emb && k < K_emb)
-        v = embedded<CPLX>(X, rows_scat, k_scat, h_scat[h], r, k, K, Kh, which, conj);
-      tile[hl][kk] = v;
+      tile[hl][kk] = (h < H && r < nrows && k < K) ? X[h_scat[h] + rows_scat[r] + k_scat[k]] : 0.0;
     }
   }
   __syncthreads();
   const int64_t plane = H * rows_pad * k_pad;
-  const int64_t er = (CPLX && which == 0) ? (r >> 1) : r;
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
     const int p = tid + 256 * j;
     const int hl = p / 16, kq = (p % 16) * 4;
     const int64_t h = h0 + hl;
     if (h >= H) continue;
-    const int e = (r < nrows_emb) ? exps[h * exp_pad + er] : 0;
+    const int e = (r < nrows) ? exps[h * exp_pad + r] : 0;
     double x[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) x[q] = (e == EXP_NONFINITE) ? 0.0 : tile[hl][kq + q];
@@ -452,9 +420,8 @@ struct OzCfg {
   static constexpr int STAGE = S * (A_TILE + B_TILE);
   static constexpr int STAGES = (S <= 6) ? 3 : 2;
   static constexpr int RING = STAGES * STAGE;
-  static constexpr int SCAT = 2 * OZ_BN * 8 + OZ_BN * 4;  // d_n, c_n, column exponents
   static constexpr int BAR = (2 * STAGES + 2) * 8 + 16;
-  static constexpr int SMEM = 1024 + RING + SCAT + BAR;
+  static constexpr int SMEM = 1024 + RING + BAR;
   static constexpr int TMEM_COLS = (S * OZ_BN <= 256) ? 256 : 512;
   static_assert(S * OZ_BN <= 512, "one INT32 accumulator per diagonal must fit in TMEM");
 };
@@ -485,7 +452,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* ring = smem;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING + Cfg::SCAT);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING);
   uint64_t* empty = full + Cfg::STAGES;
   uint64_t* accf = empty + Cfg::STAGES;
   uint64_t* tmem_empty = accf + 1;
@@ -734,7 +701,7 @@ size_t ozaki_workspace_bytes(const OzakiLayout& L) {
 // batch-innermost variants when the batch index has the smallest stride.
 template <bool CPLX>
 static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* k_s, const int64_t* h_s, int64_t nrows,
-                         int64_t nrows_emb, int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
+                         int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
                          int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
   if (hfast) {
     ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
@@ -750,10 +717,9 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
         ozaki_slice_hfast_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
                                                                exp_pad, L.k_pad, L.H, conj, L.slices, planes);
     } else {
-      ozaki_slice_hfast_kernel<CPLX>
-          <<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
-              X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, which,
-              conj, L.slices, planes);
+      ozaki_slice_hfast_kernel<<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)),
+                                 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, rows_pad, exp_pad, L.k_pad, L.H,
+                                               L.slices, planes);
     }
   } else {
     ozaki_exp_kernel<CPLX><<<dim3((unsigned)((nrows + 31) / 32), (unsigned)L.H), 256, 0, st>>>(
@@ -769,10 +735,8 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
         ozaki_slice_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
                                                          exp_pad, L.k_pad, L.H, kfast, conj, L.slices, planes);
     } else {
-      ozaki_slice_kernel<CPLX>
-          <<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
-              X, rows_s, k_s, h_s, exps, nrows_emb, K, L.k_emb, L.k_half, rows_pad, exp_pad, L.k_pad, L.H, kfast,
-              which, conj, L.slices, planes);
+      ozaki_slice_kernel<<<dim3((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H), 256, 0, st>>>(
+          X, rows_s, k_s, h_s, exps, nrows, K, rows_pad, exp_pad, L.k_pad, L.H, kfast, L.slices, planes);
     }
   }
 }
@@ -787,14 +751,14 @@ cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws,
   const double* B = static_cast<const double*>(g.B);
   // Row exponents of A (per complex row) and column exponents of B.
   if (L.cplx) {
-    pack_operand<true>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, L.m_emb, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast, L.a_hfast,
+    pack_operand<true>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast, L.a_hfast,
                        0, g.conj_a, ea, ap, st);
-    pack_operand<true>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1,
+    pack_operand<true>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1,
                        g.conj_b, eb, bp, st);
   } else {
-    pack_operand<false>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, L.m_emb, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast,
+    pack_operand<false>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast,
                         L.a_hfast, 0, 0, ea, ap, st);
-    pack_operand<false>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1, 0,
+    pack_operand<false>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1, 0,
                         eb, bp, st);
   }
   return cudaGetLastError();

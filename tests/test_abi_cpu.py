@@ -257,3 +257,29 @@ def test_planner_splits_k_only_for_deep_contractions_with_few_tiles(tp):
     assert deep["split_k"] > 1 and "64x64" in deep["family"]
     assert report(4096, 4096, 4096, dt=0)["split_k"] == 1  # enough tiles
     assert report(64, 64, 512)["split_k"] == 1  # shallow
+
+
+def test_launch_choices_reported_per_plan(tp):
+    """The plan report names the launch shape the executor will use (for 148
+    SMs): the tcgen05 split GEMM cuts the partial last wave of C2 (512 tiles)
+    into K halves, and batches of tiny products take the one-thread-per-output
+    kernel."""
+    def product(dt, ext_a, st_a, la, ext_b, st_b, lb, ext_d, st_d, ld, prec=0):
+        h = tp.Handle()
+        infos = [tp.TensorInfo(dt, ext_a, st_a), tp.TensorInfo(dt, ext_b, st_b), tp.TensorInfo(dt, ext_d, st_d),
+                 tp.TensorInfo(dt, ext_d, st_d)]
+        p = tp.TensorProduct.create(h, (0, infos[0], la), (0, infos[1], lb), (0, infos[2], ld), (0, infos[3], ld))
+        p._keep = (h, infos)
+        if prec:
+            p.set_precision(prec)
+        return p
+
+    n = 4096
+    c2 = product(0, [n, n], [1, n], [2, 0], [n, n], [1, n], [2, 1], [n, n], [1, n], [0, 1], prec=tp.PREC_BF16X6)
+    assert c2.report()["tail_parts"] == 2
+    m = 2048
+    sq = product(0, [m, m], [1, m], [2, 0], [m, m], [1, m], [2, 1], [m, m], [1, m], [0, 1], prec=tp.PREC_BF16X6)
+    assert sq.report()["tail_parts"] == 1  # 128 tiles: one partial wave of whole tiles
+    hb = 1 << 20
+    had = product(1, [hb], [1], [9], [hb], [1], [9], [hb], [1], [9])
+    assert "tiny-batched" in had.report()["family"]

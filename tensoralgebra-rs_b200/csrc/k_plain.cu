@@ -782,7 +782,7 @@ struct DmmaTileOp {
   // Grouped lists (many short-K tiles) take the cp.async ring for real f64 too.
   static constexpr int NT = 128;
   static constexpr int SMEM = DmmaRing<CPLX, WM, WN, BK>::BYTES;
-  static constexpr int MIN_BLOCKS = 3;
+  static constexpr int MIN_BLOCKS = WM == 64 ? 2 : 3;  // the tall tile's ring needs 86 KB
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
     dmma_tile_async<CPLX, WM, WN, BK>(g, h, mt, nt);
   }
@@ -806,6 +806,8 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.planar.64x64x16";
     case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.planar.64x32x8";
     case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
+    case PLAIN_F64_DMMA_128x32: return "sm100.f64.dmma884.128x32x16";
+    case PLAIN_C64_DMMA_128x32: return "sm100.c64.dmma884.planar.128x32x8";
   }
   return "auto";
 }
@@ -837,7 +839,14 @@ int choose_grouped_kernel(int dtype, int64_t M, int64_t N) {
     return (double)M * (double)N / padded;
   };
   const int L = large[dtype & 3], S = small[dtype & 3];
-  return util(L) >= 0.8 * util(S) ? L : S;
+  const int best = util(L) >= 0.8 * util(S) ? L : S;
+  // Narrow outputs (N <= 32) of many rows: the tall 128 x 32 tile amortises
+  // each tile's fixed cost (scatter loads, epilogue) over four times the rows.
+  if ((dtype == 1 || dtype == 3) && N <= 32 && M >= 256) {
+    const int T = dtype == 1 ? PLAIN_F64_DMMA_128x32 : PLAIN_C64_DMMA_128x32;
+    if (util(T) >= 0.9 * util(best)) return T;
+  }
+  return best;
 }
 
 void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms, int* kernel,
@@ -954,6 +963,12 @@ cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStre
     case PLAIN_C64_DMMA_32x32:
       if (dtype != 3) return cudaErrorInvalidValue;
       return launch_dmma<true, 16, 16, 8>(g, st);
+    case PLAIN_F64_DMMA_128x32:
+      if (dtype != 1) return cudaErrorInvalidValue;
+      return launch_dmma<false, 64, 16, 16>(g, st);
+    case PLAIN_C64_DMMA_128x32:
+      if (dtype != 3) return cudaErrorInvalidValue;
+      return launch_dmma<true, 64, 16, 8>(g, st);
     default:
       return cudaErrorInvalidValue;
   }
@@ -969,6 +984,8 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_F64_DMMA_32x32: *bm = 32; *bn = 32; return;
     case PLAIN_C64_DMMA_64x32: *bm = 64; *bn = 32; return;
     case PLAIN_C64_DMMA_32x32: *bm = 32; *bn = 32; return;
+    case PLAIN_F64_DMMA_128x32: *bm = 128; *bn = 32; return;
+    case PLAIN_C64_DMMA_128x32: *bm = 128; *bn = 32; return;
   }
   *bm = *bn = 0;
 }
@@ -979,7 +996,7 @@ namespace {
 // filled before any capture by prepare_grouped: the persistent grid must not
 // exceed what can be resident at once, or the CTAs beyond it start only when
 // others have drained the queue.
-int g_grouped_per_sm[8] = {};
+int g_grouped_per_sm[16] = {};
 
 template <class Op>
 cudaError_t grouped_prepare_op(int kernel) {
@@ -1009,6 +1026,8 @@ using GDmmaF64L = DmmaTileOp<false, 32, 32, 16>;
 using GDmmaF64S = DmmaTileOp<false, 16, 16, 16>;
 using GDmmaC64L = DmmaTileOp<true, 32, 16, 8>;
 using GDmmaC64S = DmmaTileOp<true, 16, 16, 8>;
+using GDmmaF64T = DmmaTileOp<false, 64, 16, 16>;
+using GDmmaC64T = DmmaTileOp<true, 64, 16, 8>;
 
 }  // namespace
 
@@ -1023,6 +1042,8 @@ cudaError_t prepare_grouped(int kernel) {
     case PLAIN_F64_DMMA_32x32: return grouped_prepare_op<GDmmaF64S>(kernel);
     case PLAIN_C64_DMMA_64x32: return grouped_prepare_op<GDmmaC64L>(kernel);
     case PLAIN_C64_DMMA_32x32: return grouped_prepare_op<GDmmaC64S>(kernel);
+    case PLAIN_F64_DMMA_128x32: return grouped_prepare_op<GDmmaF64T>(kernel);
+    case PLAIN_C64_DMMA_128x32: return grouped_prepare_op<GDmmaC64T>(kernel);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1053,6 +1074,12 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
       break;
     case PLAIN_C64_DMMA_32x32:
       grouped_launch_op<GDmmaC64S>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_DMMA_128x32:
+      grouped_launch_op<GDmmaF64T>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_C64_DMMA_128x32:
+      grouped_launch_op<GDmmaC64T>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
     default: return cudaErrorInvalidValue;
   }

@@ -258,7 +258,7 @@ def test_batched_product_matches_single_products(tp, ex, torch_cuda):
 
 
 # ----------------------------------------------------------- tiles and families
-FAMILIES = {"float32": [1, 2], "float64": [3, 4], "complex64": [5], "complex128": [6, 7]}
+FAMILIES = {"float32": [1, 2], "float64": [3, 4, 8], "complex64": [5], "complex128": [6, 7, 9]}
 
 
 @pytest.mark.parametrize("dt", DTYPES)

@@ -237,7 +237,10 @@ enum {
    otherwise. Refused (UNSUPPORTED) for a dtype the scheme does not apply to.
    The reference has no counterpart (its C ABI has no tuning call, product.rs:48). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan, int scheme, int slices);
-/* Pin the CTA tile (0 = autotuned). Rows/cols are the oriented M/N tile. */
+/* Pin the plain-path tile family (0 = chosen per shape). Rows x cols of the
+   oriented M/N tile: 1 f32 128x128, 2 f32 64x64, 3 f64 64x64, 4 f64 32x32,
+   5 c32 64x64, 6 c64 64x32, 7 c64 32x32, 8 f64 128x32, 9 c64 128x32. A family
+   of another dtype is refused at execution (TPRIMS_ERR_INTERNAL). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);
 /* A NUL-terminated JSON description of the plan (the counterpart of
    Plan::report, crates/tprims-contract/src/plan/mod.rs:237). Returns the full

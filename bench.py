@@ -405,6 +405,31 @@ def run_config(args, tp, torch, ex):
 
     cfg = args.config
     out = {"config": cfg, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "unit": "TFLOP/s"}
+    if cfg == "gemm":
+        # A plain square GEMM D[m,n] = sum_k A[k,m] B[k,n] (k unit-stride in
+        # both operands) of --dtype and --size: the plain kernels' efficiency
+        # against the probe-measured pipe peak.
+        code, npdt = CORPUS_DT[args.dtype]
+        n = args.size
+        tdt = getattr(torch, npdt)
+        lay = tp.LayoutSpec([n, n], [1, n])
+        prob = tp.Problem.from_labels(code, tp.OperandSpec(lay), tp.OperandSpec(lay), tp.OperandSpec(lay),
+                                      [2, 0], [2, 1], [0, 1])
+        plan = tp.Plan(prob)
+        gen = torch.Generator(device="cuda").manual_seed(20261203 + 8000)
+        A = torch.randn(n * n, dtype=tdt, device="cuda", generator=gen)
+        B = torch.randn(n * n, dtype=tdt, device="cuda", generator=gen)
+        D = torch.zeros(n * n, dtype=tdt, device="cuda")
+        fn = lambda: plan.execute_into(ex, 1.0, A.data_ptr(), B.data_ptr(), D.data_ptr())
+        ms, kt = timed(fn, args.steps, args.warmup)
+        flop = (8.0 if args.dtype[0] == "c" else 2.0) * n ** 3
+        peak = ex.probe_peak(0 if args.dtype in ("f64", "c64") else 1)
+        out["workload"] = f"plain {args.dtype} GEMM D[m,n] = sum_k A[k,m] B[k,n], m = n = k = {n}"
+        out["plain"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
+                        "family": plan.report()["family"], "pipe_peak_tflops": peak,
+                        "frac": flop / (ms * 1e-3) / 1e12 / peak}
+        print(json.dumps(out), flush=True)
+        return
     if cfg == "corpus":
         # The reference's dot_general corpus replayed through Problem::from_dot_general
         # and execute_into (plain precision), seeded inputs; each entry timed alone.
@@ -643,7 +668,9 @@ def main():
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus"],
+    ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
+    ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus", "gemm"],
                     help="c2 is the metric's workload; c1/c3/c5 print timing lines of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

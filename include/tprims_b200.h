@@ -214,6 +214,16 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor e
    register-only operation chains on every SM; *tflops receives the best of a
    few timed launches (CUDA events on the executor's stream). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int which, double* tflops);
+/* The executor's autotuner cache, persisted as a versioned text file (the
+   reference has no tuning state to persist; this is the build's only
+   checkpoint). save writes every entry; load adds the entries of a file
+   written on the same kind of device (SM count and name; others are skipped)
+   and refuses a malformed file with INVALID_ARGUMENT, adding nothing. clear
+   empties the cache; tuning returns it as JSON (full length, like snprintf). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_save_tuning(TAPP_executor exec, const char* path);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_load_tuning(TAPP_executor exec, const char* path);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_clear_tuning(TAPP_executor exec);
+TPRIMS_B200_EXPORT size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, size_t maxlen);
 /* Per-kernel timing (diagnostics, off by default): with `on` != 0 the executor
    records CUDA events on its stream around every kernel launch. The totals
    are resolved whenever the stream is drained. */
@@ -242,6 +252,24 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_prod
    5 c32 64x64, 6 c64 64x32, 7 c64 32x32, 8 f64 128x32, 9 c64 128x32. A family
    of another dtype is refused at execution (TPRIMS_ERR_INTERNAL). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);
+/* Pin the split-K factor of the plain path: 0 = chosen (model or autotuner),
+   1 = never split K, 2..64 = cut K into that many chunks of whole 64-deep
+   blocks (fewer when K is short). Split partials are summed in a fixed order.
+   The counterpart of the reference's frozen partition (select/resolve.rs:164),
+   which never splits K; INVALID_ARGUMENT outside 0..64. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_split_k(TAPP_tensor_product plan, int splits);
+/* Autotuning (PlanConfig's `autotune` switch; the reference freezes its choice
+   from an analytical model instead, contract resolve.rs:42, kernel
+   blocking/model.rs:220). With `on` != 0 and no pins, the first plain
+   execution of the plan's Problem signature (dtype, folded extents and
+   strides, conjugations, scheme, whether C is read) on an executor times every
+   candidate tile family and split-K factor on the executor's stream and keeps
+   the fastest in the executor's cache; later executions of any plan with that
+   signature use it. A grouped list whose plans all autotune has its tile policy
+   measured the same way, keyed by the list's signatures. Results stay within
+   the plain path's stated error; D is left as one execution leaves it (a D
+   that is also C is restored between the timed runs). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_autotune(TAPP_tensor_product plan, int on);
 /* A NUL-terminated JSON description of the plan (the counterpart of
    Plan::report, crates/tprims-contract/src/plan/mod.rs:237). Returns the full
    length, like snprintf. */

@@ -7,6 +7,7 @@
 // Every entry point catches all C++ exceptions: nothing unwinds across the C
 // boundary, and the message of the last failure is kept per thread.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -512,6 +513,19 @@ extern "C" TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int
   });
 }
 
+extern "C" TAPP_error tprims_b200_product_set_split_k(TAPP_tensor_product plan, int splits) {
+  return ffi([&] {
+    Product& p = product_of(plan);
+    if (splits < 0 || splits > 64)
+      throw Error(ERR_INVALID_ARGUMENT, "split-K factor must be 0 (chosen), 1 (never) or 2..64");
+    p.split_pin = splits;
+  });
+}
+
+extern "C" TAPP_error tprims_b200_product_set_autotune(TAPP_tensor_product plan, int on) {
+  return ffi([&] { product_of(plan).autotune = on != 0; });
+}
+
 extern "C" size_t tprims_b200_product_report(TAPP_tensor_product plan, char* buf, size_t maxlen) {
   std::string s;
   if (ffi([&] { s = product_of(plan).report(); }) != TPRIMS_OK) return 0;
@@ -688,6 +702,65 @@ extern "C" size_t tprims_b200_executor_kernel_times(TAPP_executor exec, char* bu
         ex.times.resolve();
         s = kernel_times_json(ex, reset != 0);
         if (prev >= 0) cudaSetDevice(prev);
+      }) != TPRIMS_OK)
+    return 0;
+  if (buf && maxlen > 0) {
+    const size_t n = s.size() < maxlen - 1 ? s.size() : maxlen - 1;
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return s.size();
+}
+
+extern "C" TAPP_error tprims_b200_executor_save_tuning(TAPP_executor exec, const char* path) {
+  return ffi([&] {
+    if (!path || !*path) throw Error(ERR_INVALID_ARGUMENT, "tuning cache path is null or empty");
+    Executor& ex = resolve_exec(exec)->get();
+    std::string text;
+    {
+      std::lock_guard<std::mutex> lk(ex.mu);
+      text = tuning_text(ex);
+    }
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) throw Error(ERR_INVALID_ARGUMENT, std::string("cannot open tuning cache for writing: ") + path);
+    const size_t n = std::fwrite(text.data(), 1, text.size(), f);
+    const int closed = std::fclose(f);
+    if (n != text.size() || closed != 0)
+      throw Error(ERR_INTERNAL, std::string("short write of tuning cache: ") + path);
+  });
+}
+
+extern "C" TAPP_error tprims_b200_executor_load_tuning(TAPP_executor exec, const char* path) {
+  return ffi([&] {
+    if (!path || !*path) throw Error(ERR_INVALID_ARGUMENT, "tuning cache path is null or empty");
+    Executor& ex = resolve_exec(exec)->get();
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) throw Error(ERR_INVALID_ARGUMENT, std::string("cannot open tuning cache: ") + path);
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+    std::fclose(f);
+    std::lock_guard<std::mutex> lk(ex.mu);
+    load_tuning_text(ex, text);  // all-or-nothing: nothing is added when a line is malformed
+  });
+}
+
+extern "C" TAPP_error tprims_b200_executor_clear_tuning(TAPP_executor exec) {
+  return ffi([&] {
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    ex.tune.clear();
+    ex.list_tune.clear();
+  });
+}
+
+extern "C" size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, size_t maxlen) {
+  std::string s;
+  if (ffi([&] {
+        Executor& ex = resolve_exec(exec)->get();
+        std::lock_guard<std::mutex> lk(ex.mu);
+        s = tuning_json(ex);
       }) != TPRIMS_OK)
     return 0;
   if (buf && maxlen > 0) {

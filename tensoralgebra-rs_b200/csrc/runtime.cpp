@@ -62,6 +62,9 @@ Executor* Executor::create(int device, uintptr_t stream) {
   check_cuda(cudaMemsetAsync(ex->status, 0, 256, ex->stream), "cudaMemset(status)");
   check_cuda(cudaStreamSynchronize(ex->stream), "cudaStreamSynchronize");
   check_cuda(cudaDeviceGetAttribute(&ex->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+  cudaDeviceProp prop;
+  check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  ex->device_name = prop.name;
   return ex.release();
 }
 
@@ -117,6 +120,7 @@ Product::Product(const Problem& p) : problem(p), uid(g_product_uid.fetch_add(1))
   view = orient(packed, packed.transposes_gemm(32));
   tiny_h = dev::TinyStrides{sequence_stride(view.h_a), sequence_stride(view.h_b), sequence_stride(view.h_c),
                             sequence_stride(view.h_d)};
+  signature = problem_signature(*this);
 }
 
 Product::~Product() {
@@ -203,11 +207,18 @@ double stated_bound(DType t, Scheme s) {
 std::string Product::report() const {
   std::ostringstream o;
   const auto& st = packed.stats;
-  int kernel = 0, splits = 1;
-  int64_t chunk = 0;
-  dev::choose_plain_launch((int)problem.dtype, kernel_pin, view.M, view.N, view.K, view.H, 148, &kernel, &splits,
-                           &chunk);
-  const bool tiny = scheme == Scheme::Plain && !kernel_pin && dev::use_tiny_batched(view.M, view.N, view.K, view.H);
+  // The configuration of the last plain execution when there was one, else
+  // the model's choice (148 SMs) under the pins.
+  PlainChoice pc;
+  ChoiceSource src;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    pc = executed ? last : model_choice(*this, 148);
+    src = executed ? last_source : ((kernel_pin || split_pin) ? ChoiceSource::Pinned : ChoiceSource::Model);
+  }
+  const bool tiny = scheme == Scheme::Plain && pc.tiny;
+  const int kernel = pc.kernel, splits = pc.splits;
+  static const char* src_names[4] = {"model", "pinned", "autotuned", "tuning-cache"};
   std::string family = tiny ? std::string("sm100.") + dtype_name(problem.dtype) + ".tiny-batched"
                        : scheme == Scheme::Plain ? dev::plain_kernel_name(kernel)
                        : scheme == Scheme::Bf16x3 ? "sm100.f32.tcgen05.bf16x3.128x256x32"
@@ -227,6 +238,8 @@ std::string Product::report() const {
     << ((scheme == Scheme::Bf16x3 || scheme == Scheme::Bf16x6)
             ? dev::split_tail_parts(dev::split_layout((int)scheme, view.M, view.N, view.K, view.H), 148)
             : 1)
+    << ",\"choice\":\"" << (scheme == Scheme::Plain ? src_names[(int)src] : "fixed")
+    << "\",\"autotune\":" << (autotune ? "true" : "false") << ",\"signature\":\"" << signature << "\""
     << ",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)
     << ",\"regular_rows\":" << regular_fraction(build_block_scatter(view.d_m, 32))
     << ",\"regular_cols\":" << regular_fraction(build_block_scatter(view.d_n, 32))
@@ -364,8 +377,36 @@ struct Timed {
   }
 };
 
-void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool output_only, char* scratch,
-                        size_t scratch_bytes) {
+// One plain execution in the configuration `c` (scratch: the split-K partials).
+void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const PlainChoice& c, char* scratch,
+                  size_t scratch_bytes) {
+  const int dt = (int)pr.problem.dtype;
+  if (c.tiny) {
+    Timed t(ex, "tiny_batched");
+    check_cuda(dev::launch_tiny_batched(dt, g, pr.tiny_h, ex.num_sms, ex.stream), "tiny batched launch");
+    return;
+  }
+  if (c.splits > 1) {
+    // Split-K: partial tiles into the scratch, then the reduce + epilogue.
+    const size_t need = (size_t)c.splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype);
+    if (need + 256 > scratch_bytes) throw Error(ERR_INTERNAL, "split-K workspace too small");
+    dev::GemmArgs gs = g;
+    gs.k_chunk = c.chunk;
+    gs.partial = reinterpret_cast<void*>(align_up((uintptr_t)scratch, 256));
+    {
+      Timed t(ex, dev::plain_kernel_name(c.kernel));
+      check_cuda(dev::launch_plain_gemm(dt, c.kernel, gs, ex.stream), "plain contraction launch");
+    }
+    Timed t(ex, "splitk_reduce");
+    check_cuda(dev::launch_splitk_reduce(dt, gs, c.splits, ex.stream), "split-K reduce launch");
+    return;
+  }
+  Timed t(ex, dev::plain_kernel_name(c.kernel));
+  check_cuda(dev::launch_plain_gemm(dt, c.kernel, g, ex.stream), "plain contraction launch");
+}
+
+void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool output_only, const PlainChoice& pc,
+                        char* scratch, size_t scratch_bytes) {
   const int dt = (int)pr.problem.dtype;
   if (output_only) {
     Timed t(ex, "output_pass");
@@ -373,34 +414,9 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
     return;
   }
   switch (pr.scheme) {
-    case Scheme::Plain: {
-      if (!pr.kernel_pin && dev::use_tiny_batched(g.M, g.N, g.K, g.H)) {
-        Timed t(ex, "tiny_batched");
-        check_cuda(dev::launch_tiny_batched(dt, g, pr.tiny_h, ex.num_sms, ex.stream), "tiny batched launch");
-        return;
-      }
-      int k = 0, splits = 1;
-      int64_t chunk = 0;
-      dev::choose_plain_launch(dt, pr.kernel_pin, g.M, g.N, g.K, g.H, ex.num_sms, &k, &splits, &chunk);
-      if (splits > 1) {
-        // Split-K: partial tiles into the scratch, then the reduce + epilogue.
-        const size_t need = (size_t)splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype);
-        if (need + 256 > scratch_bytes) throw Error(ERR_INTERNAL, "split-K workspace too small");
-        dev::GemmArgs gs = g;
-        gs.k_chunk = chunk;
-        gs.partial = reinterpret_cast<void*>(align_up((uintptr_t)scratch, 256));
-        {
-          Timed t(ex, dev::plain_kernel_name(k));
-          check_cuda(dev::launch_plain_gemm(dt, k, gs, ex.stream), "plain contraction launch");
-        }
-        Timed t(ex, "splitk_reduce");
-        check_cuda(dev::launch_splitk_reduce(dt, gs, splits, ex.stream), "split-K reduce launch");
-        return;
-      }
-      Timed t(ex, dev::plain_kernel_name(k));
-      check_cuda(dev::launch_plain_gemm(dt, k, g, ex.stream), "plain contraction launch");
+    case Scheme::Plain:
+      launch_plain(pr, ex, g, pc, scratch, scratch_bytes);
       return;
-    }
     case Scheme::Bf16x3:
     case Scheme::Bf16x6: {
       const dev::SplitLayout L = dev::split_layout((int)pr.scheme, g.M, g.N, g.K, g.H);
@@ -460,15 +476,9 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
   }
 }
 
-size_t scheme_scratch(const Product& pr, int num_sms) {
+size_t scheme_scratch(const Product& pr, const PlainChoice& pc, int num_sms) {
   const auto& v = pr.view;
-  if (pr.scheme == Scheme::Plain) {
-    if (!pr.kernel_pin && dev::use_tiny_batched(v.M, v.N, v.K, v.H)) return 0;
-    int k = 0, splits = 1;
-    int64_t chunk = 0;
-    dev::choose_plain_launch((int)pr.problem.dtype, pr.kernel_pin, v.M, v.N, v.K, v.H, num_sms, &k, &splits, &chunk);
-    return splits > 1 ? (size_t)splits * v.H * v.M * v.N * dtype_size(pr.problem.dtype) + 256 : 0;
-  }
+  if (pr.scheme == Scheme::Plain) return plain_scratch(pc, pr);
   if (pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6) {
     const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
     return dev::split_workspace_bytes(L) + dev::split_tail_bytes(L, num_sms) + 512;
@@ -585,8 +595,100 @@ dev::GemmArgs build_args(Product& pr, Executor& ex, Scalar alpha, Scalar beta, b
   return g;
 }
 
+// Events for the autotuner's measurements.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  EventPair() {
+    check_cuda(cudaEventCreate(&a), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&b), "cudaEventCreate");
+  }
+  ~EventPair() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+// Profiling is suspended while the autotuner measures (its runs are not the
+// caller's work).
+struct ProfileOff {
+  Executor& ex;
+  bool prev;
+  explicit ProfileOff(Executor& e) : ex(e), prev(e.profile) { ex.profile = false; }
+  ~ProfileOff() { ex.profile = prev; }
+};
+
+// Milliseconds of `fn`'s work on the executor's stream (the stream drains).
+template <class F>
+double time_on_stream(Executor& ex, EventPair& ev, F&& fn) {
+  check_cuda(cudaEventRecord(ev.a, ex.stream), "cudaEventRecord");
+  fn();
+  check_cuda(cudaEventRecord(ev.b, ex.stream), "cudaEventRecord");
+  drain(ex);
+  float ms = 0;
+  check_cuda(cudaEventElapsedTime(&ms, ev.a, ev.b), "cudaEventElapsedTime");
+  return ms;
+}
+
+// Repetitions of a measurement by the duration of its first run: short runs
+// are repeated more, since their times scatter more.
+int tune_reps(double first_ms) { return first_ms < 0.05 ? 10 : first_ms < 1.0 ? 5 : first_ms < 20.0 ? 3 : 1; }
+
+// Times every plain candidate of the item (minimum over repetitions after one
+// warm-up run) and returns the fastest; the model's choice is kept unless a
+// candidate is at least 3 % faster. Each run writes D; when the call reads D
+// (in-place accumulation) `d_span` is saved to `snapshot` first and restored
+// before every run and at the end, so the caller's execution afterwards sees
+// the original D.
+TuneEntry autotune_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, char* scratch, size_t scratch_bytes,
+                         char* d_span, char* snapshot, size_t span_bytes) {
+  ProfileOff off(ex);
+  const auto restore = [&] {
+    if (snapshot)
+      check_cuda(cudaMemcpyAsync(d_span, snapshot, span_bytes, cudaMemcpyDeviceToDevice, ex.stream),
+                 "autotune restore of D");
+  };
+  if (snapshot)
+    check_cuda(cudaMemcpyAsync(snapshot, d_span, span_bytes, cudaMemcpyDeviceToDevice, ex.stream),
+               "autotune snapshot of D");
+  EventPair ev;
+  const std::vector<PlainChoice> cands =
+      plain_candidates((int)pr.problem.dtype, pr.view.M, pr.view.N, pr.view.K, pr.view.H, ex.num_sms);
+  TuneEntry best;
+  best.ms = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    const PlainChoice& c = cands[i];
+    if (plain_scratch(c, pr) > scratch_bytes) continue;
+    double t = 0;
+    try {
+      const auto run = [&] { launch_plain(pr, ex, g, c, scratch, scratch_bytes); };
+      restore();
+      const double first = time_on_stream(ex, ev, run);
+      t = first;
+      const int reps = tune_reps(first);
+      for (int r = 0; r < reps; ++r) {
+        restore();
+        t = std::min(t, time_on_stream(ex, ev, run));
+      }
+    } catch (const Error& e) {
+      if (e.status != ERR_INTERNAL) throw;
+      continue;  // a configuration that cannot launch on this device
+    }
+    ++best.tried;
+    if (best.tried == 1 || t < best.ms * 0.97) {
+      best.ms = t;
+      best.choice = c;
+    }
+  }
+  restore();
+  if (best.tried == 0) throw Error(ERR_INTERNAL, "autotuner: no candidate configuration could be launched");
+  best.tuned = true;
+  return best;
+}
+
 // Enqueue one item; returns whether host copies were involved (the caller
 // must then drain the stream before returning to the host).
+int dt_code(const Product& pr) { return (int)pr.problem.dtype; }
+
 bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
   const Problem& p = pr.problem;
   if (p.out_empty) return false;
@@ -614,8 +716,53 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
     span_bytes(p, s, &st[s].lo_bytes, &st[s].bytes);
     total = align_up(total, 256) + st[s].bytes;
   }
-  const size_t scratch = output_only ? 0 : scheme_scratch(pr, ex.num_sms);
-  char* ws = static_cast<char*>(ex.workspace(align_up(total, 256) + scratch + 512));
+  // The plain path's configuration: the pins, else (autotune) the executor's
+  // tuning cache or a measurement now, else the model.
+  PlainChoice pc{};
+  ChoiceSource src = ChoiceSource::Model;
+  bool tune = false;
+  std::string key;
+  if (pr.scheme == Scheme::Plain && !output_only) {
+    pc = model_choice(pr, ex.num_sms);
+    if (pr.kernel_pin || pr.split_pin) {
+      src = ChoiceSource::Pinned;
+    } else if (pr.autotune) {
+      key = tune_key(pr, c_read);
+      const auto hit = ex.tune.find(key);
+      if (hit != ex.tune.end()) {
+        pc = hit->second.choice;
+        src = hit->second.tuned ? ChoiceSource::Cached : ChoiceSource::Model;
+      } else {
+        tune = true;
+      }
+    }
+  }
+  size_t scratch = output_only ? 0 : scheme_scratch(pr, pc, ex.num_sms);
+  int64_t d_lo = 0;
+  size_t d_bytes = 0, snap = 0;
+  if (tune) {
+    // Room for the largest candidate, and for a copy of D when the call reads it.
+    size_t tune_scratch = scratch;
+    for (const auto& c : plain_candidates(dt_code(pr), pr.view.M, pr.view.N, pr.view.K, pr.view.H, ex.num_sms))
+      tune_scratch = std::max(tune_scratch, plain_scratch(c, pr));
+    if (in_place) {
+      span_bytes(p, SD, &d_lo, &d_bytes);
+      snap = align_up(d_bytes, 256);
+    }
+    const size_t limit = std::min<size_t>(ex.ws_limit, size_t(4) << 30);
+    if (align_up(total, 256) + tune_scratch + snap + 1024 > limit) {
+      // Too large to measure within the workspace cap: keep the model's choice.
+      tune = false;
+      snap = 0;
+      TuneEntry e;
+      e.choice = pc;
+      e.tuned = false;
+      ex.tune[key] = e;
+    } else {
+      scratch = tune_scratch;
+    }
+  }
+  char* ws = static_cast<char*>(ex.workspace(align_up(total, 256) + align_up(scratch, 256) + snap + 1024));
   size_t off = 0;
   for (int s = 0; s < 4; ++s) {
     if (!st[s].staged) continue;
@@ -630,11 +777,25 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
                  "host-to-device copy");
   }
   char* scratch_ptr = ws + align_up(off, 256);
+  char* snap_ptr = snap ? scratch_ptr + align_up(scratch, 256) : nullptr;
 
   const dev::GemmArgs g = build_args(pr, ex, alpha, beta, c_read, st[SA].dev_origin, st[SB].dev_origin,
                                      c_read ? (in_place ? st[SD].dev_origin : st[SC].dev_origin) : nullptr,
                                      st[SD].dev_origin);
-  launch_contraction(pr, ex, g, output_only, scratch_ptr, scratch);
+  if (tune) {
+    const TuneEntry e = autotune_plain(pr, ex, g, scratch_ptr, scratch, snap ? st[SD].dev_origin + d_lo : nullptr,
+                                       snap_ptr, d_bytes);
+    ex.tune[key] = e;
+    pc = e.choice;
+    src = ChoiceSource::Autotuned;
+  }
+  if (pr.scheme == Scheme::Plain && !output_only) {
+    std::lock_guard<std::mutex> lk(pr.mu);
+    pr.last = pc;
+    pr.last_source = src;
+    pr.executed = true;
+  }
+  launch_contraction(pr, ex, g, output_only, pc, scratch_ptr, scratch);
 
   if (st[SD].staged)
     check_cuda(cudaMemcpyAsync(const_cast<void*>(static_cast<const void*>(static_cast<const char*>(st[SD].host) +
@@ -664,6 +825,7 @@ bool groupable(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item&
   if (pr.scheme != Scheme::Plain || p.out_empty || p.k_empty || alpha.is_zero()) return false;
   if (pr.view.H > 65535) return false;
   if (!pr.kernel_pin && dev::use_tiny_batched(pr.view.M, pr.view.N, pr.view.K, pr.view.H)) return false;
+  if (pr.split_pin > 1) return false;  // the grouped kernel does not split K
   const bool c_read = it.c != nullptr && !beta.is_zero();
   const void* ptrs[4] = {it.a, it.b, c_read ? it.c : nullptr, it.d};
   for (const void* q : ptrs)
@@ -688,7 +850,7 @@ uint64_t list_key(int n, Product* const* plans, const Scalar* alpha, const Scala
                            (uint64_t)(uintptr_t)items[i].b,
                            (uint64_t)(uintptr_t)items[i].c,
                            (uint64_t)(uintptr_t)items[i].d,
-                           (uint64_t)plans[i]->kernel_pin,
+                           (uint64_t)plans[i]->kernel_pin | ((uint64_t)plans[i]->autotune << 32),
                            ((uint64_t)plans[i]->scheme << 8) | (uint64_t)plans[i]->ozaki_slices};
     for (uint64_t v : f) key = mix(key, v);
     double sc[4] = {alpha[i].re, alpha[i].im, beta[i].re, beta[i].im};
@@ -699,21 +861,22 @@ uint64_t list_key(int n, Product* const* plans, const Scalar* alpha, const Scala
   return mix(key, (uint64_t)n);
 }
 
-// Builds, captures and caches the graph of the grouped items `idx`; the
-// entry also remembers the items that run individually (`single`).
-Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<int>& idx,
-                                 const std::vector<int>& single, Product* const* plans, const Scalar* alpha,
-                                 const Scalar* beta, const Item* items) {
-  // Families: each item takes the tile that suits its shape inside a full launch.
+// The device side of one grouped submission: descriptors of the items `idx`
+// (each with its tile family under the list's tile `policy`), tiles in
+// decreasing-K order within a family, one persistent launch per family.
+struct GroupSet {
+  void* buf = nullptr;  // descriptors, tile starts, claim counters
+  std::vector<int> family;
+  std::vector<size_t> item0, start0, count;
+  char* counters = nullptr;
+  char* starts = nullptr;
+};
+
+GroupSet build_group_set(Executor& ex, const std::vector<int>& idx, int policy, Product* const* plans,
+                         const Scalar* alpha, const Scalar* beta, const Item* items) {
   std::map<int, std::vector<int>> fam;
-  for (int i : idx) {
-    Product& pr = *plans[i];
-    const int k = pr.kernel_pin ? pr.kernel_pin : dev::choose_grouped_kernel((int)pr.problem.dtype, pr.view.M, pr.view.N);
-    fam[k].push_back(i);
-  }
-  Executor::Graph gr;
-  gr.single = single;
-  std::vector<std::pair<int, std::pair<size_t, size_t>>> launches;  // family, item offset, count
+  for (int i : idx) fam[grouped_family(*plans[i], policy)].push_back(i);
+  GroupSet gs;
   std::vector<dev::GroupItem> host_items;
   std::vector<int64_t> host_starts;
   for (auto& kv : fam) {
@@ -722,7 +885,10 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
                      [&](int a, int b) { return plans[a]->view.K > plans[b]->view.K; });
     int bm = 0, bn = 0;
     dev::plain_tile_shape(kv.first, &bm, &bn);
-    const size_t item0 = host_items.size(), start0 = host_starts.size();
+    gs.family.push_back(kv.first);
+    gs.item0.push_back(host_items.size());
+    gs.start0.push_back(host_starts.size());
+    gs.count.push_back(list.size());
     int64_t acc = 0;
     for (int i : list) {
       Product& pr = *plans[i];
@@ -738,47 +904,138 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
       acc += gi.tiles_m * gi.tiles_n * pr.view.H;
     }
     host_starts.push_back(acc);
-    launches.push_back({kv.first, {item0, start0}});
   }
   const size_t items_bytes = host_items.size() * sizeof(dev::GroupItem);
   const size_t starts_bytes = host_starts.size() * sizeof(int64_t);
-  check_cuda(cudaMalloc(&gr.buf, align_up(items_bytes, 256) + align_up(starts_bytes, 256) + 256 * (launches.size() + 1)),
+  check_cuda(cudaMalloc(&gs.buf, align_up(items_bytes, 256) + align_up(starts_bytes, 256) + 256 * (gs.family.size() + 1)),
              "cudaMalloc(groups)");
-  char* base = static_cast<char*>(gr.buf);
-  // Stream-ordered copies, complete before the capture (see Product::scatters).
-  char* starts = base + align_up(items_bytes, 256);
+  char* base = static_cast<char*>(gs.buf);
+  // Stream-ordered copies, complete before any capture (see Product::scatters).
+  gs.starts = base + align_up(items_bytes, 256);
   cudaError_t up = cudaMemcpyAsync(base, host_items.data(), items_bytes, cudaMemcpyHostToDevice, ex.stream);
   if (up == cudaSuccess)
-    up = cudaMemcpyAsync(starts, host_starts.data(), starts_bytes, cudaMemcpyHostToDevice, ex.stream);
+    up = cudaMemcpyAsync(gs.starts, host_starts.data(), starts_bytes, cudaMemcpyHostToDevice, ex.stream);
   if (up == cudaSuccess) up = cudaStreamSynchronize(ex.stream);
   if (up != cudaSuccess) {
-    cudaFree(gr.buf);
+    cudaFree(gs.buf);
     check_cuda(up, "group descriptor upload");
   }
-  char* counters = starts + align_up(starts_bytes, 256);
-  for (auto& l : launches) {
-    const cudaError_t e = dev::prepare_grouped(l.first);
+  gs.counters = gs.starts + align_up(starts_bytes, 256);
+  for (int f : gs.family) {
+    const cudaError_t e = dev::prepare_grouped(f);
     if (e != cudaSuccess) {
-      cudaFree(gr.buf);
+      cudaFree(gs.buf);
       check_cuda(e, "grouped kernel load");
     }
   }
+  return gs;
+}
+
+cudaError_t launch_group_set(Executor& ex, const GroupSet& gs, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  for (size_t l = 0; l < gs.family.size() && e == cudaSuccess; ++l)
+    e = dev::launch_grouped(gs.family[l], reinterpret_cast<dev::GroupItem*>(gs.buf) + gs.item0[l],
+                            reinterpret_cast<int64_t*>(gs.starts) + gs.start0[l], (int)gs.count[l],
+                            reinterpret_cast<unsigned long long*>(gs.counters + 256 * l), ex.status, ex.num_sms, st);
+  return e;
+}
+
+// A stable text key of a grouped list for the autotuner: the multiset of its
+// items' tuning keys (FNV-1a over the sorted keys).
+std::string list_signature(const std::vector<int>& idx, Product* const* plans, const Scalar* beta,
+                           const Item* items) {
+  std::vector<std::string> keys;
+  keys.reserve(idx.size());
+  for (int i : idx) keys.push_back(tune_key(*plans[i], items[i].c != nullptr && !beta[i].is_zero()));
+  std::sort(keys.begin(), keys.end());
+  uint64_t h = 1469598103934665603ull;
+  for (const auto& k : keys) {
+    for (unsigned char ch : k) {
+      h ^= ch;
+      h *= 1099511628211ull;
+    }
+    h ^= '|';
+    h *= 1099511628211ull;
+  }
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "list-%016llx-n%zu", (unsigned long long)h, idx.size());
+  return buf;
+}
+
+// The tile policy of a grouped list: from the executor's tuning cache, or
+// measured now (every distinct policy run directly, minimum over repetitions
+// after a warm-up; policy 0, the model, kept unless another is 3 % faster).
+// A list whose items read their own D (in-place accumulation) cannot be run
+// repeatedly and keeps the model.
+int list_policy(Executor& ex, const std::vector<int>& idx, Product* const* plans, const Scalar* alpha,
+                const Scalar* beta, const Item* items) {
+  const std::string sig = list_signature(idx, plans, beta, items);
+  const auto hit = ex.list_tune.find(sig);
+  if (hit != ex.list_tune.end()) return hit->second.policy;
+  TuneEntry best;
+  for (int i : idx)
+    if (items[i].c != nullptr && !beta[i].is_zero() && items[i].c == items[i].d) {
+      best.tuned = false;
+      ex.list_tune[sig] = best;
+      return 0;
+    }
+  ProfileOff off(ex);
+  EventPair ev;
+  std::vector<std::vector<int>> seen;
+  for (int policy = 0; policy < GROUP_POLICIES; ++policy) {
+    std::vector<int> fam;
+    for (int i : idx) fam.push_back(grouped_family(*plans[i], policy));
+    if (std::find(seen.begin(), seen.end(), fam) != seen.end()) continue;
+    seen.push_back(fam);
+    GroupSet gs = build_group_set(ex, idx, policy, plans, alpha, beta, items);
+    double t = 0;
+    try {
+      const auto run = [&] { check_cuda(launch_group_set(ex, gs, ex.stream), "grouped launch"); };
+      const double first = time_on_stream(ex, ev, run);
+      t = first;
+      const int reps = tune_reps(first);
+      for (int r = 0; r < reps; ++r) t = std::min(t, time_on_stream(ex, ev, run));
+    } catch (...) {
+      cudaFree(gs.buf);
+      throw;
+    }
+    cudaFree(gs.buf);
+    ++best.tried;
+    if (best.tried == 1 || t < best.ms * 0.97) {
+      best.ms = t;
+      best.policy = policy;
+    }
+  }
+  best.tuned = true;
+  ex.list_tune[sig] = best;
+  return best.policy;
+}
+
+// Builds, captures and caches the graph of the grouped items `idx`; the
+// entry also remembers the items that run individually (`single`).
+Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<int>& idx,
+                                 const std::vector<int>& single, int policy, Product* const* plans,
+                                 const Scalar* alpha, const Scalar* beta, const Item* items) {
+  GroupSet gs = build_group_set(ex, idx, policy, plans, alpha, beta, items);
+  Executor::Graph gr;
+  gr.single = single;
+  gr.buf = gs.buf;
   // Capture on a private non-blocking stream (a capture on a stream that
   // synchronises with the legacy stream would make other threads' legacy-stream
   // work fail meanwhile); the graph is launched on the executor's stream.
-  if (!ex.capture_stream)
-    check_cuda(cudaStreamCreateWithFlags(&ex.capture_stream, cudaStreamNonBlocking), "cudaStreamCreate(capture)");
-  check_cuda(cudaStreamBeginCapture(ex.capture_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-  cudaError_t cap = cudaSuccess;
-  for (size_t l = 0; l < launches.size() && cap == cudaSuccess; ++l) {
-    const int family = launches[l].first;
-    const size_t item0 = launches[l].second.first, start0 = launches[l].second.second;
-    const int count = (int)((l + 1 < launches.size() ? launches[l + 1].second.first : host_items.size()) - item0);
-    cap = dev::launch_grouped(family, reinterpret_cast<dev::GroupItem*>(base) + item0,
-                              reinterpret_cast<int64_t*>(starts) + start0, count,
-                              reinterpret_cast<unsigned long long*>(counters + 256 * l), ex.status, ex.num_sms,
-                              ex.capture_stream);
+  if (!ex.capture_stream) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&ex.capture_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      cudaFree(gr.buf);
+      check_cuda(e, "cudaStreamCreate(capture)");
+    }
   }
+  const cudaError_t begin = cudaStreamBeginCapture(ex.capture_stream, cudaStreamCaptureModeThreadLocal);
+  if (begin != cudaSuccess) {
+    cudaFree(gr.buf);
+    check_cuda(begin, "cudaStreamBeginCapture");
+  }
+  const cudaError_t cap = launch_group_set(ex, gs, ex.capture_stream);
   cudaGraph_t graph = nullptr;
   cudaError_t end = cudaStreamEndCapture(ex.capture_stream, &graph);
   if (cap != cudaSuccess || end != cudaSuccess) {
@@ -827,7 +1084,10 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
       single.insert(single.end(), grouped.begin(), grouped.end());
       grouped.clear();
     } else {
-      gr = &capture_grouped(ex, key, grouped, single, plans, alpha, beta, items);
+      bool tuned = true;
+      for (int i : grouped) tuned = tuned && plans[i]->autotune && !plans[i]->kernel_pin;
+      const int policy = tuned ? list_policy(ex, grouped, plans, alpha, beta, items) : 0;
+      gr = &capture_grouped(ex, key, grouped, single, policy, plans, alpha, beta, items);
     }
   }
   bool staged = false;

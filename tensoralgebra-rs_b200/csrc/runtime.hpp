@@ -46,6 +46,32 @@ struct KernelTimes {
   ~KernelTimes();
 };
 
+// One launch configuration of the plain path: a tile family, a split-K
+// factor (1: none; K is cut into `splits` chunks of `chunk`) or the tiny
+// batched kernel.
+struct PlainChoice {
+  int kernel = 0;
+  int splits = 1;
+  int64_t chunk = 0;
+  bool tiny = false;
+  bool operator==(const PlainChoice& o) const {
+    return kernel == o.kernel && splits == o.splits && chunk == o.chunk && tiny == o.tiny;
+  }
+};
+
+// How a product's launch configuration was decided.
+enum class ChoiceSource { Model = 0, Pinned = 1, Autotuned = 2, Cached = 3 };
+
+// Autotuner result for one Problem signature (single contractions) or one
+// list signature (grouped lists: `policy` is the tile policy of the list).
+struct TuneEntry {
+  PlainChoice choice;
+  int policy = 0;
+  double ms = 0;     // best measured time of one execution (0: not measured)
+  int tried = 0;     // candidates timed
+  bool tuned = true; // false: the model's choice, kept without timing
+};
+
 struct Executor {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -73,6 +99,11 @@ struct Executor {
   };
   std::map<uint64_t, Graph> graphs;
   uint64_t graph_clock = 0;
+  // Autotuner cache, keyed by Problem signature (single contractions) and by
+  // list signature (grouped lists); persisted with save_tuning / load_tuning.
+  std::map<std::string, TuneEntry> tune;
+  std::map<std::string, TuneEntry> list_tune;
+  std::string device_name;
 
   static Executor* create(int device, uintptr_t stream);
   ~Executor();
@@ -92,12 +123,19 @@ struct Product {
   Scheme scheme = Scheme::Plain;
   int ozaki_slices = 0;
   int kernel_pin = 0;
+  int split_pin = 0;       // 0: chosen; 1: never split K; s > 1: exactly s chunks
+  bool autotune = false;   // time the candidates on first execution per executor
+  std::string signature;   // dtype, folded axes and conjugations (scheme added per call)
+  // The launch configuration of the last plain execution and how it was chosen.
+  PlainChoice last{};
+  ChoiceSource last_source = ChoiceSource::Model;
+  bool executed = false;
   // Batch strides of the oriented view for the tiny batched kernel.
   dev::TinyStrides tiny_h{};
   // Unique over the process lifetime (never reused, unlike the address), so a
   // cached grouped graph can never be replayed for a newer plan.
   const uint64_t uid;
-  std::mutex mu;
+  mutable std::mutex mu;
   std::map<int, DeviceScatters> dev;  // per device
   // Adjoint contractions of Plan::vjp, built on first use.
   std::unique_ptr<Product> adj_a, adj_b;
@@ -154,5 +192,32 @@ void drain(Executor& ex);
 std::string kernel_times_json(Executor& ex, bool reset);
 
 void check_cuda(cudaError_t e, const char* what);
+
+// ---- autotuner (autotune.cpp) ----
+
+// A product's Problem signature: dtype, folded axes (extent and the strides
+// of A, B, C, D), orientation and conjugations. Spaces never occur in it.
+std::string problem_signature(const Product& p);
+// The signature under the product's current scheme, plus whether the call
+// reads C: the key of the autotuner cache.
+std::string tune_key(const Product& p, bool c_read);
+// Plain-path candidates for a shape: every tile family of the dtype, each with
+// the split-K factors that keep at most four CTAs per SM in flight, and the
+// tiny batched kernel where it applies. The model's choice comes first.
+std::vector<PlainChoice> plain_candidates(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms);
+// The model's choice (heuristics), honouring the tile and split pins.
+PlainChoice model_choice(const Product& p, int num_sms);
+// Scratch bytes a plain choice needs (split-K partials).
+size_t plain_scratch(const PlainChoice& c, const Product& p);
+// Tile family of a grouped item under a list tile policy (0: model, 1: large
+// tiles, 2: small tiles, 3: tall 128 x 32 tiles for narrow f64/c64 outputs).
+int grouped_family(const Product& p, int policy);
+constexpr int GROUP_POLICIES = 4;
+// The versioned text form of an executor's cache, and its inverse (entries of
+// another device kind are skipped; a malformed file is an error).
+std::string tuning_text(const Executor& ex);
+void load_tuning_text(Executor& ex, const std::string& text);
+std::string tuning_json(const Executor& ex);
+std::string choice_name(const PlainChoice& c, int dtype);
 
 }  // namespace tprims

@@ -69,7 +69,9 @@ ABI_SYMBOLS = [
     "tprims_b200_product_scatter", "tprims_b200_executor_set_profiling", "tprims_b200_executor_kernel_times",
     "tprims_b200_executor_set_grouping", "tprims_b200_executor_set_workspace_limit",
     "tprims_b200_executor_selftest_wait", "tprims_b200_executor_probe_peak",
-    "tprims_b200_execute_product_noalloc",
+    "tprims_b200_execute_product_noalloc", "tprims_b200_product_set_split_k", "tprims_b200_product_set_autotune",
+    "tprims_b200_executor_save_tuning", "tprims_b200_executor_load_tuning", "tprims_b200_executor_clear_tuning",
+    "tprims_b200_executor_tuning",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -130,6 +132,13 @@ lib.TAPP_execute_batched_product.argtypes = [
 ]
 lib.tprims_b200_product_set_precision.argtypes = [_ip, C.c_int, C.c_int]
 lib.tprims_b200_product_set_tile.argtypes = [_ip, C.c_int]
+lib.tprims_b200_product_set_split_k.argtypes = [_ip, C.c_int]
+lib.tprims_b200_product_set_autotune.argtypes = [_ip, C.c_int]
+lib.tprims_b200_executor_save_tuning.argtypes = [_ip, C.c_char_p]
+lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
+lib.tprims_b200_executor_clear_tuning.argtypes = [_ip]
+lib.tprims_b200_executor_tuning.argtypes = [_ip, C.c_char_p, C.c_size_t]
+lib.tprims_b200_executor_tuning.restype = C.c_size_t
 lib.tprims_b200_product_report.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_product_report.restype = C.c_size_t
 lib.tprims_b200_product_from_dot_general.argtypes = [
@@ -259,12 +268,33 @@ class Executor:
     ``cudaStream_t`` (0: the executor creates its own). ``sync=True`` is the
     TAPP contract (every execute returns after the work is done)."""
 
-    def __init__(self, device: Optional[int] = None, stream: int = 0, sync: bool = True):
+    def __init__(self, device: Optional[int] = None, stream: int = 0, sync: bool = True,
+                 tuning: Optional[str] = None):
         h = _ip(0)
         check(lib.tprims_b200_executor_create(C.byref(h), -1 if device is None else int(device), int(stream)))
         self.h = h.value
         if not sync:
             check(lib.tprims_b200_executor_set_sync(self.h, 0))
+        if tuning is not None:
+            self.load_tuning(tuning)
+
+    def save_tuning(self, path: str):
+        """Write the autotuner cache to ``path`` (versioned text)."""
+        check(lib.tprims_b200_executor_save_tuning(self.h, os.fsencode(path)))
+
+    def load_tuning(self, path: str):
+        """Add the entries of a cache file written on the same kind of device."""
+        check(lib.tprims_b200_executor_load_tuning(self.h, os.fsencode(path)))
+
+    def clear_tuning(self):
+        check(lib.tprims_b200_executor_clear_tuning(self.h))
+
+    def tuning(self) -> dict:
+        """The autotuner cache: {"single": {signature: entry}, "list": {...}}."""
+        n = lib.tprims_b200_executor_tuning(self.h, None, 0)
+        buf = C.create_string_buffer(n + 64)
+        lib.tprims_b200_executor_tuning(self.h, buf, n + 64)
+        return json.loads(buf.value.decode())
 
     @property
     def stream(self) -> int:
@@ -378,6 +408,13 @@ class TensorProduct:
     def set_kernel(self, kernel_id: int):
         check(lib.tprims_b200_product_set_tile(self.h, int(kernel_id)))
 
+    def set_split_k(self, splits: int):
+        """0: chosen; 1: never split K; 2..64: that many K chunks."""
+        check(lib.tprims_b200_product_set_split_k(self.h, int(splits)))
+
+    def set_autotune(self, on: bool):
+        check(lib.tprims_b200_product_set_autotune(self.h, 1 if on else 0))
+
     def report(self) -> dict:
         n = lib.tprims_b200_product_report(self.h, None, 0)
         buf = C.create_string_buffer(n + 1)
@@ -475,11 +512,15 @@ class DotGeneral:
 @dataclass
 class PlanConfig:
     """``plan/config.rs`` PlanConfig, with the B200 knobs: the precision scheme
-    (plain / bf16x3 / bf16x6 / ozaki-int8) and an optional pinned kernel."""
+    (plain / bf16x3 / bf16x6 / ozaki-int8), optional tile and split-K pins, and
+    the autotuner switch (tile family and split-K measured on first execution
+    per executor and cached by Problem signature)."""
 
     precision: int = PREC_PLAIN
     ozaki_slices: int = 0
     kernel: int = 0
+    split_k: int = 0
+    autotune: bool = False
 
 
 class Problem:
@@ -534,6 +575,10 @@ class Plan:
             self.product.set_precision(config.precision, config.ozaki_slices)
         if config.kernel:
             self.product.set_kernel(config.kernel)
+        if config.split_k:
+            self.product.set_split_k(config.split_k)
+        if config.autotune:
+            self.product.set_autotune(True)
 
     def report(self) -> dict:
         return self.product.report()

@@ -283,3 +283,55 @@ def test_launch_choices_reported_per_plan(tp):
     hb = 1 << 20
     had = product(1, [hb], [1], [9], [hb], [1], [9], [hb], [1], [9])
     assert "tiny-batched" in had.report()["family"]
+
+
+def _gemm_product(tp, m, n, k, dt=1, lda=None):
+    """D[m,n] = sum_k A[m,k] B[k,n], column-major; `lda` widens A's column stride."""
+    lda = lda or m
+    h = tp.Handle()
+    infos = [tp.TensorInfo(dt, [m, k], [1, lda]), tp.TensorInfo(dt, [k, n], [1, k]),
+             tp.TensorInfo(dt, [m, n], [1, m]), tp.TensorInfo(dt, [m, n], [1, m])]
+    p = tp.TensorProduct.create(h, (0, infos[0], [0, 2]), (0, infos[1], [2, 1]), (0, infos[2], [0, 1]),
+                                (0, infos[3], [0, 1]))
+    p._keep = (h, infos)
+    return p
+
+
+def test_problem_signature_keys_the_folded_layout(tp):
+    """The autotuner's cache key: equal for two plans of the same folded
+    layout, different when a stride, an extent or the dtype differs."""
+    a = _gemm_product(tp, 300, 200, 100).report()
+    b = _gemm_product(tp, 300, 200, 100).report()
+    assert a["signature"] == b["signature"] and " " not in a["signature"]
+    assert a["signature"].startswith("f64;")
+    assert _gemm_product(tp, 300, 200, 100, lda=320).report()["signature"] != a["signature"]
+    assert _gemm_product(tp, 300, 200, 101).report()["signature"] != a["signature"]
+    assert _gemm_product(tp, 300, 200, 100, dt=0).report()["signature"] != a["signature"]
+
+
+def test_split_k_and_autotune_switches(tp):
+    """PlanConfig's pins and autotune switch: the split-K pin is reported
+    before any execution as the pinned choice (chunks of whole 64-deep blocks),
+    out-of-range factors are refused, and an autotuning plan reports the model's
+    choice until it has run."""
+    p = _gemm_product(tp, 512, 512, 4096)
+    assert p.report()["choice"] == "model" and p.report()["autotune"] is False
+    p.set_split_k(4)
+    rep = p.report()
+    assert rep["choice"] == "pinned" and rep["split_k"] == 4
+    p.set_split_k(1)
+    assert p.report()["split_k"] == 1
+    p.set_split_k(3)
+    assert p.report()["split_k"] == 3  # chunks of 1408 = 22 blocks of 64
+    for bad in (-1, 65):
+        with pytest.raises(tp.TprimsError) as ei:
+            p.set_split_k(bad)
+        assert ei.value.status == 1  # INVALID_ARGUMENT
+    q = _gemm_product(tp, 512, 512, 4096)
+    q.set_autotune(True)
+    assert q.report()["autotune"] is True and q.report()["choice"] == "model"
+    plan = tp.Plan(tp.Problem.from_labels(1, tp.OperandSpec(tp.LayoutSpec([8, 8], [1, 8])),
+                                          tp.OperandSpec(tp.LayoutSpec([8, 8], [1, 8])),
+                                          tp.OperandSpec(tp.LayoutSpec([8, 8], [1, 8])), [0, 2], [2, 1], [0, 1]),
+                   tp.PlanConfig(autotune=True, split_k=1))
+    assert plan.report()["autotune"] is True and plan.report()["choice"] == "pinned"

@@ -507,7 +507,7 @@ extern "C" TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan
 extern "C" TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id) {
   return ffi([&] {
     Product& p = product_of(plan);
-    if (kernel_id < 0 || kernel_id > dev::PLAIN_C64_DMMA_128x32)
+    if (kernel_id < 0 || kernel_id > dev::PLAIN_LAST)
       throw Error(ERR_INVALID_ARGUMENT, "unknown kernel id " + std::to_string(kernel_id));
     p.kernel_pin = kernel_id;
   });

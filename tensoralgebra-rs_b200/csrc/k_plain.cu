@@ -5,7 +5,10 @@
 // pack/pack.rs:152-203): each K step reads A'[m, k] = A[h_a + a_m[m] + a_k[k]]
 // and B'[k, n] through the scatter vectors straight into shared memory, with
 // threads running along whichever index is unit-stride in memory, and folds
-// conjugation into the sign of the imaginary plane. The register tile replaces
+// conjugation into the sign of the imaginary plane. Real tiles stage the next
+// K step in registers (TileGather); complex tiles and grouped f64 lists fill a
+// ring of four shared-memory stages with cp.async (AsyncGather), which keeps
+// three stages of global loads in flight. The register tile replaces
 // the microkernels (kernels/reference/scalar.rs:31-175): FP32 FFMA for f32,
 // FP64 DMMA (mma.sync m8n8k4) for f64, and four real products per complex MAC
 // for c32/c64 (the planar method, writeback.rs:54-97 Planar). The epilogue is
@@ -293,9 +296,17 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <bool CPLX, int ROWS, int BK, int NT>
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_addr_u32(smem)), "l"(gmem),
+               "r"(ok ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(double* smem, const double* gmem, bool ok) { cp_async8(smem, gmem, ok); }
+__device__ __forceinline__ void cp_async_elem(float* smem, const float* gmem, bool ok) { cp_async4(smem, gmem, ok); }
+
+template <class R, bool CPLX, int ROWS, int BK, int NT>
 struct AsyncGather {
-  using T = typename Elem<double, CPLX>::type;
+  using T = typename Elem<R, CPLX>::type;
   static constexpr int PER = ROWS * BK / NT;
   static_assert(ROWS * BK % NT == 0 && NT % BK == 0 && NT % ROWS == 0, "one k or one row per thread");
   int64_t var[PER];
@@ -336,16 +347,16 @@ struct AsyncGather {
     }
   }
   // Copies of this thread's elements of the stage whose offsets are loaded.
-  __device__ inline void issue(const T* base, double* s_re, double* s_im, int stride, int kfast, int tid) const {
+  __device__ inline void issue(const T* base, R* s_re, R* s_im, int stride, int kfast, int tid) const {
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
       int kk, rr;
       coords(tid + j * NT, kfast, kk, rr);
       const bool ok = var[j] != INT64_MIN && fixed != INT64_MIN;
       const T* src = ok ? base + var[j] + fixed : base;  // not read when !ok
-      const double* d = reinterpret_cast<const double*>(src);
-      cp_async8(s_re + kk * stride + rr, d, ok);
-      if (CPLX) cp_async8(s_im + kk * stride + rr, d + 1, ok);
+      const R* d = reinterpret_cast<const R*>(src);
+      cp_async_elem(s_re + kk * stride + rr, d, ok);
+      if (CPLX) cp_async_elem(s_im + kk * stride + rr, d + 1, ok);
     }
   }
 };
@@ -404,8 +415,8 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
 
   const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
   const T* Bb = static_cast<const T*>(g.B) + g.s.h_b[h];
-  AsyncGather<CPLX, BM, BK, NT> ga;
-  AsyncGather<CPLX, BN, BK, NT> gb;
+  AsyncGather<double, CPLX, BM, BK, NT> ga;
+  AsyncGather<double, CPLX, BN, BK, NT> gb;
 
   double cr[TI][TJ][4], ci[CPLX ? TI : 1][CPLX ? TJ : 1][4];
 #pragma unroll
@@ -509,6 +520,200 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
           epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
                                      Db + dm_s[rr] + dn_s[cc]);
       }
+}
+
+// ---------------------------------------------------------------- SIMT (FFMA), cp.async ring
+
+// Shape of the FP32 stage ring (dynamic shared memory): planar [k][row]
+// stages, rows padded by 4 floats.
+template <bool CPLX, int BM, int BN, int BK>
+struct SimtRing {
+  static constexpr int SA = BM + 4, SB = BN + 4;
+  static constexpr int NPL = CPLX ? 2 : 1;
+  static constexpr int STAGES = 4;
+  static constexpr int A_STAGE = NPL * BK * SA, B_STAGE = NPL * BK * SB;  // floats
+  static constexpr int BYTES = STAGES * (A_STAGE + B_STAGE) * 4;
+};
+
+// FP32 register tile fed by a ring of STAGES shared-memory stages filled with
+// cp.async (the gather of TileGather, without staging through registers), so
+// the global loads of three stages are in flight behind the FFMA work. Each
+// thread owns a TM x TN tile (two halves of TM/2 rows and TN/2 columns, so the
+// fragment reads are vector loads without bank conflicts) and accumulates each
+// BK-deep stage into a fresh register tile that is then added to the total
+// (FP32 error near u * (sqrt(BK) + sqrt(K / BK))). CA / CB: conjugated A' / B'
+// (complex only), folded into the signs of the FFMAs at compile time.
+template <int BM, int BN>
+struct TileScatters {
+  int64_t am[BM], bn[BN], dm[BM], cm[BM], dn[BN], cn[BN];
+};
+
+template <bool CPLX, bool CA, bool CB, int BM, int BN, int BK, int TM, int TN>
+__device__ __forceinline__ void simt_tile_async_body(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                                     int64_t split, TileScatters<BM, BN>& sc) {
+  using R = float;
+  using Ring = SimtRing<CPLX, BM, BN, BK>;
+  constexpr int NT = (BM / TM) * (BN / TN);
+  constexpr int SA = Ring::SA, SB = Ring::SB, NPL = Ring::NPL, STAGES = Ring::STAGES;
+  using T = typename Elem<R, CPLX>::type;
+
+  extern __shared__ __align__(16) float simt_ring[];
+  R(*As)[NPL][BK * SA] = reinterpret_cast<R(*)[NPL][BK * SA]>(simt_ring);
+  R(*Bs)[NPL][BK * SB] = reinterpret_cast<R(*)[NPL][BK * SB]>(simt_ring + STAGES * Ring::A_STAGE);
+  int64_t *am_s = sc.am, *bn_s = sc.bn, *dm_s = sc.dm, *cm_s = sc.cm, *dn_s = sc.dn, *cn_s = sc.cn;
+
+  const int tid = threadIdx.x;
+  const int64_t m0 = mtile * BM, n0 = ntile * BN;
+  for (int i = tid; i < BM; i += NT) {
+    const int64_t m = m0 + i;
+    const bool ok = m < g.M;
+    am_s[i] = ok ? g.s.a_m[m] : 0;
+    dm_s[i] = ok ? g.s.d_m[m] : 0;
+    cm_s[i] = ok ? g.s.c_m[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int64_t n = n0 + i;
+    const bool ok = n < g.N;
+    bn_s[i] = ok ? g.s.b_n[n] : 0;
+    dn_s[i] = ok ? g.s.d_n[n] : 0;
+    cn_s[i] = ok ? g.s.c_n[n] : 0;
+  }
+  __syncthreads();
+
+  const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
+  const T* Bb = static_cast<const T*>(g.B) + g.s.h_b[h];
+  AsyncGather<R, CPLX, BM, BK, NT> ga;
+  AsyncGather<R, CPLX, BN, BK, NT> gb;
+
+  constexpr int HM = TM / 2, HN = TN / 2;
+  const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+  R tot_re[TM][TN], tot_im[CPLX ? TM : 1][CPLX ? TN : 1];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      tot_re[i][j] = R(0);
+      if (CPLX) tot_im[i][j] = R(0);
+    }
+
+  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
+  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
+  const int64_t nt = (ke - kb + BK - 1) / BK;
+  ga.init(am_s, m0, g.M, g.a_kfast, tid);
+  gb.init(bn_s, n0, g.N, g.b_kfast, tid);
+#pragma unroll
+  for (int sidx = 0; sidx < STAGES - 1; ++sidx) {
+    if (sidx < nt) {
+      ga.load_idx(g.s.a_k, kb + sidx * BK, ke, g.a_kfast, tid);
+      gb.load_idx(g.s.b_k, kb + sidx * BK, ke, g.b_kfast, tid);
+      ga.issue(Ab, As[sidx][0], As[sidx][NPL - 1], SA, g.a_kfast, tid);
+      gb.issue(Bb, Bs[sidx][0], Bs[sidx][NPL - 1], SB, g.b_kfast, tid);
+    }
+    cp_async_commit();
+  }
+
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t tp = t + STAGES - 1;
+    if (tp < nt) {
+      ga.load_idx(g.s.a_k, kb + tp * BK, ke, g.a_kfast, tid);
+      gb.load_idx(g.s.b_k, kb + tp * BK, ke, g.b_kfast, tid);
+    }
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    if (tp < nt) {
+      const int pb = (int)(tp % STAGES);
+      ga.issue(Ab, As[pb][0], As[pb][NPL - 1], SA, g.a_kfast, tid);
+      gb.issue(Bb, Bs[pb][0], Bs[pb][NPL - 1], SB, g.b_kfast, tid);
+    }
+    cp_async_commit();
+    const int buf = (int)(t % STAGES);
+    R acc_re[TM][TN], acc_im[CPLX ? TM : 1][CPLX ? TN : 1];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        acc_re[i][j] = R(0);
+        if (CPLX) acc_im[i][j] = R(0);
+      }
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      R ar[TM], br[TN], ai[CPLX ? TM : 1], bi[CPLX ? TN : 1];
+#pragma unroll
+      for (int i = 0; i < HM; ++i) {
+        ar[i] = As[buf][0][kk * SA + tx * HM + i];
+        ar[HM + i] = As[buf][0][kk * SA + BM / 2 + tx * HM + i];
+        if (CPLX) {
+          ai[i] = As[buf][NPL - 1][kk * SA + tx * HM + i];
+          ai[HM + i] = As[buf][NPL - 1][kk * SA + BM / 2 + tx * HM + i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < HN; ++j) {
+        br[j] = Bs[buf][0][kk * SB + ty * HN + j];
+        br[HN + j] = Bs[buf][0][kk * SB + BN / 2 + ty * HN + j];
+        if (CPLX) {
+          bi[j] = Bs[buf][NPL - 1][kk * SB + ty * HN + j];
+          bi[HN + j] = Bs[buf][NPL - 1][kk * SB + BN / 2 + ty * HN + j];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+          if (CPLX) {
+            // (ar + i sa ai)(br + i sb bi), sa = -1 when A' is conjugated, sb likewise.
+            acc_re[i][j] = fma(ar[i], br[j], acc_re[i][j]);
+            acc_re[i][j] = fma((CA != CB) ? ai[i] : -ai[i], bi[j], acc_re[i][j]);
+            acc_im[i][j] = fma(CB ? -ar[i] : ar[i], bi[j], acc_im[i][j]);
+            acc_im[i][j] = fma(CA ? -ai[i] : ai[i], br[j], acc_im[i][j]);
+          } else {
+            acc_re[i][j] = fma(ar[i], br[j], acc_re[i][j]);
+          }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        tot_re[i][j] += acc_re[i][j];
+        if (CPLX) tot_im[i][j] += acc_im[i][j];
+      }
+  }
+  cp_async_wait<0>();  // no copy may still target the ring when the next tile starts
+
+  const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
+  T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int rr = (i < HM) ? (tx * HM + i) : (BM / 2 + tx * HM + (i - HM));
+    if (m0 + rr >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int cc = (j < HN) ? (ty * HN + j) : (BN / 2 + ty * HN + (j - HN));
+      if (n0 + cc >= g.N) continue;
+      if (g.partial)
+        Elem<R, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
+                             tot_re[i][j], CPLX ? tot_im[i][j] : R(0));
+      else
+        epilogue_store<R, CPLX>(g.e, tot_re[i][j], CPLX ? tot_im[i][j] : R(0), Cb + cm_s[rr] + cn_s[cc],
+                              Db + dm_s[rr] + dn_s[cc]);
+    }
+  }
+}
+
+// The conjugation variant of a complex tile is chosen per tile.
+template <bool CPLX, int BM, int BN, int BK, int TM, int TN>
+__device__ __forceinline__ void simt_tile_async(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
+                                                int64_t split = 0) {
+  __shared__ TileScatters<BM, BN> sc;
+  if (!CPLX || (!g.conj_a && !g.conj_b))
+    simt_tile_async_body<CPLX, false, false, BM, BN, BK, TM, TN>(g, h, mtile, ntile, split, sc);
+  else if (g.conj_a && !g.conj_b)
+    simt_tile_async_body<CPLX, true, false, BM, BN, BK, TM, TN>(g, h, mtile, ntile, split, sc);
+  else if (!g.conj_a)
+    simt_tile_async_body<CPLX, false, true, BM, BN, BK, TM, TN>(g, h, mtile, ntile, split, sc);
+  else
+    simt_tile_async_body<CPLX, true, true, BM, BN, BK, TM, TN>(g, h, mtile, ntile, split, sc);
 }
 
 // Register-staged variant (used for real f64): 4 warps in a 2x2 arrangement,
@@ -694,6 +899,18 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(Gem
   }
 }
 
+template <bool CPLX, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_ring_gemm_kernel(GemmArgs g) {
+  const int64_t tn = (g.N + BN - 1) / BN, tm = (g.M + BM - 1) / BM;
+  const int64_t total = tn * tm * g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1);
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int64_t nt, mt, z;
+    tile_coords(t, tn, tm, nt, mt, z);
+    simt_tile_async<CPLX, BM, BN, BK, TM, TN>(g, z % g.H, mt, nt, z / g.H);
+    __syncthreads();  // the next tile rewrites the shared scatter arrays
+  }
+}
+
 // Three CTAs per SM (at most 170 registers a thread): twelve warps to hide the
 // gather and shared-memory latency around the DMMA pipe.
 template <bool CPLX, int WM, int WN, int BK>
@@ -777,6 +994,15 @@ struct SimtTileOp {
     simt_tile<R, CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
   }
 };
+template <bool CPLX, int BM, int BN, int BK, int TM, int TN>
+struct SimtRingTileOp {
+  static constexpr int NT = (BM / TM) * (BN / TN);
+  static constexpr int SMEM = SimtRing<CPLX, BM, BN, BK>::BYTES;
+  static constexpr int MIN_BLOCKS = 1;
+  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
+    simt_tile_async<CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
+  }
+};
 template <bool CPLX, int WM, int WN, int BK>
 struct DmmaTileOp {
   // Grouped lists (many short-K tiles) take the cp.async ring for real f64 too.
@@ -803,7 +1029,7 @@ const char* plain_kernel_name(int k) {
     case PLAIN_F32_SIMT_64x64: return "sm100.f32.simt.64x64x16";
     case PLAIN_F64_DMMA_64x64: return "sm100.f64.dmma884.64x64x16";
     case PLAIN_F64_DMMA_32x32: return "sm100.f64.dmma884.32x32x16";
-    case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.planar.64x64x16";
+    case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.ring.planar.64x64x16";
     case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.planar.64x32x8";
     case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
     case PLAIN_F64_DMMA_128x32: return "sm100.f64.dmma884.128x32x16";
@@ -936,6 +1162,18 @@ cudaError_t launch_dmma(const GemmArgs& g, cudaStream_t st) {
 }
 }  // namespace
 
+namespace {
+template <bool CPLX, int BM, int BN, int BK, int TM, int TN>
+cudaError_t launch_simt_ring(const GemmArgs& g, cudaStream_t st) {
+  constexpr int bytes = SimtRing<CPLX, BM, BN, BK>::BYTES;
+  const cudaError_t e = cudaFuncSetAttribute(simt_ring_gemm_kernel<CPLX, BM, BN, BK, TM, TN>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  simt_ring_gemm_kernel<CPLX, BM, BN, BK, TM, TN><<<grid_for<BM, BN>(g), (BM / TM) * (BN / TN), bytes, st>>>(g);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.H <= 0) return cudaSuccess;
   switch (kernel) {
@@ -949,8 +1187,7 @@ cudaError_t launch_plain_gemm(int dtype, int kernel, const GemmArgs& g, cudaStre
       break;
     case PLAIN_C32_SIMT_64x64:
       if (dtype != 2) return cudaErrorInvalidValue;
-      simt_gemm_kernel<float, true, 64, 64, 16, 4, 4><<<grid_for<64, 64>(g), 256, 0, st>>>(g);
-      break;
+      return launch_simt_ring<true, 64, 64, 16, 4, 4>(g, st);
     case PLAIN_F64_DMMA_64x64:
       if (dtype != 1) return cudaErrorInvalidValue;
       return launch_dmma<false, 32, 32, 16>(g, st);
@@ -1021,7 +1258,7 @@ void grouped_launch_op(int kernel, const GroupItem* items, const int64_t* tile_s
 
 using GSimtF32L = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
 using GSimtF32S = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
-using GSimtC32 = SimtTileOp<float, true, 64, 64, 16, 4, 4>;
+using GSimtC32 = SimtRingTileOp<true, 64, 64, 16, 4, 4>;
 using GDmmaF64L = DmmaTileOp<false, 32, 32, 16>;
 using GDmmaF64S = DmmaTileOp<false, 16, 16, 16>;
 using GDmmaC64L = DmmaTileOp<true, 32, 16, 8>;

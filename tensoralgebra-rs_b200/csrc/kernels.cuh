@@ -66,6 +66,7 @@ enum PlainKernel : int {
   PLAIN_C64_DMMA_32x32 = 7,
   PLAIN_F64_DMMA_128x32 = 8,  // tall tiles for N <= 32 (grouped lists)
   PLAIN_C64_DMMA_128x32 = 9,
+  PLAIN_LAST = 9,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).

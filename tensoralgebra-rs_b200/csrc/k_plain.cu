@@ -943,19 +943,38 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
   __shared__ long long claimed;
   __shared__ int item_s;
   __shared__ int stop;
+  __shared__ int sg_item;  // the item whose arguments `sg` holds
+  if (threadIdx.x == 0) sg_item = -1;
   const int64_t total = tile_start[nitems];
   const uint64_t t_start = globaltimer_ns();
   constexpr uint64_t LIMIT_NS = 60000000000ull;  // 60 s for one grouped launch
   for (int64_t iter = 0;; ++iter) {
-    if (threadIdx.x == 0) {
-      stop = 0;
-      claimed = (long long)atomicAdd(counter, 1ull);
-      int lo = 0, hi = nitems - 1;  // the item whose tile range holds `claimed`
+    if (threadIdx.x < 32) {
+      // Claim a tile, then find the item whose tile range holds it (the last
+      // index with tile_start <= claimed) by a 32-way search across the warp:
+      // each round probes 32 evenly spaced entries at once, so a list of n
+      // items costs about log32(n) dependent loads instead of log2(n).
+      const int lane = threadIdx.x;
+      long long c = 0;
+      if (lane == 0) c = (long long)atomicAdd(counter, 1ull);
+      c = __shfl_sync(0xffffffffu, c, 0);
+      int lo = 0, hi = nitems - 1;
       while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_start[mid] <= claimed) lo = mid; else hi = mid - 1;
+        const int step = (hi - lo + 32) / 32;
+        const int pos = lo + lane * step;
+        const bool le = pos <= hi && tile_start[pos] <= c;
+        const unsigned m = __ballot_sync(0xffffffffu, le) | 1u;  // tile_start[lo] <= c holds for lo
+        lo += (31 - __clz(m)) * step;
+        hi = min(hi, lo + step - 1);
       }
-      item_s = lo;
+      if (lane == 0) {
+        stop = 0;
+        claimed = c;
+        item_s = lo;
+      }
+    }
+    if (threadIdx.x == 0) {
+      const int lo = item_s;
       if (claimed < total) {
         const int64_t local = claimed - tile_start[lo];
         const int64_t nt = items[lo].tiles_m * items[lo].tiles_n * items[lo].g.H;
@@ -972,12 +991,13 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
     const long long t = claimed;
     if (t >= total || stop) break;
     const int it = item_s;
-    {
+    if (it != sg_item) {  // uniform: both values were written before the barrier above
       const int4* src = reinterpret_cast<const int4*>(&items[it].g);
       int4* dst = reinterpret_cast<int4*>(&sg);
       for (int w = threadIdx.x; w < (int)(sizeof(GemmArgs) / 16); w += NT) dst[w] = src[w];
+      __syncthreads();
+      if (threadIdx.x == 0) sg_item = it;
     }
-    __syncthreads();
     const int64_t local = t - tile_start[it];
     const int64_t tn = items[it].tiles_n, tm = items[it].tiles_m;
     Tile::run(sg, local / (tm * tn), (local / tn) % tm, local % tn);

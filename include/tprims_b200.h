@@ -318,6 +318,50 @@ typedef struct {
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_contract_batched(TAPP_executor exec, int n,
                                                            const tprims_b200_batch_item* items);
 
+/* N-ary contraction networks. The reference keeps the N-ary layer (einsum)
+   above its stack (docs/architecture.md:54): its callers contract a network
+   pair by pair through Problem::from_labels / Plan::execute_into. These calls
+   are that caller on the GPU. A network is created from its input tensors
+   (extents, signed element strides or NULL for column-major, labels, and
+   TAPP_IDENTITY / TAPP_CONJUGATE per input), the output's layout and labels,
+   and a pairwise path of n_steps = n_inputs - 1 steps given as 2 * n_steps
+   positions in the current operand list (opt_einsum convention: both operands
+   are removed and the result appended); n_steps = 0 chooses a greedy path.
+   Labels follow the TAPP rules per step: labels shared by the two operands
+   and needed later are batch, others shared are contracted, a label of one
+   operand needed nowhere else is summed, an output label found in no input is
+   UNSUPPORTED, extents of one label must agree (SHAPE). Intermediates are
+   dense column-major in a device arena of tprims_b200_network_workspace_size
+   bytes (the caller's `workspace`, or the network's own when NULL).
+   Execution computes out = alpha * network + beta * out (out is read only when
+   beta != 0), synchronously like TAPP_execute_product; inputs and out may be
+   host or device memory. tprims_b200_networks_execute runs a list of
+   networks, step s of every network as one grouped submission. */
+typedef intptr_t tprims_b200_network;
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_create(tprims_b200_network* net, TAPP_datatype dtype, int n_inputs,
+                                                         const int* nmodes, const int64_t* const* extents,
+                                                         const int64_t* const* strides,
+                                                         const int64_t* const* labels, const TAPP_element_op* ops,
+                                                         int out_nmode, const int64_t* out_extents,
+                                                         const int64_t* out_strides, const int64_t* out_labels,
+                                                         int n_steps, const int* path);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_destroy(tprims_b200_network net);
+/* Precision scheme and autotuning of every step's plan (as for a product). */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_set_precision(tprims_b200_network net, int scheme, int slices);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_set_autotune(tprims_b200_network net, int on);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_workspace_size(tprims_b200_network net, size_t* bytes);
+/* JSON: the path, each step's operands, labels, extents, arena offset and plan
+   report. Returns the full length, like snprintf. */
+TPRIMS_B200_EXPORT size_t tprims_b200_network_report(tprims_b200_network net, char* buf, size_t maxlen);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_network_execute(tprims_b200_network net, TAPP_executor exec,
+                                                          const void* alpha, const void* const* inputs,
+                                                          const void* beta, void* out, void* workspace);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_networks_execute(TAPP_executor exec, int n, const tprims_b200_network* nets,
+                                                           const void* const* alphas,
+                                                           const void* const* const* inputs,
+                                                           const void* const* betas, void* const* outs,
+                                                           void* const* workspaces);
+
 /* Plan::vjp. For D = alpha*op_A(A)*op_B(B) (+ beta*C), given the cotangent dD,
    write dA (when non-NULL) and dB (when non-NULL) in the layouts of A and B:
    dA = conj-correct adjoint contraction of dD with B, scattered onto A's

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/tprims_b200.h"
+#include "network.hpp"
 #include "runtime.hpp"
 
 using namespace tprims;
@@ -587,6 +588,139 @@ extern "C" TAPP_error tprims_b200_contract_batched(TAPP_executor exec, int n, co
     Executor& ex = resolve_exec(exec)->get();
     execute_items(ex, n, ps.data(), als.data(), bes.data(), its.data());
   });
+}
+
+// ---- N-ary networks
+
+namespace {
+Network& network_of(tprims_b200_network net) {
+  if (net == 0) null_arg("network");
+  return *reinterpret_cast<Network*>(net);
+}
+}  // namespace
+
+extern "C" TAPP_error tprims_b200_network_create(tprims_b200_network* net, TAPP_datatype dtype, int n_inputs,
+                                                 const int* nmodes, const int64_t* const* extents,
+                                                 const int64_t* const* strides, const int64_t* const* labels,
+                                                 const TAPP_element_op* ops, int out_nmode,
+                                                 const int64_t* out_extents, const int64_t* out_strides,
+                                                 const int64_t* out_labels, int n_steps, const int* path) {
+  return ffi([&] {
+    if (!net) null_arg("network out-parameter");
+    if (n_inputs < 0 || out_nmode < 0 || n_steps < 0) throw Error(ERR_SHAPE, "negative count");
+    if (n_inputs > 0 && (!nmodes || !extents || !strides || !labels)) null_arg("input descriptions");
+    const DType dt = dtype_from(dtype);
+    auto operand = [&](int rank, const int64_t* e, const int64_t* st, const int64_t* l, bool conj,
+                       const std::string& what) {
+      if (rank < 0) throw Error(ERR_SHAPE, what + ": negative rank");
+      if (rank > 0 && (!e || !l)) null_arg(what + " extents or labels");
+      NetworkOperand o;
+      std::vector<int64_t> dense;
+      if (rank > 0 && !st) {  // null strides: column-major
+        int64_t acc = 1;
+        for (int k = 0; k < rank; ++k) {
+          dense.push_back(acc);
+          acc *= std::max<int64_t>(e[k], 1);
+        }
+        st = dense.data();
+      }
+      o.op.layout = layout_from_signed(e, st, rank, 0);
+      o.op.conj = conj;
+      o.labels.assign(l, l + rank);
+      return o;
+    };
+    std::vector<NetworkOperand> ins;
+    for (int i = 0; i < n_inputs; ++i)
+      ins.push_back(operand(nmodes[i], extents[i], strides[i], labels[i],
+                            ops ? op_conj(ops[i], "a network input") : false, "input " + std::to_string(i)));
+    NetworkOperand out = operand(out_nmode, out_extents, out_strides, out_labels, false, "output");
+    std::vector<std::pair<int, int>> pth;
+    if (n_steps > 0) {
+      if (!path) null_arg("path");
+      for (int s = 0; s < n_steps; ++s) pth.push_back({path[2 * s], path[2 * s + 1]});
+    }
+    *net = reinterpret_cast<tprims_b200_network>(Network::create(dt, std::move(ins), std::move(out), std::move(pth)));
+  });
+}
+
+extern "C" TAPP_error tprims_b200_network_destroy(tprims_b200_network net) {
+  return ffi([&] {
+    if (net == 0) null_arg("network");
+    delete reinterpret_cast<Network*>(net);
+  });
+}
+
+extern "C" TAPP_error tprims_b200_network_set_precision(tprims_b200_network net, int scheme, int slices) {
+  return ffi([&] {
+    Network& n = network_of(net);
+    for (auto& s : n.steps) {
+      const TAPP_error e = tprims_b200_product_set_precision(reinterpret_cast<TAPP_tensor_product>(s.plan.get()),
+                                                           scheme, slices);
+      if (e != TPRIMS_OK) throw Error(e, g_last_error);
+    }
+  });
+}
+
+extern "C" TAPP_error tprims_b200_network_set_autotune(tprims_b200_network net, int on) {
+  return ffi([&] {
+    for (auto& s : network_of(net).steps) s.plan->autotune = on != 0;
+  });
+}
+
+extern "C" TAPP_error tprims_b200_network_workspace_size(tprims_b200_network net, size_t* bytes) {
+  return ffi([&] {
+    if (!bytes) null_arg("bytes out-parameter");
+    *bytes = network_of(net).arena_bytes;
+  });
+}
+
+extern "C" size_t tprims_b200_network_report(tprims_b200_network net, char* buf, size_t maxlen) {
+  std::string s;
+  if (ffi([&] { s = network_of(net).report(); }) != TPRIMS_OK) return 0;
+  if (buf && maxlen > 0) {
+    const size_t n = s.size() < maxlen - 1 ? s.size() : maxlen - 1;
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return s.size();
+}
+
+extern "C" TAPP_error tprims_b200_networks_execute(TAPP_executor exec, int n, const tprims_b200_network* nets,
+                                                   const void* const* alphas, const void* const* const* inputs,
+                                                   const void* const* betas, void* const* outs,
+                                                   void* const* workspaces) {
+  return ffi([&] {
+    if (n < 0) throw Error(ERR_SHAPE, "negative network count");
+    if (n == 0) return;
+    if (!nets || !alphas || !inputs || !betas || !outs) null_arg("network arrays");
+    std::vector<Network*> ns;
+    std::vector<Scalar> al, be;
+    for (int i = 0; i < n; ++i) {
+      Network& net = network_of(nets[i]);
+      if (!alphas[i]) null_arg("alpha");
+      if (!betas[i]) null_arg("beta");
+      if (!inputs[i]) null_arg("input pointers");
+      if (!outs[i]) null_arg("output");
+      for (size_t j = 0; j < net.inputs.size(); ++j)
+        if (!inputs[i][j]) null_arg("input " + std::to_string(j));
+      ns.push_back(&net);
+      al.push_back(read_scalar(net.dtype, alphas[i]));
+      be.push_back(read_scalar(net.dtype, betas[i]));
+    }
+    Executor& ex = resolve_exec(exec)->get();
+    execute_networks(ex, n, ns.data(), al.data(), be.data(), inputs, outs, workspaces);
+  });
+}
+
+extern "C" TAPP_error tprims_b200_network_execute(tprims_b200_network net, TAPP_executor exec, const void* alpha,
+                                                  const void* const* inputs, const void* beta, void* out,
+                                                  void* workspace) {
+  void* ws[1] = {workspace};
+  const void* const* ins[1] = {inputs};
+  const void* al[1] = {alpha};
+  const void* be[1] = {beta};
+  void* outs[1] = {out};
+  return tprims_b200_networks_execute(exec, 1, &net, al, ins, be, outs, ws);
 }
 
 extern "C" TAPP_error tprims_b200_product_vjp(TAPP_tensor_product plan, TAPP_executor exec, const void* alpha,

@@ -1,6 +1,8 @@
 // Executors, device state of products, operand staging and kernel dispatch.
 #include "runtime.hpp"
 
+#include "network.hpp"
+
 #include <algorithm>
 #include <climits>
 #include <atomic>
@@ -1065,10 +1067,14 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
 
 }  // namespace
 
-void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
+namespace {
+
+// The body of execute_items under the caller's lock and device guard: the
+// grouped graph and the individual items are enqueued; returns whether a
+// host operand was staged (the caller must then drain before reusing the
+// workspace).
+bool enqueue_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
                    const Item* items) {
-  std::lock_guard<std::mutex> lk(ex.mu);
-  DeviceGuard g(ex.device);
   const uint64_t key = ex.grouping ? list_key(n, plans, alpha, beta, items) : 0;
   auto hit = ex.grouping ? ex.graphs.find(key) : ex.graphs.end();
   Executor::Graph* gr = nullptr;
@@ -1102,7 +1108,78 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
     // A staged item's workspace is reused by the next item: drain between.
     if (staged && j + 1 < single.size()) finish(ex);
   }
+  return staged;
+}
+
+}  // namespace
+
+void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
+                   const Item* items) {
+  std::lock_guard<std::mutex> lk(ex.mu);
+  DeviceGuard g(ex.device);
+  const bool staged = enqueue_items(ex, n, plans, alpha, beta, items);
   if (ex.sync || staged) finish(ex);
+}
+
+void execute_networks(Executor& ex, int n, Network* const* nets, const Scalar* alpha, const Scalar* beta,
+                      const void* const* const* inputs, void* const* outs, void* const* workspaces) {
+  std::lock_guard<std::mutex> lk(ex.mu);
+  DeviceGuard g(ex.device);
+  // Arenas of the intermediates: the caller's workspace or the network's own.
+  std::vector<char*> base(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    Network& net = *nets[i];
+    if (net.arena_bytes == 0) continue;
+    if (workspaces && workspaces[i]) {
+      if (classify(workspaces[i], ex.device) != Where::Device)
+        throw Error(ERR_DEVICE, "network workspace " + std::to_string(i) + " is not device memory of the executor");
+      base[i] = static_cast<char*>(workspaces[i]);
+      continue;
+    }
+    std::lock_guard<std::mutex> nl(net.mu);
+    void*& a = net.arena[ex.device];
+    if (!a) check_cuda(cudaMalloc(&a, net.arena_bytes), "cudaMalloc(network arena)");
+    base[i] = static_cast<char*>(a);
+  }
+  // Every step's operands, validated before anything runs (all-or-nothing).
+  size_t max_steps = 0;
+  for (int i = 0; i < n; ++i) max_steps = std::max(max_steps, nets[i]->steps.size());
+  std::vector<std::vector<Item>> step_items(max_steps);
+  for (int i = 0; i < n; ++i) {
+    const Network& net = *nets[i];
+    const int nin = (int)net.inputs.size();
+    auto origin = [&](int id) -> const void* {
+      if (id < nin) return inputs[i][id];
+      return base[i] + net.steps[id - nin].offset;
+    };
+    for (size_t s = 0; s < net.steps.size(); ++s) {
+      const NetworkStep& st = net.steps[s];
+      void* d = st.last ? outs[i] : static_cast<void*>(base[i] + st.offset);
+      const bool c_read = st.last && !beta[i].is_zero();
+      const Item it{origin(st.a), origin(st.b), c_read ? d : nullptr, d};
+      validate_item(*st.plan, it, !c_read);
+      step_items[s].push_back(it);
+    }
+  }
+  const Scalar one{1.0, 0.0}, zero{};
+  for (size_t s = 0; s < max_steps; ++s) {
+    std::vector<Product*> plans;
+    std::vector<Scalar> al, be;
+    size_t k = 0;
+    for (int i = 0; i < n; ++i) {
+      if (s >= nets[i]->steps.size()) continue;
+      const NetworkStep& st = nets[i]->steps[s];
+      plans.push_back(st.plan.get());
+      al.push_back(st.last ? alpha[i] : one);
+      be.push_back(st.last ? beta[i] : zero);
+      ++k;
+    }
+    if (k == 0) continue;
+    // Stream order keeps step s + 1 behind step s; a staged host operand's
+    // workspace is reused by the next step, so that case drains first.
+    if (enqueue_items(ex, (int)k, plans.data(), al.data(), be.data(), step_items[s].data())) finish(ex);
+  }
+  if (ex.sync) finish(ex);
 }
 
 namespace {

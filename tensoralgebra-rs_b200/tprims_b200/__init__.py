@@ -71,7 +71,9 @@ ABI_SYMBOLS = [
     "tprims_b200_executor_selftest_wait", "tprims_b200_executor_probe_peak",
     "tprims_b200_execute_product_noalloc", "tprims_b200_product_set_split_k", "tprims_b200_product_set_autotune",
     "tprims_b200_executor_save_tuning", "tprims_b200_executor_load_tuning", "tprims_b200_executor_clear_tuning",
-    "tprims_b200_executor_tuning",
+    "tprims_b200_executor_tuning", "tprims_b200_network_create", "tprims_b200_network_destroy",
+    "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
+    "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -139,6 +141,19 @@ lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_clear_tuning.argtypes = [_ip]
 lib.tprims_b200_executor_tuning.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_executor_tuning.restype = C.c_size_t
+_i64pp = C.POINTER(_i64p)
+lib.tprims_b200_network_create.argtypes = [C.POINTER(_ip), C.c_int, C.c_int, C.POINTER(C.c_int), _i64pp, _i64pp,
+                                           _i64pp, C.POINTER(C.c_int), C.c_int, _i64p, _i64p, _i64p, C.c_int,
+                                           C.POINTER(C.c_int)]
+lib.tprims_b200_network_destroy.argtypes = [_ip]
+lib.tprims_b200_network_set_precision.argtypes = [_ip, C.c_int, C.c_int]
+lib.tprims_b200_network_set_autotune.argtypes = [_ip, C.c_int]
+lib.tprims_b200_network_workspace_size.argtypes = [_ip, C.POINTER(C.c_size_t)]
+lib.tprims_b200_network_report.argtypes = [_ip, C.c_char_p, C.c_size_t]
+lib.tprims_b200_network_report.restype = C.c_size_t
+lib.tprims_b200_network_execute.argtypes = [_ip, _ip, _vp, C.POINTER(_vp), _vp, _vp, _vp]
+lib.tprims_b200_networks_execute.argtypes = [_ip, C.c_int, C.POINTER(_ip), C.POINTER(_vp), C.POINTER(C.POINTER(_vp)),
+                                             C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]
 lib.tprims_b200_product_report.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_product_report.restype = C.c_size_t
 lib.tprims_b200_product_from_dot_general.argtypes = [
@@ -626,6 +641,119 @@ class PreparedBatch:
 
     def run(self, exec_: Optional[Executor] = None):
         check(lib.tprims_b200_contract_batched(exec_.h if exec_ else 0, self.n, self.arr))
+
+
+class Network:
+    """An N-ary contraction network executed as binary steps on the GPU (the
+    einsum layer the reference leaves to its callers).
+
+    ``inputs``: (OperandSpec, labels) per input tensor; ``output``:
+    (LayoutSpec, labels); ``path``: pairs of positions in the current operand
+    list (opt_einsum convention), or None for the greedy path."""
+
+    def __init__(self, dtype: int, inputs, output, path=None):
+        self.dtype = dtype
+        n = len(inputs)
+        # The C call reads one label per mode; a mismatch is refused here,
+        # before any array is read past its end.
+        for i, (sp, labels) in enumerate(list(inputs) + [(OperandSpec(output[0]), output[1])]):
+            if len(labels) != len(sp.layout.dims) or len(sp.layout.strides) != len(sp.layout.dims):
+                what = "output" if i == n else f"input {i}"
+                raise TprimsError(ERR_LABELS, f"{what}: {len(labels)} labels for {len(sp.layout.dims)} modes")
+        nm = (C.c_int * max(n, 1))(*[len(sp.layout.dims) for sp, _ in inputs])
+        self._arrs = []
+
+        def arr(v):
+            a = _arr(v)
+            self._arrs.append(a)
+            return C.cast(a, _i64p)
+
+        ext = (_i64p * max(n, 1))(*[arr(sp.layout.dims) for sp, _ in inputs])
+        st = (_i64p * max(n, 1))(*[arr(sp.layout.strides) for sp, _ in inputs])
+        lab = (_i64p * max(n, 1))(*[arr(l) for _, l in inputs])
+        ops = (C.c_int * max(n, 1))(*[CONJUGATE if sp.conj else IDENTITY for sp, _ in inputs])
+        olay, olab = output
+        pth = [x for pair in (path or []) for x in pair]
+        parr = (C.c_int * max(len(pth), 1))(*pth)
+        h = _ip(0)
+        check(lib.tprims_b200_network_create(C.byref(h), int(dtype), n, nm, ext, st, lab, ops, len(olay.dims),
+                                             arr(olay.dims), arr(olay.strides), arr(olab), len(pth) // 2, parr))
+        self.h = h.value
+        self.n_inputs = n
+
+    def set_precision(self, scheme: int, slices: int = 0):
+        check(lib.tprims_b200_network_set_precision(self.h, int(scheme), int(slices)))
+
+    def set_autotune(self, on: bool):
+        check(lib.tprims_b200_network_set_autotune(self.h, 1 if on else 0))
+
+    def workspace_size(self) -> int:
+        v = C.c_size_t(0)
+        check(lib.tprims_b200_network_workspace_size(self.h, C.byref(v)))
+        return v.value
+
+    def report(self) -> dict:
+        n = lib.tprims_b200_network_report(self.h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        lib.tprims_b200_network_report(self.h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
+    def execute(self, exec_: Optional[Executor], alpha, inputs, out, beta=0.0, workspace=None):
+        ins = (_vp * max(self.n_inputs, 1))(*[ptr_of(x) for x in inputs])
+        al, be = scalar_bytes(self.dtype, alpha), scalar_bytes(self.dtype, beta)
+        check(lib.tprims_b200_network_execute(self.h, exec_.h if exec_ else 0, C.cast(al, _vp), ins, C.cast(be, _vp),
+                                              ptr_of(out), ptr_of(workspace)))
+
+    def close(self):
+        if getattr(self, "h", 0):
+            check(lib.tprims_b200_network_destroy(self.h))
+            self.h = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PreparedNetworks:
+    """A list of networks and their operands frozen into the C argument arrays
+    once (the network counterpart of PreparedBatch): repeated runs pay no
+    per-network marshaling."""
+
+    def __init__(self, nets: Sequence[Network], inputs, outs, alphas=None, betas=None, workspaces=None):
+        n = len(nets)
+        alphas = alphas if alphas is not None else [1.0] * n
+        betas = betas if betas is not None else [0.0] * n
+        workspaces = workspaces if workspaces is not None else [None] * n
+        if not (len(inputs) == len(outs) == len(alphas) == len(betas) == len(workspaces) == n):
+            raise TprimsError(ERR_INVALID_ARGUMENT, "one inputs list, output, alpha, beta and workspace per network")
+        self.n = n
+        self._keep = [list(nets)]
+        self.hs = (_ip * max(n, 1))(*[x.h for x in nets])
+        self.al = (_vp * max(n, 1))()
+        self.be = (_vp * max(n, 1))()
+        self.ins = (C.POINTER(_vp) * max(n, 1))()
+        self.outs = (_vp * max(n, 1))(*[ptr_of(o) for o in outs])
+        self.ws = (_vp * max(n, 1))(*[ptr_of(w) for w in workspaces])
+        for i, net in enumerate(nets):
+            if len(inputs[i]) != net.n_inputs:
+                raise TprimsError(ERR_INVALID_ARGUMENT, f"network {i} takes {net.n_inputs} inputs")
+            a, b = scalar_bytes(net.dtype, alphas[i]), scalar_bytes(net.dtype, betas[i])
+            arr = (_vp * max(net.n_inputs, 1))(*[ptr_of(x) for x in inputs[i]])
+            self._keep += [a, b, arr]
+            self.al[i], self.be[i] = C.cast(a, _vp), C.cast(b, _vp)
+            self.ins[i] = C.cast(arr, C.POINTER(_vp))
+
+    def run(self, exec_: Optional[Executor] = None):
+        check(lib.tprims_b200_networks_execute(exec_.h if exec_ else 0, self.n, self.hs, self.al, self.ins, self.be,
+                                               self.outs, self.ws))
+
+
+def execute_networks(exec_: Optional[Executor], nets: Sequence[Network], inputs, outs, alphas=None, betas=None,
+                     workspaces=None):
+    """Run a list of networks: step s of every network in one grouped submission."""
+    PreparedNetworks(nets, inputs, outs, alphas, betas, workspaces).run(exec_)
 
 
 def contract_batched(items: Sequence[Item], exec_: Optional[Executor] = None):

@@ -1,0 +1,126 @@
+"""N-ary contraction networks without a GPU: path walking, the labels and
+extents of every intermediate, the arena layout, the greedy path and the
+refusals (TAPP status codes). Execution is covered by test_gpu_network.py."""
+import pytest
+
+F64, C64 = 1, 3
+
+
+def spec(tp, dims, conj=False):
+    return tp.OperandSpec(tp.LayoutSpec.col_major(dims), conj)
+
+
+def env_update(tp, a=20, b=24, s=4, p=2, dtype=C64, path=((0, 1), (2, 0), (1, 0))):
+    """The environment update of the list benchmark as one network:
+    E'[a',s',b'] = sum E[a,s,b] M[a,p,a'] W[s,p,s',q] conj(M[b,q,b'])."""
+    A, S, B, P, A2, S2, Q, B2 = range(8)
+    inputs = [(spec(tp, [a, s, b]), [A, S, B]), (spec(tp, [a, p, a]), [A, P, A2]),
+              (spec(tp, [s, p, s, p]), [S, P, S2, Q]), (spec(tp, [b, p, b], conj=True), [B, Q, B2])]
+    out = (tp.LayoutSpec.col_major([a, s, b]), [A2, S2, B2])
+    return tp.Network(dtype, inputs, out, path)
+
+
+def test_environment_update_steps_match_the_hand_built_lists(tp):
+    rep = env_update(tp).report()
+    st = rep["steps"]
+    assert [s["last"] for s in st] == [False, False, True]
+    # T1[s,b,p,a'], T2[b,a',s',q], then the output E'[a',s',b'].
+    assert st[0]["labels"] == [1, 2, 3, 4] and st[0]["dims"] == [4, 24, 2, 20]
+    assert st[1]["labels"] == [2, 4, 5, 6] and st[1]["dims"] == [24, 20, 4, 2]
+    assert st[2]["labels"] == [4, 5, 7]
+    assert (st[0]["a"], st[0]["b"]) == (0, 1) and (st[1]["a"], st[1]["b"]) == (4, 2) and (st[2]["a"], st[2]["b"]) == (5, 3)
+    # Dense intermediates in one arena, 256-byte aligned, complex128 elements.
+    t1 = 4 * 24 * 2 * 20 * 16
+    assert st[0]["offset"] == 0 and st[1]["offset"] == (t1 + 255) // 256 * 256
+    assert rep["arena_bytes"] == st[1]["offset"] + (24 * 20 * 4 * 2 * 16 + 255) // 256 * 256
+    # MACs: a s b p a' + b a' s p s' q + a' s' b q b'.
+    assert rep["macs"] == 20 * 4 * 24 * 2 * 20 + 24 * 20 * 4 * 2 * 4 * 2 + 20 * 4 * 24 * 2 * 24
+    # The conjugation of the last input reaches its step's plan.
+    assert st[2]["plan"]["dtype"] == "c64" and rep["greedy_path"] is False
+
+
+def test_greedy_path_is_complete_and_avoids_outer_products(tp):
+    net = env_update(tp, path=None)
+    rep = net.report()
+    assert rep["greedy_path"] is True and len(rep["path"]) == 3
+    for s in rep["steps"]:
+        assert set(s["labels_a"]) & set(s["labels_b"]), s  # every step contracts or batches a shared label
+    assert net.workspace_size() == rep["arena_bytes"]
+
+
+def test_reductions_and_batch_labels(tp):
+    # D[i] = sum_{j,k} X[i,j] Y[j,k] Z[i,k]: the last step batches i and contracts k.
+    I, J, K = 0, 1, 2
+    inputs = [(spec(tp, [5, 6]), [I, J]), (spec(tp, [6, 7]), [J, K]), (spec(tp, [5, 7]), [I, K])]
+    rep = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([5]), [I]), [(0, 1), (1, 0)]).report()
+    assert rep["steps"][0]["labels"] == [I, K]
+    assert rep["steps"][1]["plan"]["batch"] == 5 and rep["steps"][1]["plan"]["k"] == 7
+    # A label of one input needed nowhere else is summed in its first step.
+    inputs = [(spec(tp, [5, 6, 3]), [I, J, 9]), (spec(tp, [6, 7]), [J, K])]
+    rep = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([5, 7]), [I, K]), None).report()
+    assert rep["steps"][0]["plan"]["k"] == 18
+
+
+@pytest.mark.parametrize("case,status", [
+    ("extent", 2), ("broadcast", 15), ("short_path", 1), ("bad_position", 1), ("one_input", 15), ("labels", 14),
+])
+def test_refusals(tp, case, status):
+    I, J, K = 0, 1, 2
+    inputs = [(spec(tp, [5, 6]), [I, J]), (spec(tp, [6, 7]), [J, K])]
+    out = (tp.LayoutSpec.col_major([5, 7]), [I, K])
+    path = [(0, 1)]
+    if case == "extent":
+        inputs[1] = (spec(tp, [8, 7]), [J, K])
+    elif case == "broadcast":
+        out = (tp.LayoutSpec.col_major([5, 7, 2]), [I, K, 3])
+    elif case == "short_path":
+        path = [(0, 1), (0, 1)]
+    elif case == "bad_position":
+        path = [(0, 2)]
+    elif case == "one_input":
+        inputs = inputs[:1]
+        out = (tp.LayoutSpec.col_major([5]), [I])
+        path = None
+    elif case == "labels":
+        inputs[0] = (spec(tp, [5, 6]), [I])
+    with pytest.raises(tp.TprimsError) as ei:
+        tp.Network(F64, inputs, out, path)
+    assert ei.value.status == status
+
+
+def test_prepared_networks_marshal_every_pointer(tp, monkeypatch):
+    """The argument arrays handed to tprims_b200_networks_execute (the C call
+    is replaced by a recorder: nothing runs without a GPU)."""
+    import ctypes as C
+
+    import numpy as np
+
+    nets = [env_update(tp, a=10 + i, b=12, dtype=F64) for i in range(3)]
+    inputs = [[np.zeros(4, dtype=np.float64) for _ in range(4)] for _ in nets]
+    outs = [np.zeros(4, dtype=np.float64) for _ in nets]
+    wss = [None, np.zeros(8, dtype=np.uint8), None]
+    seen = {}
+
+    def recorder(exec_h, n, hs, al, ins, be, ou, ws):
+        seen["n"] = n
+        seen["hs"] = [hs[i] for i in range(n)]
+        seen["ins"] = [[ins[i][j] for j in range(4)] for i in range(n)]
+        seen["outs"] = [ou[i] for i in range(n)]
+        seen["ws"] = [ws[i] for i in range(n)]
+        seen["alpha"] = [C.cast(al[i], C.POINTER(C.c_double))[0] for i in range(n)]
+        seen["beta"] = [C.cast(be[i], C.POINTER(C.c_double))[0] for i in range(n)]
+        return 0
+
+    monkeypatch.setattr(tp.lib, "tprims_b200_networks_execute", recorder)
+    prep = tp.PreparedNetworks(nets, inputs, outs, alphas=[1.0, 0.5, -2.0], betas=[0.0, 1.0, 0.25], workspaces=wss)
+    prep.run(None)
+    prep.run(None)  # the arrays stay valid across runs
+    assert seen["n"] == 3 and seen["hs"] == [n.h for n in nets]
+    assert seen["ins"] == [[x.ctypes.data for x in row] for row in inputs]
+    assert seen["outs"] == [o.ctypes.data for o in outs]
+    assert seen["ws"] == [None, wss[1].ctypes.data, None]
+    assert seen["alpha"] == [1.0, 0.5, -2.0] and seen["beta"] == [0.0, 1.0, 0.25]
+    with pytest.raises(tp.TprimsError):
+        tp.PreparedNetworks(nets, inputs[:2], outs)
+    for n in nets:
+        n.close()

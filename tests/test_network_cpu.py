@@ -124,3 +124,68 @@ def test_prepared_networks_marshal_every_pointer(tp, monkeypatch):
         tp.PreparedNetworks(nets, inputs[:2], outs)
     for n in nets:
         n.close()
+
+
+def _chain_through_oracle(orc, rep, arrays, conj):
+    """Runs a network's reported steps with the CPU oracle's brute-force binary
+    contraction: every intermediate dense column-major with the step's labels
+    and extents, exactly as the GPU arena holds them."""
+    import numpy as np
+
+    n = len(arrays)
+    cm = lambda dims: [int(np.prod(dims[:i])) for i in range(len(dims))]
+    ops = {i: (np.ascontiguousarray(a.ravel(order="F")), list(a.shape), conj[i]) for i, a in enumerate(arrays)}
+    out = None
+    for s, st in enumerate(rep["steps"]):
+        (ba, ea, ca), (bb, eb, cb) = ops[st["a"]], ops[st["b"]]
+        dims = st["dims"]
+        buf = np.zeros(int(np.prod(dims)), dtype=arrays[0].dtype)
+        orc.label_contract(1.0, orc.View(ba, ea, cm(ea), st["labels_a"], conj=ca),
+                           orc.View(bb, eb, cm(eb), st["labels_b"], conj=cb), 0.0, None,
+                           orc.View(buf, dims, cm(dims), st["labels"]))
+        ops[n + s] = (buf, dims, False)
+        out = buf.reshape(dims, order="F")
+    return out
+
+
+@pytest.mark.parametrize("greedy", [False, True])
+def test_network_steps_compose_to_the_whole_contraction(tp, orc, greedy):
+    """The planner's step labels, extents and intermediate layouts, chained
+    through the oracle, give the full network contraction (numpy einsum)."""
+    import numpy as np
+
+    g = np.random.default_rng(5)
+    a, b, s, p = 5, 4, 3, 2
+    dims = [[a, s, b], [a, p, a], [s, p, s, p], [b, p, b]]
+    arrays = [g.uniform(-1, 1, d) + 1j * g.uniform(-1, 1, d) for d in dims]
+    net = env_update(tp, a=a, b=b, s=s, p=p, dtype=C64, path=None if greedy else ((0, 1), (2, 0), (1, 0)))
+    got = _chain_through_oracle(orc, net.report(), arrays, [False, False, False, True])
+    want = np.einsum("asb,apc,spdq,bqe->cde", arrays[0], arrays[1], arrays[2], np.conj(arrays[3]))
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    net.close()
+
+
+def test_five_tensor_network_with_batch_and_reduction(tp, orc):
+    """A ring of five tensors with a batch label kept to the output and a
+    label summed inside one input, on the greedy path."""
+    import numpy as np
+
+    g = np.random.default_rng(6)
+    ext = {0: 3, 1: 4, 2: 2, 3: 5, 4: 3, 5: 2, 6: 3}  # 6: batch (kept), 5: summed in input 0 only
+    labels = [[0, 1, 5, 6], [1, 2, 6], [2, 3], [3, 4, 6], [4, 0]]
+    arrays = [g.uniform(-1, 1, [ext[l] for l in ls]) for ls in labels]
+    inputs = [(spec(tp, [ext[l] for l in ls]), ls) for ls in labels]
+    net = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([ext[6]]), [6]), None)
+    rep = net.report()
+    assert rep["greedy_path"] and len(rep["steps"]) == 4
+    got = _chain_through_oracle(orc, rep, arrays, [False] * 5)
+    want = np.einsum("abfg,bcg,cd,deg,ea->g", *arrays)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    net.close()
+
+
+def test_greedy_path_orders_a_matrix_chain_by_cost(tp):
+    # A(10x100) B(100x5) C(5x50): (AB) first costs 5000 MACs, (BC) first 25000.
+    inputs = [(spec(tp, [10, 100]), [0, 1]), (spec(tp, [100, 5]), [1, 2]), (spec(tp, [5, 50]), [2, 3])]
+    rep = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([10, 50]), [0, 3]), None).report()
+    assert rep["path"][0] == [0, 1] and rep["macs"] == 10 * 100 * 5 + 10 * 5 * 50

@@ -240,6 +240,13 @@ std::string Product::report() const {
     << ((scheme == Scheme::Bf16x3 || scheme == Scheme::Bf16x6)
             ? dev::split_tail_parts(dev::split_layout((int)scheme, view.M, view.N, view.K, view.H), 148)
             : 1)
+    << ",\"autotune_candidates\":[";
+  if (scheme == Scheme::Plain) {
+    const auto cands = plain_candidates((int)problem.dtype, view.M, view.N, view.K, view.H, 148);
+    for (size_t i = 0; i < cands.size(); ++i)
+      o << (i ? "," : "") << "\"" << choice_name(cands[i], (int)problem.dtype) << "\"";
+  }
+  o << "]"
     << ",\"choice\":\"" << (scheme == Scheme::Plain ? src_names[(int)src] : "fixed")
     << "\",\"autotune\":" << (autotune ? "true" : "false") << ",\"signature\":\"" << signature << "\""
     << ",\"stated_rel_error\":" << stated_bound(problem.dtype, scheme)

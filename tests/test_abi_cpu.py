@@ -335,3 +335,19 @@ def test_split_k_and_autotune_switches(tp):
                                           tp.OperandSpec(tp.LayoutSpec([8, 8], [1, 8])), [0, 2], [2, 1], [0, 1]),
                    tp.PlanConfig(autotune=True, split_k=1))
     assert plan.report()["autotune"] is True and plan.report()["choice"] == "pinned"
+
+
+def test_autotune_candidates(tp):
+    """What the autotuner times (for 148 SMs): the model's choice first, every
+    tile family of the dtype, split-K only while tiles x splits <= 4 x SMs and
+    the chunks stay at least 128 deep."""
+    c1 = _gemm_product(tp, 576, 576, 576).report()["autotune_candidates"]
+    assert c1[0] == _gemm_product(tp, 576, 576, 576).report()["family"]
+    assert {"sm100.f64.dmma884.64x64x16", "sm100.f64.dmma884.32x32x16", "sm100.f64.dmma884.128x32x16"} <= set(c1)
+    assert any("+splitk" in c for c in c1) and len(c1) == len(set(c1))
+    big = _gemm_product(tp, 4096, 4096, 4096, dt=0).report()["autotune_candidates"]
+    assert sorted(big) == ["sm100.f32.simt.128x128x16", "sm100.f32.simt.64x64x16"]  # enough tiles: no split
+    shallow = _gemm_product(tp, 64, 64, 128).report()["autotune_candidates"]
+    assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
+    c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]
+    assert c32[0].startswith("sm100.c32.simt.ring")

@@ -10,7 +10,7 @@
 // ring of four shared-memory stages with cp.async (AsyncGather), which keeps
 // three stages of global loads in flight. The register tile replaces
 // the microkernels (kernels/reference/scalar.rs:31-175): FP32 FFMA for f32,
-// FP64 DMMA (mma.sync m8n8k4) for f64, and four real products per complex MAC
+// FP64 DMMA (mma.sync m16n8k8) for f64, and four real products per complex MAC
 // for c32/c64 (the planar method, writeback.rs:54-97 Planar). The epilogue is
 // the scatter write-back (writeback.rs:311-486) applied once per element after
 // the full K loop.

@@ -6,7 +6,7 @@
  *
  * Part 1 repeats the standard TAPP declarations (numeric values and prototypes
  * are ABI and are kept identical to the pinned upstream headers the reference
- * ships in crates/tprims-capi/include/tapp/*.h). When the upstream <tapp.h> has
+ * ships in the headers of crates/tprims-capi/include/tapp/). When the upstream <tapp.h> has
  * already been included, part 1 is skipped and its declarations are used.
  *
  * Part 2 repeats the tprims extensions of crates/tprims-capi/include/tprims/

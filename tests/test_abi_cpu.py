@@ -351,3 +351,23 @@ def test_autotune_candidates(tp):
     assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
     c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]
     assert c32[0].startswith("sm100.c32.simt.ring")
+
+
+def test_plain_c_consumer_compiles_links_and_runs(tmp_path):
+    """tests/c/abi_consumer.c: the header as strict C99 (-Wall -Wextra -Werror
+    -pedantic), linked against the built library, run without a GPU (handles,
+    infos, products, report, refusals, network planning)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    libdir = os.path.join(REPO, "tensoralgebra-rs_b200", "tprims_b200")
+    exe = str(tmp_path / "abi_consumer")
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "c", "abi_consumer.c"), "-L", libdir, "-ltprims_b200",
+                    "-Wl,-rpath," + libdir, "-o", exe], check=True, capture_output=True, text=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "ok"

@@ -224,6 +224,12 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_save_tuning(TAPP_executor exe
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_load_tuning(TAPP_executor exec, const char* path);
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_clear_tuning(TAPP_executor exec);
 TPRIMS_B200_EXPORT size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, size_t maxlen);
+/* Number of device allocations the library has made in this process (every
+   cudaMalloc of executors, workspaces, scatter vectors, grouped-list
+   descriptors and network arenas). Diagnostics: once a call has run, repeating
+   it leaves the count unchanged (the counterpart of the reference's allocation
+   counter tests, tprims-contract tests packed_workspace_alloc.rs). */
+TPRIMS_B200_EXPORT uint64_t tprims_b200_device_allocations(void);
 /* Per-kernel timing (diagnostics, off by default): with `on` != 0 the executor
    records CUDA events on its stream around every kernel launch. The totals
    are resolved whenever the stream is drained. */

@@ -905,6 +905,8 @@ extern "C" size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, siz
   return s.size();
 }
 
+extern "C" uint64_t tprims_b200_device_allocations(void) { return device_allocations(); }
+
 extern "C" TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on) {
   return ffi([&] {
     Executor& ex = resolve_exec(exec)->get();

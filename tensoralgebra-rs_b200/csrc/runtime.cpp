@@ -25,6 +25,18 @@ void check_cuda(cudaError_t e, const char* what) {
 }
 
 namespace {
+std::atomic<uint64_t> g_device_allocations{0};
+}  // namespace
+
+cudaError_t device_alloc(void** p, size_t bytes) {
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) g_device_allocations.fetch_add(1, std::memory_order_relaxed);
+  return e;
+}
+
+uint64_t device_allocations() { return g_device_allocations.load(std::memory_order_relaxed); }
+
+namespace {
 
 // Makes `device` current for the scope and restores the caller's device.
 struct DeviceGuard {
@@ -60,7 +72,7 @@ Executor* Executor::create(int device, uintptr_t stream) {
   } else {
     ex->stream = reinterpret_cast<cudaStream_t>(stream);
   }
-  check_cuda(cudaMalloc(&ex->status, 256), "cudaMalloc(status)");
+  check_cuda(device_alloc(reinterpret_cast<void**>(&ex->status), 256), "cudaMalloc(status)");
   check_cuda(cudaMemsetAsync(ex->status, 0, 256, ex->stream), "cudaMemset(status)");
   check_cuda(cudaStreamSynchronize(ex->stream), "cudaStreamSynchronize");
   check_cuda(cudaDeviceGetAttribute(&ex->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
@@ -97,7 +109,7 @@ void* Executor::workspace(size_t bytes) {
   ws = nullptr;
   ws_bytes = 0;
   const size_t want = std::max(bytes, ws_bytes + ws_bytes / 2);
-  check_cuda(cudaMalloc(&ws, want), "cudaMalloc(workspace)");
+  check_cuda(device_alloc(&ws, want), "cudaMalloc(workspace)");
   ws_bytes = want;
   return ws;
 }
@@ -150,7 +162,7 @@ const dev::Scatters& Product::scatters(int device, cudaStream_t stream) {
     while (host.size() % 4) host.push_back(0);
   }
   DeviceScatters ds;
-  check_cuda(cudaMalloc(&ds.buf, host.size() * sizeof(int64_t)), "cudaMalloc(scatters)");
+  check_cuda(device_alloc(reinterpret_cast<void**>(&ds.buf), host.size() * sizeof(int64_t)), "cudaMalloc(scatters)");
   // A plain cudaMemcpy from pageable memory may return before its DMA lands,
   // and it is ordered on the legacy stream, which a non-blocking stream does
   // not wait for: copy on the caller's stream and wait for it, so that the
@@ -916,7 +928,7 @@ GroupSet build_group_set(Executor& ex, const std::vector<int>& idx, int policy, 
   }
   const size_t items_bytes = host_items.size() * sizeof(dev::GroupItem);
   const size_t starts_bytes = host_starts.size() * sizeof(int64_t);
-  check_cuda(cudaMalloc(&gs.buf, align_up(items_bytes, 256) + align_up(starts_bytes, 256) + 256 * (gs.family.size() + 1)),
+  check_cuda(device_alloc(&gs.buf, align_up(items_bytes, 256) + align_up(starts_bytes, 256) + 256 * (gs.family.size() + 1)),
              "cudaMalloc(groups)");
   char* base = static_cast<char*>(gs.buf);
   // Stream-ordered copies, complete before any capture (see Product::scatters).
@@ -1145,7 +1157,7 @@ void execute_networks(Executor& ex, int n, Network* const* nets, const Scalar* a
     }
     std::lock_guard<std::mutex> nl(net.mu);
     void*& a = net.arena[ex.device];
-    if (!a) check_cuda(cudaMalloc(&a, net.arena_bytes), "cudaMalloc(network arena)");
+    if (!a) check_cuda(device_alloc(&a, net.arena_bytes), "cudaMalloc(network arena)");
     base[i] = static_cast<char*>(a);
   }
   // Every step's operands, validated before anything runs (all-or-nothing).

@@ -193,6 +193,12 @@ std::string kernel_times_json(Executor& ex, bool reset);
 
 void check_cuda(cudaError_t e, const char* what);
 
+// Every device allocation of the library goes through device_alloc, which
+// counts it; device_allocations() is the process-wide count (diagnostics: a
+// steady-state execution must leave it unchanged).
+cudaError_t device_alloc(void** p, size_t bytes);
+uint64_t device_allocations();
+
 // ---- autotuner (autotune.cpp) ----
 
 // A product's Problem signature: dtype, folded axes (extent and the strides

@@ -74,6 +74,7 @@ ABI_SYMBOLS = [
     "tprims_b200_executor_tuning", "tprims_b200_network_create", "tprims_b200_network_destroy",
     "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
     "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
+    "tprims_b200_device_allocations",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -141,6 +142,8 @@ lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_clear_tuning.argtypes = [_ip]
 lib.tprims_b200_executor_tuning.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_executor_tuning.restype = C.c_size_t
+lib.tprims_b200_device_allocations.argtypes = []
+lib.tprims_b200_device_allocations.restype = C.c_uint64
 _i64pp = C.POINTER(_i64p)
 lib.tprims_b200_network_create.argtypes = [C.POINTER(_ip), C.c_int, C.c_int, C.POINTER(C.c_int), _i64pp, _i64pp,
                                            _i64pp, C.POINTER(C.c_int), C.c_int, _i64p, _i64p, _i64p, C.c_int,
@@ -714,6 +717,11 @@ class Network:
             self.close()
         except Exception:
             pass
+
+
+def device_allocations() -> int:
+    """Device allocations the library has made in this process (diagnostics)."""
+    return int(lib.tprims_b200_device_allocations())
 
 
 class PreparedNetworks:

@@ -208,6 +208,11 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_grouping(TAPP_executor ex
    on a flag nothing sets and gives up after `limit_ns`; the executor reports
    the recorded timeout as TPRIMS_ERR_INTERNAL and stays usable. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_workspace_limit(TAPP_executor exec, size_t bytes);
+/* Launch-failure injection (simulated stream errors, on the host): the
+   contraction launch `after` launches from now (0 = the next) is refused with
+   TPRIMS_ERR_INTERNAL before anything of it reaches the GPU; its output is
+   left as it was and later calls run normally. -1 switches the hook off. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_inject_launch_failure(TAPP_executor exec, int after);
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor exec, uint64_t limit_ns);
 /* Measured pipe peak for roofline denominators (diagnostics): which = 0 runs
    the FP64 DMMA pipe (mma.sync m8n8k4), 1 the FP32 FFMA pipe, with

@@ -907,6 +907,15 @@ extern "C" size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, siz
 
 extern "C" uint64_t tprims_b200_device_allocations(void) { return device_allocations(); }
 
+extern "C" TAPP_error tprims_b200_executor_inject_launch_failure(TAPP_executor exec, int after) {
+  return ffi([&] {
+    if (after < -1) throw Error(ERR_INVALID_ARGUMENT, "launch count must be -1 (off) or >= 0");
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    ex.fail_launch_after = after;
+  });
+}
+
 extern "C" TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on) {
   return ffi([&] {
     Executor& ex = resolve_exec(exec)->get();

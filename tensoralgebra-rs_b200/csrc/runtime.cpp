@@ -426,8 +426,16 @@ void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const Plain
   check_cuda(dev::launch_plain_gemm(dt, c.kernel, g, ex.stream), "plain contraction launch");
 }
 
+// The fault-injection hook: counts launches down and refuses the chosen one.
+void injected_failure_check(Executor& ex) {
+  if (ex.fail_launch_after < 0) return;
+  if (ex.fail_launch_after-- == 0)
+    throw Error(ERR_INTERNAL, "injected launch failure (tprims_b200_executor_inject_launch_failure)");
+}
+
 void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool output_only, const PlainChoice& pc,
                         char* scratch, size_t scratch_bytes) {
+  injected_failure_check(ex);
   const int dt = (int)pr.problem.dtype;
   if (output_only) {
     Timed t(ex, "output_pass");
@@ -1117,6 +1125,7 @@ bool enqueue_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
   }
   bool staged = false;
   if (gr) {
+    injected_failure_check(ex);
     Timed t(ex, "grouped");
     gr->last_use = ++ex.graph_clock;
     check_cuda(cudaGraphLaunch(gr->exec, ex.stream), "cudaGraphLaunch");

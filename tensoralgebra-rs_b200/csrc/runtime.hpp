@@ -81,6 +81,9 @@ struct Executor {
   bool profile = false;
   bool grouping = true;
   size_t ws_limit = SIZE_MAX;  // cap of the workspace arena (allocation-failure injection)
+  // Launch-failure injection: the launch this many launches from now is
+  // refused on the host with an error, before it reaches the stream (-1: off).
+  int fail_launch_after = -1;
   int drain_limit_s = 300;     // bound of one wait for the stream to drain
   KernelTimes times;
   size_t pool_size = 0, budget = 1;  // recorded for the pooled-executor extension

@@ -74,7 +74,7 @@ ABI_SYMBOLS = [
     "tprims_b200_executor_tuning", "tprims_b200_network_create", "tprims_b200_network_destroy",
     "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
     "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
-    "tprims_b200_device_allocations",
+    "tprims_b200_device_allocations", "tprims_b200_executor_inject_launch_failure",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -142,6 +142,7 @@ lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_clear_tuning.argtypes = [_ip]
 lib.tprims_b200_executor_tuning.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_executor_tuning.restype = C.c_size_t
+lib.tprims_b200_executor_inject_launch_failure.argtypes = [_ip, C.c_int]
 lib.tprims_b200_device_allocations.argtypes = []
 lib.tprims_b200_device_allocations.restype = C.c_uint64
 _i64pp = C.POINTER(_i64p)
@@ -333,6 +334,10 @@ class Executor:
     def set_workspace_limit(self, nbytes: int):
         """Cap the workspace arena (0 = no cap); larger requests are refused."""
         check(lib.tprims_b200_executor_set_workspace_limit(self.h, int(nbytes)))
+
+    def inject_launch_failure(self, after: int):
+        """Refuse the launch `after` launches from now (host-side fault injection; -1: off)."""
+        check(lib.tprims_b200_executor_inject_launch_failure(self.h, int(after)))
 
     def selftest_wait(self, limit_ns: int) -> int:
         """Run the bounded-wait self-test kernel; returns the status it produced."""

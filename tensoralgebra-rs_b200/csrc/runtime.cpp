@@ -218,6 +218,10 @@ double stated_bound(DType t, Scheme s) {
 
 }  // namespace
 
+namespace {
+size_t scheme_scratch(const Product& pr, const PlainChoice& pc, int num_sms);
+}  // namespace
+
 std::string Product::report() const {
   std::ostringstream o;
   const auto& st = packed.stats;
@@ -252,7 +256,16 @@ std::string Product::report() const {
     << ((scheme == Scheme::Bf16x3 || scheme == Scheme::Bf16x6)
             ? dev::split_tail_parts(dev::split_layout((int)scheme, view.M, view.N, view.K, view.H), 148)
             : 1)
-    << ",\"autotune_candidates\":[";
+    << ",\"scratch_bytes\":" << scheme_scratch(*this, pc, 148);
+  if (scheme == Scheme::Plain && !tiny) {
+    // The CTA tile and the CTAs of the main launch (before the 1-D grid's
+    // wrap-around) for 148 SMs.
+    int bm = 0, bn = 0;
+    dev::plain_tile_shape(kernel, &bm, &bn);
+    const int64_t tiles = bm > 0 ? ((view.M + bm - 1) / bm) * ((view.N + bn - 1) / bn) * view.H : 0;
+    o << ",\"tile\":[" << bm << "," << bn << "],\"ctas\":" << tiles * splits;
+  }
+  o << ",\"autotune_candidates\":[";
   if (scheme == Scheme::Plain) {
     const auto cands = plain_candidates((int)problem.dtype, view.M, view.N, view.K, view.H, 148);
     for (size_t i = 0; i < cands.size(); ++i)

@@ -371,3 +371,14 @@ def test_plain_c_consumer_compiles_links_and_runs(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == "ok"
+
+
+def test_report_tile_ctas_and_scratch(tp):
+    """The report's launch geometry for 148 SMs: CTA tile, CTAs of the main
+    launch (tiles x K chunks) and the workspace the scheme needs."""
+    r = _gemm_product(tp, 576, 576, 576).report()
+    bm, bn = r["tile"]
+    assert r["ctas"] == -(-576 // bm) * -(-576 // bn) and r["scratch_bytes"] == 0
+    deep = _gemm_product(tp, 512, 512, 32768).report()
+    assert deep["split_k"] > 1 and deep["ctas"] == 64 * deep["split_k"]
+    assert deep["scratch_bytes"] >= deep["split_k"] * 512 * 512 * 8  # the split-K partials

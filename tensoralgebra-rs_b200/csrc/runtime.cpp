@@ -3,6 +3,8 @@
 
 #include "network.hpp"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <climits>
 #include <atomic>
@@ -37,6 +39,15 @@ cudaError_t device_alloc(void** p, size_t bytes) {
 uint64_t device_allocations() { return g_device_allocations.load(std::memory_order_relaxed); }
 
 namespace {
+
+// An NVTX range for the scope (a no-op unless a profiler is attached), so the
+// library's calls show up by name on an Nsight or ncu --nvtx timeline.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Makes `device` current for the scope and restores the caller's device.
 struct DeviceGuard {
@@ -683,6 +694,7 @@ int tune_reps(double first_ms) { return first_ms < 0.05 ? 10 : first_ms < 1.0 ? 
 // the original D.
 TuneEntry autotune_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, char* scratch, size_t scratch_bytes,
                          char* d_span, char* snapshot, size_t span_bytes) {
+  NvtxRange range("tprims.autotune");
   ProfileOff off(ex);
   const auto restore = [&] {
     if (snapshot)
@@ -852,6 +864,7 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
 }  // namespace
 
 void execute_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
+  NvtxRange range("tprims.execute_product");
   std::lock_guard<std::mutex> lk(ex.mu);
   DeviceGuard g(ex.device);
   const bool staged = enqueue_item(pr, ex, alpha, beta, it);
@@ -1156,6 +1169,7 @@ bool enqueue_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
 
 void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
                    const Item* items) {
+  NvtxRange range("tprims.contract_batched");
   std::lock_guard<std::mutex> lk(ex.mu);
   DeviceGuard g(ex.device);
   const bool staged = enqueue_items(ex, n, plans, alpha, beta, items);
@@ -1164,6 +1178,7 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
 
 void execute_networks(Executor& ex, int n, Network* const* nets, const Scalar* alpha, const Scalar* beta,
                       const void* const* const* inputs, void* const* outs, void* const* workspaces) {
+  NvtxRange range("tprims.execute_networks");
   std::lock_guard<std::mutex> lk(ex.mu);
   DeviceGuard g(ex.device);
   // Arenas of the intermediates: the caller's workspace or the network's own.
@@ -1282,6 +1297,7 @@ void zero_layout(Executor& ex, DType dt, const Operand& op, void* origin) {
 // diagonal (the rest of dA is zeroed first).
 void execute_vjp(Product& p, Executor& ex, Scalar alpha, const void* A, const void* B, const void* dD, void* dA,
                  void* dB) {
+  NvtxRange range("tprims.vjp");
   const Problem& pb = p.problem;
   const bool ca = pb.a.conj, cb = pb.b.conj, cd = pb.d.conj;
   const bool cplx = dtype_complex(pb.dtype);

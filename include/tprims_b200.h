@@ -263,6 +263,13 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_prod
    5 c32 64x64, 6 c64 64x32, 7 c64 32x32, 8 f64 128x32, 9 c64 128x32. A family
    of another dtype is refused at execution (TPRIMS_ERR_INTERNAL). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);
+/* Plan::check_raw (crates/tprims-contract/src/plan/mod.rs:384): the aliasing
+   preflight of a call from its origins alone (nothing is dereferenced; a NULL
+   origin is absent): TPRIMS_ERR_ALIASED when D's reachable address range
+   overlaps A's or B's, or a separate C's without being the same mapping at the
+   same origin; TPRIMS_OK otherwise. Every execute entry runs it first. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_check_raw(TAPP_tensor_product plan, const void* A, const void* B,
+                                                            const void* C, const void* D);
 /* Pin the split-K factor of the plain path: 0 = chosen (model or autotuner),
    1 = never split K, 2..64 = cut K into that many chunks of whole 64-deep
    blocks (fewer when K is short). Split partials are summed in a fixed order.

@@ -514,6 +514,11 @@ extern "C" TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int
   });
 }
 
+extern "C" TAPP_error tprims_b200_product_check_raw(TAPP_tensor_product plan, const void* A, const void* B,
+                                                    const void* C, const void* D) {
+  return ffi([&] { check_raw(product_of(plan), Item{A, B, C, const_cast<void*>(D)}); });
+}
+
 extern "C" TAPP_error tprims_b200_product_set_split_k(TAPP_tensor_product plan, int splits) {
   return ffi([&] {
     Product& p = product_of(plan);

@@ -326,20 +326,24 @@ bool overlaps(const Problem& p, int s1, const void* o1, int s2, const void* o2) 
 
 }  // namespace
 
-void validate_item(const Product& pr, const Item& it, bool beta_zero) {
-  if (!it.a || !it.b || !it.d) throw Error(ERR_INVALID_ARGUMENT, "A, B or D data pointer is null or zero");
-  if (!it.c && !beta_zero)
-    throw Error(ERR_UNSUPPORTED,
-                "a null C (TAPP_IN_PLACE) with a nonzero beta is ambiguous in TAPP and not supported; pass D as C to "
-                "accumulate in place");
+void check_raw(const Product& pr, const Item& it) {
   const Problem& p = pr.problem;
-  if (p.out_empty) return;
+  if (p.out_empty || !it.d) return;
   if (overlaps(p, SD, it.d, SA, it.a)) throw Error(ERR_ALIASED, "D overlaps A");
   if (overlaps(p, SD, it.d, SB, it.b)) throw Error(ERR_ALIASED, "D overlaps B");
   if (p.cmode == CMode::Separate && it.c) {
     const bool same = it.c == it.d && p.c_matches_d;
     if (!same && overlaps(p, SD, it.d, SC, it.c)) throw Error(ERR_ALIASED, "C and D overlap without being the same mapping");
   }
+}
+
+void validate_item(const Product& pr, const Item& it, bool beta_zero) {
+  if (!it.a || !it.b || !it.d) throw Error(ERR_INVALID_ARGUMENT, "A, B or D data pointer is null or zero");
+  if (!it.c && !beta_zero)
+    throw Error(ERR_UNSUPPORTED,
+                "a null C (TAPP_IN_PLACE) with a nonzero beta is ambiguous in TAPP and not supported; pass D as C to "
+                "accumulate in place");
+  check_raw(pr, it);
 }
 
 namespace {

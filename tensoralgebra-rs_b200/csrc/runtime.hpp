@@ -167,8 +167,12 @@ struct Scalar {
 };
 Scalar read_scalar(DType t, const void* p);
 
-// The semantic preflight (Plan::check_raw, plan/mod.rs:384-428) plus the C-ABI
-// null rules (execute.rs:34-39).
+// Plan::check_raw (plan/mod.rs:384-428): the aliasing preflight from the
+// origins alone, nothing dereferenced, a null origin treated as absent: D
+// overlapping A or B, a separate C overlapping D without being the same mapping
+// at the same origin. Throws ERR_ALIASED.
+void check_raw(const Product& p, const Item& it);
+// check_raw plus the C-ABI null rules (execute.rs:34-39).
 void validate_item(const Product& p, const Item& it, bool beta_zero);
 
 // Run one validated item on the executor (stage host operands, launch,

@@ -74,7 +74,7 @@ ABI_SYMBOLS = [
     "tprims_b200_executor_tuning", "tprims_b200_network_create", "tprims_b200_network_destroy",
     "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
     "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
-    "tprims_b200_device_allocations", "tprims_b200_executor_inject_launch_failure",
+    "tprims_b200_device_allocations", "tprims_b200_executor_inject_launch_failure", "tprims_b200_product_check_raw",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -136,6 +136,7 @@ lib.TAPP_execute_batched_product.argtypes = [
 lib.tprims_b200_product_set_precision.argtypes = [_ip, C.c_int, C.c_int]
 lib.tprims_b200_product_set_tile.argtypes = [_ip, C.c_int]
 lib.tprims_b200_product_set_split_k.argtypes = [_ip, C.c_int]
+lib.tprims_b200_product_check_raw.argtypes = [_ip, _vp, _vp, _vp, _vp]
 lib.tprims_b200_product_set_autotune.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_save_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
@@ -545,6 +546,12 @@ class PlanConfig:
     split_k: int = 0
     autotune: bool = False
 
+    @staticmethod
+    def packed() -> "PlanConfig":
+        """``PlanConfig::packed()`` (plan/config.rs:134): the packed strategy,
+        which is the only strategy here, in drop-in precision."""
+        return PlanConfig()
+
 
 class Problem:
     """A validated problem: built through ``from_labels`` or ``from_dot_general``.
@@ -605,6 +612,17 @@ class Plan:
 
     def report(self) -> dict:
         return self.product.report()
+
+    def check_raw(self, a, b, c, d):
+        """``Plan::check_raw``: the aliasing preflight from the origins alone
+        (nothing is read; None is absent). Raises TprimsError(ERR_ALIASED)."""
+        check(lib.tprims_b200_product_check_raw(self.product.h, ptr_of(a), ptr_of(b), ptr_of(c), ptr_of(d)))
+
+    def execute_raw(self, exec_: Optional[Executor], alpha, a, b, beta, c, d):
+        """``Plan::execute_raw``: check_raw, then D = op_D(alpha AB + beta op_C(C))
+        on raw origins (C may be D itself for an in-place update)."""
+        self.check_raw(a, b, c, d)
+        check(self.product.execute(exec_, alpha, a, b, beta, c, d))
 
     def execute_into(self, exec_: Optional[Executor], alpha, a, b, d):
         """The overwrite form: D = op_D(alpha * op_A(A) op_B(B)); D's old value is not read."""

@@ -382,3 +382,25 @@ def test_report_tile_ctas_and_scratch(tp):
     deep = _gemm_product(tp, 512, 512, 32768).report()
     assert deep["split_k"] > 1 and deep["ctas"] == 64 * deep["split_k"]
     assert deep["scratch_bytes"] >= deep["split_k"] * 512 * 512 * 8  # the split-K partials
+
+
+def test_check_raw_judges_aliasing_from_addresses(tp):
+    """Plan::check_raw (plan/mod.rs:384-428) from the origins alone: nothing is
+    dereferenced, so plain integers serve as addresses here."""
+    m, n, k = 6, 5, 4
+    plan = tp.Plan(tp.Problem.from_labels(1, tp.OperandSpec(tp.LayoutSpec.col_major([m, k])),
+                                          tp.OperandSpec(tp.LayoutSpec.col_major([k, n])),
+                                          tp.OperandSpec(tp.LayoutSpec.col_major([m, n])), [0, 2], [2, 1], [0, 1]),
+                   tp.PlanConfig.packed())
+    A, B, D = 0x100000, 0x200000, 0x300000
+    plan.check_raw(A, B, None, D)
+    plan.check_raw(A, B, D, D)  # C = D, the same mapping: an in-place update
+    plan.check_raw(None, None, None, D)  # absent operands are not judged
+    plan.check_raw(A, B, None, None)
+    for a, b, c, d in [(A, B, None, A + 8 * (m * k - 1)),  # D's first element is A's last
+                       (A, B, None, B - 8 * (m * n - 1)),  # D's last element is B's first
+                       (A, B, D + 8, D)]:  # C shifted by one element over D
+        with pytest.raises(tp.TprimsError) as ei:
+            plan.check_raw(a, b, c, d)
+        assert ei.value.status == tp.ERR_ALIASED
+    plan.check_raw(A, B, None, A + 8 * m * k)  # just past A's range

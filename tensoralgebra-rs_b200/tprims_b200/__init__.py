@@ -787,6 +787,118 @@ def execute_networks(exec_: Optional[Executor], nets: Sequence[Network], inputs,
     PreparedNetworks(nets, inputs, outs, alphas, betas, workspaces).run(exec_)
 
 
+def _parse_einsum(subscripts: str, n: int):
+    """Input and output label lists of an einsum string ("ab,bc->ac"; without
+    "->" the output is the letters that appear once, in alphabetical order).
+    Labels are the letters' code points."""
+    s = subscripts.replace(" ", "")
+    if "->" in s:
+        lhs, rhs = s.split("->")
+    else:
+        lhs, rhs = s, None
+    terms = lhs.split(",")
+    if len(terms) != n:
+        raise TprimsError(ERR_LABELS, f"{len(terms)} input terms for {n} operands")
+    for t in terms + ([rhs] if rhs is not None else []):
+        if not all(ch.isalpha() for ch in t):
+            raise TprimsError(ERR_LABELS, f"einsum term {t!r}: only letters are supported")
+    if rhs is None:
+        counts = {}
+        for t in terms:
+            for ch in t:
+                counts[ch] = counts.get(ch, 0) + 1
+        rhs = "".join(sorted(ch for ch, c in counts.items() if c == 1))
+    return [[ord(ch) for ch in t] for t in terms], [ord(ch) for ch in rhs]
+
+
+def einsum_network(subscripts: str, *operands, conj=None, path=None, out_layout=None):
+    """The Network (and output extents) of an einsum over the given arrays or
+    tensors: one network input per operand with its own extents and strides;
+    a single operand is paired with a rank-0 one (a 1-element array), so traces,
+    sums and permutations run as one binary step. ``out_layout``: (extents,
+    strides) of the output, column-major when None."""
+    if not operands:
+        raise TprimsError(ERR_INVALID_ARGUMENT, "einsum needs at least one operand")
+    labels, out_labels = _parse_einsum(subscripts, len(operands))
+    dt = dtype_of(operands[0])
+    conj = list(conj) if conj is not None else [False] * len(operands)
+    if len(conj) != len(operands):
+        raise TprimsError(ERR_INVALID_ARGUMENT, "one conj flag per operand")
+    inputs, ext = [], {}
+    for x, l, c in zip(operands, labels, conj):
+        if dtype_of(x) != dt:
+            raise TprimsError(ERR_DTYPE, "einsum operands have different dtypes")
+        _, shape, strides = layout_of(x)
+        if len(shape) != len(l):
+            raise TprimsError(ERR_LABELS, f"term of {len(l)} letters for an operand of rank {len(shape)}")
+        for e, lab in zip(shape, l):
+            ext.setdefault(lab, e)
+        inputs.append((OperandSpec(LayoutSpec(list(shape), list(strides)), bool(c)), list(l)))
+    for lab in out_labels:
+        if lab not in ext:
+            raise TprimsError(ERR_UNSUPPORTED, f"output letter {chr(lab)!r} appears in no input")
+    out_shape = [int(ext[lab]) for lab in out_labels]
+    if out_layout is None:
+        st, acc = [], 1
+        for e in out_shape:
+            st.append(acc)
+            acc *= max(e, 1)
+    else:
+        oshape, st = [int(e) for e in out_layout[0]], [int(v) for v in out_layout[1]]
+        if oshape != out_shape:
+            raise TprimsError(ERR_SHAPE, f"out has shape {oshape}, the result {out_shape}")
+    if len(inputs) == 1:
+        inputs.append((OperandSpec(LayoutSpec([], [])), []))
+    net = Network(dt, inputs, (LayoutSpec(out_shape, st), out_labels), path)
+    return net, out_shape
+
+
+def einsum(subscripts: str, *operands, exec_: Optional[Executor] = None, out=None, conj=None, path=None,
+           precision: int = PREC_PLAIN, alpha=1.0, beta=0.0):
+    """``out = alpha * einsum(subscripts, *operands) + beta * out`` through the
+    network driver (binary steps on the GPU, intermediates in device memory).
+
+    Operands are torch tensors (device or host) or numpy arrays of one dtype,
+    with any strides; ``conj`` conjugates chosen operands; ``path`` is a
+    pairwise path (opt_einsum convention) or None for the greedy one. Without
+    ``out`` the result is a new column-major tensor (torch operands: on the
+    first operand's device) or numpy array; with ``out`` its layout is used."""
+    import numpy as np
+
+    out_layout = None
+    if out is not None:
+        _, oshape, ostrides = layout_of(out)
+        out_layout = (oshape, ostrides)
+    net, out_shape = einsum_network(subscripts, *operands, conj=conj, path=path, out_layout=out_layout)
+    try:
+        if precision != PREC_PLAIN:
+            net.set_precision(precision)
+        first = operands[0]
+        torch = None
+        try:
+            import torch
+        except ImportError:  # pragma: no cover
+            pass
+        on_torch = torch is not None and isinstance(first, torch.Tensor)
+        if out is None:
+            if on_torch:
+                n = int(np.prod(out_shape)) if out_shape else 1
+                flat = torch.zeros(n, dtype=first.dtype, device=first.device)
+                # Column-major: the reversed shape in row-major order, permuted back.
+                out = flat.reshape(list(reversed(out_shape))).permute(*reversed(range(len(out_shape)))) \
+                    if out_shape else flat.reshape(())
+            else:
+                out = np.zeros(out_shape, dtype=first.dtype, order="F")
+        ins = list(operands)
+        if len(ins) == 1:  # the rank-0 partner of a single operand
+            ins.append(torch.ones(1, dtype=first.dtype, device=first.device) if on_torch
+                       else np.ones(1, dtype=first.dtype))
+        net.execute(exec_, alpha, ins, out, beta=beta)
+    finally:
+        net.close()
+    return out
+
+
 def contract_batched(items: Sequence[Item], exec_: Optional[Executor] = None):
     """Validate every item, then run them as one grouped submission."""
     arr = (BatchItem * max(len(items), 1))()

@@ -116,3 +116,30 @@ def test_network_in_ozaki_precision(tp, torch_cuda, ex):
     net.execute(ex, 1.0, dev, out)
     assert rel(out.cpu().numpy().reshape((48, 8, 40), order="F"), want) <= 1e-12
     net.close()
+
+
+@pytest.mark.parametrize("dtype", ["float64", "complex128"])
+def test_einsum_front_end(tp, torch_cuda, ex, dtype):
+    """tp.einsum over torch tensors (row-major, device), a given output layout,
+    conjugation, and host numpy operands, against torch.einsum."""
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(3)
+    cplx = dtype == "complex128"
+
+    def rnd(*shape):
+        x = torch.randn(*shape, dtype=torch.float64, device="cuda", generator=g)
+        return torch.complex(x, torch.randn(*shape, dtype=torch.float64, device="cuda", generator=g)) if cplx else x
+
+    def rel(got, want):
+        return float(torch.linalg.norm(got - want) / torch.linalg.norm(want))
+
+    x, y, z = rnd(30, 40), rnd(40, 25), rnd(25, 12)
+    got = tp.einsum("ij,jk,kl->il", x, y, z, exec_=ex)
+    assert got.shape == (30, 12) and rel(got, x @ y @ z) <= 1e-13
+    a, b = rnd(8, 20, 30), rnd(8, 30, 10)
+    out = torch.zeros(10, 8, 20, dtype=a.dtype, device="cuda")
+    assert tp.einsum("bij,bjk->kbi", a, b, exec_=ex, out=out, conj=[True, False]) is out
+    assert rel(out, torch.einsum("bij,bjk->kbi", a.conj().resolve_conj(), b)) <= 1e-13
+    xn, yn = x.cpu().numpy(), y.cpu().numpy()
+    res = tp.einsum("ij,jk->ik", xn, yn, exec_=ex)
+    assert float(np.linalg.norm(res - xn @ yn) / np.linalg.norm(xn @ yn)) <= 1e-13

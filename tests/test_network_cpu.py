@@ -1,6 +1,7 @@
 """N-ary contraction networks without a GPU: path walking, the labels and
 extents of every intermediate, the arena layout, the greedy path and the
 refusals (TAPP status codes). Execution is covered by test_gpu_network.py."""
+import numpy as np
 import pytest
 
 F64, C64 = 1, 3
@@ -189,3 +190,71 @@ def test_greedy_path_orders_a_matrix_chain_by_cost(tp):
     inputs = [(spec(tp, [10, 100]), [0, 1]), (spec(tp, [100, 5]), [1, 2]), (spec(tp, [5, 50]), [2, 3])]
     rep = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([10, 50]), [0, 3]), None).report()
     assert rep["path"][0] == [0, 1] and rep["macs"] == 10 * 100 * 5 + 10 * 5 * 50
+
+
+def test_einsum_parsing_and_refusals(tp):
+    import numpy as np
+
+    a, b = np.zeros((3, 4)), np.zeros((4, 5))
+    net, shape = tp.einsum_network("ab,bc->ac", a, b)
+    assert shape == [3, 5] and net.report()["steps"][0]["labels"] == [ord("a"), ord("c")]
+    assert tp.einsum_network("ab,bc", a, b)[1] == [3, 5]  # implicit output: letters seen once, sorted
+    assert tp.einsum_network("ba,cb", a.T, b.T)[1] == [5, 3][::-1]
+    for args, status in [(("ab,bc,cd->ad", a, b), 14), (("a1,bc->ac", a, b), 14), (("ab,bc->az", a, b), 15),
+                         (("abc,bc->a", a, b), 14), (("ab,bc->ac", a, b.astype(np.float32)), 3)]:
+        with pytest.raises(tp.TprimsError) as ei:
+            tp.einsum_network(*args)
+        assert ei.value.status == status, args
+
+
+@pytest.mark.parametrize("expr,shapes,want", [
+    ("ii->", [(4, 4)], lambda x: np.trace(x)),
+    ("abc->cab", [(2, 3, 4)], lambda x: np.transpose(x, (2, 0, 1))),
+    ("ij->j", [(5, 3)], lambda x: x.sum(axis=0)),
+    ("ij,jk,kl->il", [(3, 4), (4, 5), (5, 2)], lambda x, y, z: x @ y @ z),
+])
+def test_einsum_plans_compose_through_the_oracle(tp, orc, expr, shapes, want):
+    """The einsum front end's networks (a single operand paired with a rank-0
+    one) chained through the CPU oracle equal numpy's result."""
+    g = np.random.default_rng(4)
+    arrays = [g.uniform(-1, 1, s) for s in shapes]
+    net, shape = tp.einsum_network(expr, *arrays)
+    ins = list(arrays) + ([np.ones(())] if len(arrays) == 1 else [])
+    got = _chain_through_oracle(orc, net.report(), ins, [False] * len(ins))
+    assert list(np.shape(got)) == shape
+    np.testing.assert_allclose(got, want(*arrays), rtol=1e-12, atol=1e-12)
+    net.close()
+
+
+def test_einsum_glue_hands_the_right_pointers(tp, monkeypatch):
+    """einsum's allocation and argument passing, with the C execute replaced
+    by a recorder (no GPU): numpy operands give a column-major numpy result,
+    torch operands a column-major tensor, and a single operand gets a
+    one-element partner holding 1."""
+    import ctypes as C
+
+    import torch
+
+    seen = {}
+
+    def recorder(net_h, exec_h, alpha, ins, beta, out, ws):
+        seen["ins"] = [ins[i] for i in range(len(ins))]
+        seen["second"] = C.cast(ins[1], C.POINTER(C.c_double))[0]  # read while the call's buffers live
+        seen["out"] = out
+        seen["alpha"] = C.cast(alpha, C.POINTER(C.c_double))[0]
+        return 0
+
+    monkeypatch.setattr(tp.lib, "tprims_b200_network_execute", recorder)
+    a, b = np.ones((3, 4)), np.ones((4, 5))
+    out = tp.einsum("ab,bc->ac", a, b, alpha=2.0)
+    assert out.shape == (3, 5) and out.flags["F_CONTIGUOUS"]
+    assert seen["ins"][:2] == [a.ctypes.data, b.ctypes.data] and seen["out"] == out.ctypes.data
+    assert seen["alpha"] == 2.0
+    t = torch.ones(6, 2, dtype=torch.float64)
+    res = tp.einsum("ij->ji", t)
+    assert tuple(res.shape) == (2, 6) and res.stride() == (1, 2)
+    assert seen["ins"][0] == t.data_ptr() and seen["second"] == 1.0
+    given = np.zeros((5, 3))  # C order: the result is written through its strides
+    assert tp.einsum("ab,bc->ca", a, b, out=given) is given and seen["out"] == given.ctypes.data
+    with pytest.raises(tp.TprimsError):
+        tp.einsum("ab,bc->ca", a, b, out=np.zeros((3, 5)))

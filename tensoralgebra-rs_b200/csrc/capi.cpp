@@ -809,9 +809,7 @@ extern "C" TAPP_error tprims_b200_execute_product_dlpack(TAPP_tensor_product pla
 extern "C" int64_t tprims_b200_product_scatter(TAPP_tensor_product plan, int which, int64_t* out, int64_t cap) {
   int64_t n = -1;
   ffi([&] {
-    const PackedPlan& pk = product_of(plan).packed;
-    const std::vector<int64_t>* vs[12] = {&pk.a_m, &pk.a_k, &pk.b_k, &pk.b_n, &pk.c_m, &pk.c_n,
-                                          &pk.d_m, &pk.d_n, &pk.h_a, &pk.h_b, &pk.h_c, &pk.h_d};
+    const std::vector<const std::vector<int64_t>*> vs = unorient(product_of(plan).view);
     if (which < 0 || which >= 12) throw Error(ERR_INVALID_ARGUMENT, "scatter index out of range");
     const auto& v = *vs[which];
     n = (int64_t)v.size();

@@ -74,16 +74,24 @@ std::vector<int64_t> build_scatter(const std::vector<int64_t>& extents, const st
   for (auto e : extents) total *= e;
   std::vector<int64_t> out;
   if (total <= 0) return out;
-  out.reserve((size_t)total);
-  // Mixed-radix odometer, fastest axis first (scatter.rs:70).
+  out.resize((size_t)total);
+  if (extents.empty()) {
+    out[0] = 0;
+    return out;
+  }
+  // Mixed-radix odometer, fastest axis first (scatter.rs:70): the fastest
+  // axis is written as one arithmetic run per position of the outer axes,
+  // and only the outer axes step the odometer.
+  const int64_t e0 = extents[0], s0 = strides[0];
   std::vector<int64_t> ctr(extents.size(), 0);
-  int64_t off = 0;
-  for (int64_t i = 0; i < total; ++i) {
-    out.push_back(off);
-    for (size_t d = 0; d < extents.size(); ++d) {
-      off += strides[d];
+  int64_t base = 0;
+  int64_t* o = out.data();
+  for (int64_t i = 0; i < total; i += e0) {
+    for (int64_t j = 0; j < e0; ++j) o[i + j] = base + j * s0;
+    for (size_t d = 1; d < extents.size(); ++d) {
+      base += strides[d];
       if (++ctr[d] < extents[d]) break;
-      off -= strides[d] * extents[d];
+      base -= strides[d] * extents[d];
       ctr[d] = 0;
     }
   }
@@ -192,23 +200,25 @@ bool PackedPlan::transposes_gemm(size_t mr) const {
   return d_n_run_len < d_m_run_len;
 }
 
-OrientedView orient(const PackedPlan& pk, bool swap) {
+OrientedView orient(PackedPlan& pk, bool swap) {
   OrientedView v;
   v.swapped = swap;
+  // The vectors move into the view (they are the plan's largest part); the
+  // packed plan keeps its statistics, and unorient() gives the vectors back.
   if (!swap) {
-    v.a_m = pk.a_m; v.a_k = pk.a_k; v.b_k = pk.b_k; v.b_n = pk.b_n;
-    v.c_m = pk.c_m; v.c_n = pk.c_n; v.d_m = pk.d_m; v.d_n = pk.d_n;
-    v.h_a = pk.h_a; v.h_b = pk.h_b;
+    v.a_m = std::move(pk.a_m); v.a_k = std::move(pk.a_k); v.b_k = std::move(pk.b_k); v.b_n = std::move(pk.b_n);
+    v.c_m = std::move(pk.c_m); v.c_n = std::move(pk.c_n); v.d_m = std::move(pk.d_m); v.d_n = std::move(pk.d_n);
+    v.h_a = std::move(pk.h_a); v.h_b = std::move(pk.h_b);
     v.conj_a = pk.conj_a; v.conj_b = pk.conj_b;
   } else {
     // D^T = B^T A^T: B plays A's role and the output's row/column scatters swap.
-    v.a_m = pk.b_n; v.a_k = pk.b_k; v.b_k = pk.a_k; v.b_n = pk.a_m;
-    v.c_m = pk.c_n; v.c_n = pk.c_m; v.d_m = pk.d_n; v.d_n = pk.d_m;
-    v.h_a = pk.h_b; v.h_b = pk.h_a;
+    v.a_m = std::move(pk.b_n); v.a_k = std::move(pk.b_k); v.b_k = std::move(pk.a_k); v.b_n = std::move(pk.a_m);
+    v.c_m = std::move(pk.c_n); v.c_n = std::move(pk.c_m); v.d_m = std::move(pk.d_n); v.d_n = std::move(pk.d_m);
+    v.h_a = std::move(pk.h_b); v.h_b = std::move(pk.h_a);
     v.conj_a = pk.conj_b; v.conj_b = pk.conj_a;
   }
-  v.h_c = pk.h_c;
-  v.h_d = pk.h_d;
+  v.h_c = std::move(pk.h_c);
+  v.h_d = std::move(pk.h_d);
   v.conj_c = pk.conj_c;
   v.conj_d = pk.conj_d;
   v.M = (int64_t)v.d_m.size();
@@ -220,6 +230,12 @@ OrientedView orient(const PackedPlan& pk, bool swap) {
   v.d_mfast = lead_stride(v.d_m) <= lead_stride(v.d_n);
   v.c_mfast = lead_stride(v.c_m) <= lead_stride(v.c_n);
   return v;
+}
+
+std::vector<const std::vector<int64_t>*> unorient(const OrientedView& v) {
+  if (!v.swapped)
+    return {&v.a_m, &v.a_k, &v.b_k, &v.b_n, &v.c_m, &v.c_n, &v.d_m, &v.d_n, &v.h_a, &v.h_b, &v.h_c, &v.h_d};
+  return {&v.b_n, &v.b_k, &v.a_k, &v.a_m, &v.c_n, &v.c_m, &v.d_n, &v.d_m, &v.h_b, &v.h_a, &v.h_c, &v.h_d};
 }
 
 }  // namespace tprims

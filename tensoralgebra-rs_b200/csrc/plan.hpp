@@ -66,6 +66,11 @@ struct OrientedView {
   bool a_kfast = false, b_kfast = true, d_mfast = true, c_mfast = true;
 };
 
-OrientedView orient(const PackedPlan& pk, bool swap);
+// The kernels' view of a packed plan; the scatter vectors move out of `pk`
+// (which keeps its statistics and run structure).
+OrientedView orient(PackedPlan& pk, bool swap);
+// The packed plan's 12 scatter vectors (a_m, a_k, b_k, b_n, c_m, c_n, d_m,
+// d_n, h_a, h_b, h_c, h_d) as they were before orientation, read from the view.
+std::vector<const std::vector<int64_t>*> unorient(const OrientedView& v);
 
 }  // namespace tprims

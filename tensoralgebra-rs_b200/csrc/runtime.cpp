@@ -142,7 +142,8 @@ int64_t sequence_stride(const std::vector<int64_t>& v) {
 
 Product::Product(const Problem& p) : problem(p), uid(g_product_uid.fetch_add(1)) {
   packed = PackedPlan::from_problem(p);
-  view = orient(packed, packed.transposes_gemm(32));
+  const bool swap = packed.transposes_gemm(32);
+  view = orient(packed, swap);
   tiny_h = dev::TinyStrides{sequence_stride(view.h_a), sequence_stride(view.h_b), sequence_stride(view.h_c),
                             sequence_stride(view.h_d)};
   signature = problem_signature(*this);

@@ -121,7 +121,7 @@ struct DeviceScatters {
 
 struct Product {
   Problem problem;
-  PackedPlan packed;
+  PackedPlan packed;  // statistics and run structure; its scatter vectors moved into `view`
   OrientedView view;
   Scheme scheme = Scheme::Plain;
   int ozaki_slices = 0;

@@ -384,7 +384,7 @@ def test_report_tile_ctas_and_scratch(tp):
     assert deep["scratch_bytes"] >= deep["split_k"] * 512 * 512 * 8  # the split-K partials
 
 
-def test_check_raw_judges_aliasing_from_addresses(tp):
+def test_check_raw_decides_aliasing_from_addresses(tp):
     """Plan::check_raw (plan/mod.rs:384-428) from the origins alone: nothing is
     dereferenced, so plain integers serve as addresses here."""
     m, n, k = 6, 5, 4
@@ -395,7 +395,7 @@ def test_check_raw_judges_aliasing_from_addresses(tp):
     A, B, D = 0x100000, 0x200000, 0x300000
     plan.check_raw(A, B, None, D)
     plan.check_raw(A, B, D, D)  # C = D, the same mapping: an in-place update
-    plan.check_raw(None, None, None, D)  # absent operands are not judged
+    plan.check_raw(None, None, None, D)  # absent operands are not checked
     plan.check_raw(A, B, None, None)
     for a, b, c, d in [(A, B, None, A + 8 * (m * k - 1)),  # D's first element is A's last
                        (A, B, None, B - 8 * (m * n - 1)),  # D's last element is B's first

@@ -380,6 +380,20 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_networks_execute(TAPP_executor exec, i
                                                            const void* const* betas, void* const* outs,
                                                            void* const* workspaces);
 
+/* Scale-out without collectives: contract_batched over several executors
+   (one per GPU, or several per GPU). The items are validated all-or-nothing,
+   balanced longest-first by their multiply-accumulates over the executors of
+   the device that holds each item's D (a host D may go anywhere; a device with
+   no executor in `execs` is TPRIMS_ERR_DEVICE), and each executor's share runs
+   as one grouped submission on its own stream, all streams side by side; no
+   data moves between devices. tprims_b200_balance is the assignment alone:
+   item i of cost costs[i] and home device homes[i] (NULL or < 0: any) goes to
+   part assignment[i] of n_parts parts on part_devices. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_contract_batched_sharded(const TAPP_executor* execs, int n_exec, int n,
+                                                                   const tprims_b200_batch_item* items);
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_balance(int n, const double* costs, const int* homes, int n_parts,
+                                                  const int* part_devices, int* assignment);
+
 /* Plan::vjp. For D = alpha*op_A(A)*op_B(B) (+ beta*C), given the cotangent dD,
    write dA (when non-NULL) and dB (when non-NULL) in the layouts of A and B:
    dA = conj-correct adjoint contraction of dD with B, scattered onto A's

@@ -728,6 +728,54 @@ extern "C" TAPP_error tprims_b200_network_execute(tprims_b200_network net, TAPP_
   return tprims_b200_networks_execute(exec, 1, &net, al, ins, be, outs, ws);
 }
 
+extern "C" TAPP_error tprims_b200_balance(int n, const double* costs, const int* homes, int n_parts,
+                                         const int* part_devices, int* assignment) {
+  return ffi([&] {
+    if (n < 0 || n_parts < 0) throw Error(ERR_SHAPE, "negative count");
+    if (n > 0 && (!costs || !assignment)) null_arg("costs or assignment");
+    if (n_parts > 0 && !part_devices) null_arg("part devices");
+    std::vector<double> c(costs, costs + n);
+    std::vector<int> h(n, -1);
+    if (homes)
+      for (int i = 0; i < n; ++i) h[i] = homes[i];
+    const std::vector<int> d(part_devices, part_devices + n_parts);
+    const std::vector<int> part = balance_parts(c, h, d);
+    for (int i = 0; i < n; ++i) assignment[i] = part[i];
+  });
+}
+
+extern "C" TAPP_error tprims_b200_contract_batched_sharded(const TAPP_executor* execs, int n_exec, int n,
+                                                           const tprims_b200_batch_item* items) {
+  return ffi([&] {
+    if (n < 0 || n_exec < 0) throw Error(ERR_SHAPE, "negative count");
+    if (n > 0 && !items) null_arg("item array");
+    if (n_exec == 0 || !execs) throw Error(ERR_INVALID_ARGUMENT, "no executors");
+    std::vector<Product*> ps;
+    std::vector<Scalar> als, bes;
+    std::vector<Item> its;
+    // All-or-nothing: every item is checked before anything runs (batch.rs:127-130).
+    for (int i = 0; i < n; ++i) {
+      Product& p = product_of(items[i].plan);
+      if (!items[i].alpha) null_arg("alpha");
+      if (!items[i].beta) null_arg("beta");
+      const Scalar al = read_scalar(p.problem.dtype, items[i].alpha), be = read_scalar(p.problem.dtype, items[i].beta);
+      Item it{items[i].A, items[i].B, items[i].C, items[i].D};
+      validate_item(p, it, be.is_zero());
+      ps.push_back(&p);
+      als.push_back(al);
+      bes.push_back(be);
+      its.push_back(it);
+    }
+    if (n == 0) return;
+    std::vector<Executor*> exs;
+    for (int e = 0; e < n_exec; ++e) {
+      if (execs[e] == 0) null_arg("executor " + std::to_string(e));
+      exs.push_back(&resolve_exec(execs[e])->get());
+    }
+    execute_items_sharded(exs.data(), n_exec, n, ps.data(), als.data(), bes.data(), its.data());
+  });
+}
+
 extern "C" TAPP_error tprims_b200_product_vjp(TAPP_tensor_product plan, TAPP_executor exec, const void* alpha,
                                               const void* A, const void* B, const void* dD, void* dA, void* dB) {
   return ffi([&] {

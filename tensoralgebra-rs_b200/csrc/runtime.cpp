@@ -1181,6 +1181,73 @@ void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alp
   if (ex.sync || staged) finish(ex);
 }
 
+std::vector<int> balance_parts(const std::vector<double>& costs, const std::vector<int>& homes,
+                               const std::vector<int>& part_devices) {
+  const size_t n = costs.size();
+  if (homes.size() != n) throw Error(ERR_INVALID_ARGUMENT, "one home device per item");
+  if (part_devices.empty() && n > 0) throw Error(ERR_INVALID_ARGUMENT, "no parts to balance over");
+  std::vector<size_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return costs[a] > costs[b]; });
+  std::vector<double> load(part_devices.size(), 0.0);
+  std::vector<int> part(n, -1);
+  for (size_t i : order) {
+    int best = -1;
+    for (size_t q = 0; q < part_devices.size(); ++q)
+      if ((homes[i] < 0 || part_devices[q] == homes[i]) && (best < 0 || load[q] < load[(size_t)best]))
+        best = (int)q;
+    if (best < 0)
+      throw Error(ERR_DEVICE, "item " + std::to_string(i) + " lives on CUDA device " + std::to_string(homes[i]) +
+                                  ", which no executor of the call serves");
+    part[i] = best;
+    load[(size_t)best] += costs[i];
+  }
+  return part;
+}
+
+void execute_items_sharded(Executor* const* exs, int n_exec, int n, Product* const* plans, const Scalar* alpha,
+                           const Scalar* beta, const Item* items) {
+  NvtxRange range("tprims.contract_batched_sharded");
+  std::vector<double> costs(n);
+  std::vector<int> homes(n, -1), devs(n_exec);
+  for (int e = 0; e < n_exec; ++e) devs[e] = exs[e]->device;
+  for (int i = 0; i < n; ++i) {
+    costs[i] = plans[i]->problem.macs();
+    cudaPointerAttributes at;
+    if (items[i].d && cudaPointerGetAttributes(&at, items[i].d) == cudaSuccess && at.type == cudaMemoryTypeDevice)
+      homes[i] = at.device;
+    else
+      cudaGetLastError();
+  }
+  const std::vector<int> part = balance_parts(costs, homes, devs);
+  std::vector<std::vector<int>> idx(n_exec);
+  for (int i = 0; i < n; ++i) idx[part[i]].push_back(i);
+  // Enqueue every share first (the streams run side by side), then drain.
+  for (int e = 0; e < n_exec; ++e) {
+    if (idx[e].empty()) continue;
+    std::vector<Product*> ps;
+    std::vector<Scalar> al, be;
+    std::vector<Item> its;
+    for (int i : idx[e]) {
+      ps.push_back(plans[i]);
+      al.push_back(alpha[i]);
+      be.push_back(beta[i]);
+      its.push_back(items[i]);
+    }
+    Executor& ex = *exs[e];
+    std::lock_guard<std::mutex> lk(ex.mu);
+    DeviceGuard g(ex.device);
+    if (enqueue_items(ex, (int)ps.size(), ps.data(), al.data(), be.data(), its.data())) finish(ex);
+  }
+  for (int e = 0; e < n_exec; ++e) {
+    if (idx[e].empty() || !exs[e]->sync) continue;
+    Executor& ex = *exs[e];
+    std::lock_guard<std::mutex> lk(ex.mu);
+    DeviceGuard g(ex.device);
+    finish(ex);
+  }
+}
+
 void execute_networks(Executor& ex, int n, Network* const* nets, const Scalar* alpha, const Scalar* beta,
                       const void* const* const* inputs, void* const* outs, void* const* workspaces) {
   NvtxRange range("tprims.execute_networks");

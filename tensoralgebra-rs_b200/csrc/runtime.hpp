@@ -183,6 +183,21 @@ void execute_item(Product& p, Executor& ex, Scalar alpha, Scalar beta, const Ite
 void execute_items(Executor& ex, int n, Product* const* plans, const Scalar* alpha, const Scalar* beta,
                    const Item* items);
 
+// Longest-first balance of items over parts: items in decreasing cost (ties
+// by index) each go to the least-loaded part whose device is the item's home
+// (home < 0: any part). Returns the part of each item; ERR_DEVICE when an
+// item's home has no part.
+std::vector<int> balance_parts(const std::vector<double>& costs, const std::vector<int>& homes,
+                               const std::vector<int>& part_devices);
+
+// contract_batched over several executors (one per GPU, or several per GPU):
+// the validated items are balanced by their multiply-accumulates over the
+// executors of the device that holds each item's output (host outputs go
+// anywhere), each executor's share is one grouped submission on its own stream,
+// and every stream is drained before returning. No data moves between devices.
+void execute_items_sharded(Executor* const* exs, int n_exec, int n, Product* const* plans, const Scalar* alpha,
+                           const Scalar* beta, const Item* items);
+
 // Plan::vjp: cotangents of A and B.
 void execute_vjp(Product& p, Executor& ex, Scalar alpha, const void* A, const void* B, const void* dD, void* dA,
                  void* dB);

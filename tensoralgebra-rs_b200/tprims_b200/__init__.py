@@ -75,6 +75,7 @@ ABI_SYMBOLS = [
     "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
     "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
     "tprims_b200_device_allocations", "tprims_b200_executor_inject_launch_failure", "tprims_b200_product_check_raw",
+    "tprims_b200_contract_batched_sharded", "tprims_b200_balance",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -175,6 +176,9 @@ class BatchItem(C.Structure):
 
 
 lib.tprims_b200_contract_batched.argtypes = [_ip, C.c_int, C.POINTER(BatchItem)]
+lib.tprims_b200_contract_batched_sharded.argtypes = [C.POINTER(_ip), C.c_int, C.c_int, C.POINTER(BatchItem)]
+lib.tprims_b200_balance.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int,
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]
 
 
 class TprimsError(RuntimeError):
@@ -897,6 +901,39 @@ def einsum(subscripts: str, *operands, exec_: Optional[Executor] = None, out=Non
     finally:
         net.close()
     return out
+
+
+def balance(costs, part_devices, homes=None):
+    """Longest-first assignment of items (costs, home devices; None: any) to
+    parts living on ``part_devices``; returns the part of each item."""
+    n, p = len(costs), len(part_devices)
+    c = (C.c_double * max(n, 1))(*[float(x) for x in costs])
+    h = (C.c_int * max(n, 1))(*[(-1 if x is None else int(x)) for x in (homes or [None] * n)])
+    d = (C.c_int * max(p, 1))(*[int(x) for x in part_devices])
+    out = (C.c_int * max(n, 1))()
+    check(lib.tprims_b200_balance(n, c, h, p, d, out))
+    return [out[i] for i in range(n)]
+
+
+def _batch_items(items: Sequence[Item]):
+    arr = (BatchItem * max(len(items), 1))()
+    keep = []
+    for i, it in enumerate(items):
+        al = scalar_bytes(it.plan.dtype, it.alpha)
+        be = scalar_bytes(it.plan.dtype, it.beta)
+        keep += [al, be]
+        arr[i] = BatchItem(it.plan.product.h, C.cast(al, _vp), ptr_of(it.a), ptr_of(it.b), C.cast(be, _vp),
+                           ptr_of(it.c), ptr_of(it.d))
+    return arr, keep
+
+
+def contract_batched_sharded(items: Sequence[Item], execs: Sequence[Executor]):
+    """contract_batched over several executors (one per GPU, or several per
+    GPU): items balanced by cost over the executors of their output's device,
+    each share one grouped submission on its executor's stream."""
+    arr, keep = _batch_items(items)
+    hs = (_ip * max(len(execs), 1))(*[e.h for e in execs])
+    check(lib.tprims_b200_contract_batched_sharded(hs, len(execs), len(items), arr))
 
 
 def contract_batched(items: Sequence[Item], exec_: Optional[Executor] = None):

@@ -61,3 +61,33 @@ def test_threads_share_one_executor_and_use_a_second(tp, torch_cuda):
     assert not errors, errors[0]
     ex1.close()
     ex2.close()
+
+
+def test_sharded_list_over_two_executors(tp, torch_cuda):
+    """contract_batched_sharded: a list balanced over two executors (both on
+    this GPU, as two GPUs would each hold one), every item exact, host-staged
+    outputs included."""
+    torch = torch_cuda
+    g = np.random.default_rng(31)
+    execs = [tp.Executor(), tp.Executor()]
+    items, wants, outs = [], [], []
+    for q in range(10):
+        m, n, k = (int(x) for x in g.integers(20, 160, size=3))
+        A, B = g.uniform(-1, 1, (m, k)), g.uniform(-1, 1, (k, n))
+        a = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+        b = torch.from_numpy(B.ravel(order="F").copy()).cuda()
+        d = torch.zeros(m * n, dtype=torch.float64, device="cuda") if q % 3 else np.zeros(m * n)
+        plan = tp.Plan(tp.Problem.from_labels(1, tp.OperandSpec(tp.LayoutSpec.col_major([m, k])),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major([k, n])),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major([m, n])), [0, 2], [2, 1], [0, 1]))
+        items.append(tp.Item(plan, 1.0, a, b, d, _keep=[a, b]))
+        wants.append((A @ B, m, n))
+        outs.append(d)
+    part = tp.balance([it.plan.report()["macs"] for it in items], [0, 0])
+    assert set(part) == {0, 1}  # both executors get work
+    tp.contract_batched_sharded(items, execs)
+    for (w, m, n), d in zip(wants, outs):
+        got = (d.cpu().numpy() if hasattr(d, "cpu") else d).reshape((m, n), order="F")
+        assert float(np.linalg.norm(got - w) / np.linalg.norm(w)) <= 1e-13
+    for e in execs:
+        e.close()

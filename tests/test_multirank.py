@@ -49,3 +49,20 @@ def test_shard_is_balanced():
     for n in (10, 4096, 3):
         sizes = [bench.shard(n, r, 8)[1] - bench.shard(n, r, 8)[0] for r in range(8)]
         assert sum(sizes) == n and max(sizes) - min(sizes) <= 1
+
+
+def test_balance_is_longest_first_and_respects_devices(tp):
+    """The assignment behind contract_batched_sharded: items in decreasing
+    cost go to the least-loaded part of their output's device."""
+    # Six items on any device over three parts: LPT gives loads 9, 9, 9.
+    part = tp.balance([5, 4, 3, 3, 2, 2][::-1], [0, 0, 0])
+    costs = [5, 4, 3, 3, 2, 2][::-1]
+    loads = [sum(c for c, q in zip(costs, part) if q == k) for k in range(3)]
+    assert sorted(loads) == [6, 6, 7]
+    # Homes: items on device 1 go only to parts on device 1.
+    part = tp.balance([10, 1, 1, 10], [0, 1, 1], homes=[1, 0, None, 1])
+    assert part[0] in (1, 2) and part[3] in (1, 2) and part[0] != part[3] and part[1] == 0
+    with pytest.raises(tp.TprimsError) as ei:
+        tp.balance([1, 1], [0, 0], homes=[0, 3])
+    assert ei.value.status == tp.ERR_DEVICE
+    assert tp.balance([], [0]) == []

@@ -404,3 +404,62 @@ def test_check_raw_decides_aliasing_from_addresses(tp):
             plan.check_raw(a, b, c, d)
         assert ei.value.status == tp.ERR_ALIASED
     plan.check_raw(A, B, None, A + 8 * m * k)  # just past A's range
+
+
+def _random_problem(g):
+    """Random labels over roles batch / M / N / K (with a diagonal or a
+    reduction now and then), random extents, permuted and sometimes negative
+    or padded strides; returns (a, b, d) dicts for _product and the base
+    offsets that keep every addressed element inside its buffer."""
+    roles = {"h": g.integers(0, 2), "m": g.integers(1, 3), "n": g.integers(1, 3), "k": g.integers(1, 3)}
+    labels, nxt = {}, 0
+    for r, cnt in roles.items():
+        labels[r] = list(range(nxt, nxt + int(cnt)))
+        nxt += int(cnt)
+    ext = {l: int(g.integers(1, 5)) for ls in labels.values() for l in ls}
+    la = labels["h"] + labels["m"] + labels["k"]
+    lb = labels["h"] + labels["k"] + labels["n"]
+    ld = labels["h"] + labels["m"] + labels["n"]
+    if g.random() < 0.3:  # a reduction label only in A
+        r = nxt
+        ext[r] = int(g.integers(2, 4))
+        la = la + [r]
+    if g.random() < 0.3 and labels["k"]:  # a diagonal: one K label twice in A
+        la = la + [labels["k"][0]]
+
+    def layout(ls):
+        ls = [ls[i] for i in g.permutation(len(ls))]
+        st, acc = [], 1
+        for l in ls:
+            st.append(acc * (-1 if g.random() < 0.2 else 1))
+            acc *= ext[l] + (1 if g.random() < 0.3 else 0)
+        lo = sum((ext[l] - 1) * s for l, s in zip(ls, st) if s < 0)
+        return {"ext": [ext[l] for l in ls], "str": st, "lab": ls}, -lo, acc
+
+    return layout(la), layout(lb), layout(ld), ext
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_scatter_vectors_reproduce_the_contraction(tp, orc, seed):
+    """The plan's 12 scatter vectors (as the kernels address memory: h + m + k
+    for A, h + k + n for B, h + m + n for D) contract random data exactly as
+    the brute-force oracle does, in whichever orientation the planner picked."""
+    g = np.random.default_rng(1000 + seed)
+    (a, oa, na), (b, ob, nb), (d, od, nd), ext = _random_problem(g)
+    p = _product(tp, a, b, d)
+    sc = {name: np.array(tp.product_scatter(p, name), dtype=np.int64) for name in tp.SCATTER_NAMES}
+    A = g.uniform(-1, 1, na + 8)
+    B = g.uniform(-1, 1, nb + 8)
+    D = np.zeros(nd + 8)
+    h_n = max(len(sc["h_d"]), 1)
+    h_a = sc["h_a"] if len(sc["h_a"]) else np.zeros(1, np.int64)
+    h_b = sc["h_b"] if len(sc["h_b"]) else np.zeros(1, np.int64)
+    h_d = sc["h_d"] if len(sc["h_d"]) else np.zeros(1, np.int64)
+    for h in range(h_n):
+        Am = A[oa + h_a[h] + sc["a_m"][:, None] + sc["a_k"][None, :]]
+        Bn = B[ob + h_b[h] + sc["b_k"][:, None] + sc["b_n"][None, :]]
+        D[od + h_d[h] + sc["d_m"][:, None] + sc["d_n"][None, :]] = Am @ Bn
+    want = np.zeros(nd + 8)
+    orc.label_contract(1.0, orc.View(A, a["ext"], a["str"], a["lab"], oa), orc.View(B, b["ext"], b["str"], b["lab"], ob),
+                       0.0, None, orc.View(want, d["ext"], d["str"], d["lab"], od))
+    np.testing.assert_allclose(D, want, rtol=1e-12, atol=1e-12)

@@ -35,7 +35,9 @@ def _rank_main(rank, world, port, n, out):
 @pytest.mark.parametrize("n", [4096, 7, 1])
 def test_two_gloo_ranks_shard_and_reduce(n):
     world = 2
-    with mp.Manager() as mgr:
+    # A spawned manager: forking this (possibly multi-threaded) test process
+    # could deadlock the child.
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), n, out), nprocs=world, join=True)
         res = dict(out)

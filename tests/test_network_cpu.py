@@ -258,3 +258,41 @@ def test_einsum_glue_hands_the_right_pointers(tp, monkeypatch):
     assert tp.einsum("ab,bc->ca", a, b, out=given) is given and seen["out"] == given.ctypes.data
     with pytest.raises(tp.TprimsError):
         tp.einsum("ab,bc->ca", a, b, out=np.zeros((3, 5)))
+
+
+@pytest.mark.parametrize("seed", range(30))
+def test_random_networks_compose_through_the_oracle(tp, orc, seed):
+    """Random networks of 3 to 5 tensors (labels shared by one to three
+    tensors, some kept in the output, some summed inside one tensor), planned
+    on the greedy path or a random valid path, chained through the oracle,
+    equal numpy's einsum."""
+    g = np.random.default_rng(500 + seed)
+    n_t = int(g.integers(3, 6))
+    n_l = int(g.integers(3, 8))
+    ext = [int(g.integers(1, 4)) for _ in range(n_l)]
+    labels = [[] for _ in range(n_t)]
+    for l in range(n_l):
+        for t in g.choice(n_t, size=int(g.integers(1, 4)), replace=False):
+            labels[t].append(l)
+    for t in range(n_t):  # no empty tensor
+        if not labels[t]:
+            labels[t].append(int(g.integers(0, n_l)))
+    present = sorted({l for ls in labels for l in ls})
+    out = [l for l in present if g.random() < 0.35]
+    arrays = [g.uniform(-1, 1, [ext[l] for l in ls]) for ls in labels]
+    inputs = [(spec(tp, [ext[l] for l in ls]), ls) for ls in labels]
+    if seed % 2:
+        path, m = [], n_t
+        while m > 1:
+            i, j = (int(x) for x in g.choice(m, size=2, replace=False))
+            path.append((i, j))
+            m -= 1
+    else:
+        path = None
+    net = tp.Network(F64, inputs, (tp.LayoutSpec.col_major([ext[l] for l in out]), out), path)
+    got = _chain_through_oracle(orc, net.report(), arrays, [False] * n_t)
+    letters = "abcdefgh"
+    expr = ",".join("".join(letters[l] for l in ls) for ls in labels) + "->" + "".join(letters[l] for l in out)
+    want = np.einsum(expr, *arrays)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+    net.close()

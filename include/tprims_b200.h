@@ -249,8 +249,8 @@ TPRIMS_B200_EXPORT size_t tprims_b200_executor_kernel_times(TAPP_executor exec, 
    error bound is stated in the plan report. */
 enum {
   TPRIMS_PREC_PLAIN = 0,
-  TPRIMS_PREC_BF16X3 = 1, /* f32/c32: hi/lo BF16 split, 3 products, FP32 accumulation */
-  TPRIMS_PREC_BF16X6 = 2, /* f32/c32: 3-way BF16 split, 6 products, FP32 accumulation */
+  TPRIMS_PREC_BF16X3 = 1, /* f32: hi/lo BF16 split, 3 products, FP32 accumulation */
+  TPRIMS_PREC_BF16X6 = 2, /* f32: 3-way BF16 split, 6 products, FP32 accumulation */
   TPRIMS_PREC_OZAKI_INT8 = 3 /* f64/c64: INT8 slices, exact INT32 accumulation */
 };
 /* Choose the precision scheme of a product. `slices` is the INT8 slice count

@@ -495,35 +495,6 @@ def test_contract_batched_uneven_items(tp, ex, torch_cuda, orc):
         assert np.allclose(got, want, rtol=1e-12, atol=1e-12)
 
 
-@pytest.mark.parametrize("dt", ["float32", "complex64"])
-def test_contract_batched_single_precision_lists(tp, ex, torch_cuda, dt):
-    """Grouped lists of f32 items (SIMT tiles) and c32 items (SIMT tiles fed by
-    the cp.async ring, the conjugation variant chosen per tile) of uneven
-    extents, against float64 / complex128 sums (plain bound 1e-6)."""
-    torch = torch_cuda
-    rng = np.random.default_rng(13)
-    code = tp.F32 if dt == "float32" else tp.C32
-    items, refs = [], []
-    for q, (m, n, k) in enumerate([(16, 40, 8), (100, 3, 50), (33, 65, 17), (130, 70, 90), (64, 64, 64),
-                                   (7, 200, 33), (257, 129, 40)]):
-        conj_a = dt == "complex64" and q % 2 == 1
-        a, b = rnd(rng, dt, m * k), rnd(rng, dt, k * n)
-        ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
-        td = torch.zeros(m * n, dtype=ta.dtype, device="cuda")
-        plan = tp.Plan(tp.Problem.from_labels(code, tp.OperandSpec(tp.LayoutSpec.col_major([m, k]), conj_a),
-                                              tp.OperandSpec(tp.LayoutSpec.col_major([k, n])),
-                                              tp.OperandSpec(tp.LayoutSpec.col_major([m, n])), [0, 2], [2, 1], [0, 1]))
-        items.append(tp.Item(plan, 1.0, ta.data_ptr(), tb.data_ptr(), td.data_ptr()))
-        A = a.astype(np.complex128 if dt == "complex64" else np.float64).reshape(k, m).T
-        B = b.astype(A.dtype).reshape(n, k).T
-        refs.append(((np.conj(A) if conj_a else A) @ B, td, (ta, tb)))
-    tp.contract_batched(items, ex)
-    torch.cuda.synchronize()
-    for want, td, _ in refs:
-        got = td.cpu().numpy().astype(want.dtype).reshape(want.shape[1], want.shape[0]).T
-        assert float(np.linalg.norm(got - want) / np.linalg.norm(want)) <= 1e-6
-
-
 def test_dlpack_execute_with_cuda_tensors(tp, ex, torch_cuda):
     import ctypes as C
 
@@ -580,3 +551,32 @@ def test_reference_c_consumers_run_against_this_library(prog):
         pytest.skip("reference consumers not built (the reference tree was absent at build time)")
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("dt", ["float32", "complex64"])
+def test_contract_batched_single_precision_lists(tp, ex, torch_cuda, dt):
+    """Grouped lists of f32 items (SIMT tiles) and c32 items (SIMT tiles fed by
+    the cp.async ring, the conjugation variant chosen per tile) of uneven
+    extents, against float64 / complex128 sums (plain bound 1e-6)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(13)
+    code = tp.F32 if dt == "float32" else tp.C32
+    items, refs = [], []
+    for q, (m, n, k) in enumerate([(16, 40, 8), (100, 3, 50), (33, 65, 17), (130, 70, 90), (64, 64, 64),
+                                   (7, 200, 33), (257, 129, 40)]):
+        conj_a = dt == "complex64" and q % 2 == 1
+        a, b = rnd(rng, dt, m * k), rnd(rng, dt, k * n)
+        ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+        td = torch.zeros(m * n, dtype=ta.dtype, device="cuda")
+        plan = tp.Plan(tp.Problem.from_labels(code, tp.OperandSpec(tp.LayoutSpec.col_major([m, k]), conj_a),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major([k, n])),
+                                              tp.OperandSpec(tp.LayoutSpec.col_major([m, n])), [0, 2], [2, 1], [0, 1]))
+        items.append(tp.Item(plan, 1.0, ta.data_ptr(), tb.data_ptr(), td.data_ptr()))
+        A = a.astype(np.complex128 if dt == "complex64" else np.float64).reshape(k, m).T
+        B = b.astype(A.dtype).reshape(n, k).T
+        refs.append(((np.conj(A) if conj_a else A) @ B, td, (ta, tb)))
+    tp.contract_batched(items, ex)
+    torch.cuda.synchronize()
+    for want, td, _ in refs:
+        got = td.cpu().numpy().astype(want.dtype).reshape(want.shape[1], want.shape[0]).T
+        assert float(np.linalg.norm(got - want) / np.linalg.norm(want)) <= 1e-6

@@ -296,3 +296,35 @@ def test_random_networks_compose_through_the_oracle(tp, orc, seed):
     want = np.einsum(expr, *arrays)
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
     net.close()
+
+
+def test_c_entry_refusals_need_no_gpu(tp):
+    """Argument checks of the network and sharded-list entry points run before
+    any executor is touched, so they answer without a GPU."""
+    import ctypes as C
+
+    lib = tp.lib
+    assert lib.tprims_b200_network_destroy(0) == tp.ERR_INVALID_ARGUMENT
+    assert lib.tprims_b200_network_report(0, None, 0) == 0
+    size = C.c_size_t(0)
+    assert lib.tprims_b200_network_workspace_size(0, C.byref(size)) == tp.ERR_INVALID_ARGUMENT
+    h = tp._ip(0)
+    # Null descriptions, a negative count, too few inputs.
+    assert lib.tprims_b200_network_create(C.byref(h), 1, 2, None, None, None, None, None, 0, None, None, None, 0,
+                                          None) == tp.ERR_INVALID_ARGUMENT
+    assert lib.tprims_b200_network_create(C.byref(h), 1, -1, None, None, None, None, None, 0, None, None, None, 0,
+                                          None) == tp.ERR_SHAPE
+    assert lib.tprims_b200_network_create(None, 1, 2, None, None, None, None, None, 0, None, None, None, 0,
+                                          None) == tp.ERR_INVALID_ARGUMENT
+    nets = (tp._ip * 1)(0)
+    ptrs = (tp._vp * 1)()
+    ins = (C.POINTER(tp._vp) * 1)()
+    assert lib.tprims_b200_networks_execute(0, 1, nets, ptrs, ins, ptrs, ptrs, ptrs) == tp.ERR_INVALID_ARGUMENT
+    assert lib.tprims_b200_networks_execute(0, 0, None, None, None, None, None, None) == tp.OK
+    # The sharded list: no executors, a null item array, a null plan.
+    execs = (tp._ip * 1)(0)
+    assert lib.tprims_b200_contract_batched_sharded(None, 0, 0, None) == tp.ERR_INVALID_ARGUMENT
+    assert lib.tprims_b200_contract_batched_sharded(execs, 1, 2, None) == tp.ERR_INVALID_ARGUMENT
+    items = (tp.BatchItem * 1)()
+    assert lib.tprims_b200_contract_batched_sharded(execs, 1, 1, items) == tp.ERR_INVALID_ARGUMENT
+    assert lib.tprims_b200_balance(2, None, None, 1, None, None) == tp.ERR_INVALID_ARGUMENT

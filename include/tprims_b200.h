@@ -228,6 +228,12 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_save_tuning(TAPP_executor exec, const char* path);
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_load_tuning(TAPP_executor exec, const char* path);
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_clear_tuning(TAPP_executor exec);
+/* Checks a cache file without an executor (no GPU needed): the header's SM
+   count and device name, and the number of single-contraction and list
+   entries; a malformed file is INVALID_ARGUMENT, another version UNSUPPORTED.
+   Any out-parameter may be NULL. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_tuning_file_info(const char* path, int* sms, char* device,
+                                                          size_t device_len, int* singles, int* lists);
 TPRIMS_B200_EXPORT size_t tprims_b200_executor_tuning(TAPP_executor exec, char* buf, size_t maxlen);
 /* Number of device allocations the library has made in this process (every
    cudaMalloc of executors, workspaces, scatter vectors, grouped-list

@@ -196,18 +196,17 @@ std::string tuning_text(const Executor& ex) {
   return o.str();
 }
 
-void load_tuning_text(Executor& ex, const std::string& text) {
+TuningFile parse_tuning_text(const std::string& text) {
   std::istringstream in(text);
   std::string line;
   if (!std::getline(in, line)) throw Error(ERR_INVALID_ARGUMENT, "tuning cache: empty file");
   std::istringstream h(line);
-  std::string magic, dev;
-  int version = 0, sms = 0;
-  if (!(h >> magic >> version >> sms >> dev) || magic != "tprims-b200-tune")
+  std::string magic;
+  int version = 0;
+  TuningFile tf;
+  if (!(h >> magic >> version >> tf.sms >> tf.device) || magic != "tprims-b200-tune")
     throw Error(ERR_INVALID_ARGUMENT, "tuning cache: not a tprims-b200-tune file");
   if (version != 1) throw Error(ERR_UNSUPPORTED, "tuning cache: version " + std::to_string(version) + " (expected 1)");
-  const bool same_device = sms == ex.num_sms && dev == device_tag(ex);
-  std::map<std::string, TuneEntry> singles, lists;
   int lineno = 1;
   while (std::getline(in, line)) {
     ++lineno;
@@ -220,7 +219,7 @@ void load_tuning_text(Executor& ex, const std::string& text) {
     if (ok && kind == "single") {
       ok = static_cast<bool>(f >> e.choice.kernel >> e.choice.splits >> e.choice.chunk >> tiny >> tuned >> e.ms >>
                              e.tried);
-      ok = ok && (tiny != 0 || (e.choice.kernel >= 1 && e.choice.kernel <= dev::PLAIN_C64_DMMA_128x32)) &&
+      ok = ok && (tiny != 0 || (e.choice.kernel >= 1 && e.choice.kernel <= dev::PLAIN_LAST)) &&
            e.choice.splits >= 1 && e.choice.splits <= 64 && e.choice.chunk >= 0 &&
            (e.choice.splits == 1 || e.choice.chunk > 0);
     } else if (ok && kind == "list") {
@@ -233,11 +232,16 @@ void load_tuning_text(Executor& ex, const std::string& text) {
     if (!ok || (f >> extra)) throw Error(ERR_INVALID_ARGUMENT, "tuning cache: malformed line " + std::to_string(lineno));
     e.choice.tiny = tiny != 0;
     e.tuned = tuned != 0;
-    (kind == "single" ? singles : lists)[sig] = e;
+    (kind == "single" ? tf.singles : tf.lists)[sig] = e;
   }
-  if (!same_device) return;  // valid file, but measured on another kind of device
-  for (auto& kv : singles) ex.tune[kv.first] = kv.second;
-  for (auto& kv : lists) ex.list_tune[kv.first] = kv.second;
+  return tf;
+}
+
+void load_tuning_text(Executor& ex, const std::string& text) {
+  const TuningFile tf = parse_tuning_text(text);  // all-or-nothing: a malformed file adds nothing
+  if (tf.sms != ex.num_sms || tf.device != device_tag(ex)) return;  // measured on another kind of device
+  for (auto& kv : tf.singles) ex.tune[kv.first] = kv.second;
+  for (auto& kv : tf.lists) ex.list_tune[kv.first] = kv.second;
 }
 
 std::string tuning_json(const Executor& ex) {

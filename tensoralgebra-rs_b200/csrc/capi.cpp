@@ -931,6 +931,29 @@ extern "C" TAPP_error tprims_b200_executor_load_tuning(TAPP_executor exec, const
   });
 }
 
+extern "C" TAPP_error tprims_b200_tuning_file_info(const char* path, int* sms, char* device, size_t device_len,
+                                                  int* singles, int* lists) {
+  return ffi([&] {
+    if (!path || !*path) throw Error(ERR_INVALID_ARGUMENT, "tuning cache path is null or empty");
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) throw Error(ERR_INVALID_ARGUMENT, std::string("cannot open tuning cache: ") + path);
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+    std::fclose(f);
+    const TuningFile tf = parse_tuning_text(text);
+    if (sms) *sms = tf.sms;
+    if (singles) *singles = (int)tf.singles.size();
+    if (lists) *lists = (int)tf.lists.size();
+    if (device && device_len > 0) {
+      const size_t k = std::min(tf.device.size(), device_len - 1);
+      std::memcpy(device, tf.device.data(), k);
+      device[k] = 0;
+    }
+  });
+}
+
 extern "C" TAPP_error tprims_b200_executor_clear_tuning(TAPP_executor exec) {
   return ffi([&] {
     Executor& ex = resolve_exec(exec)->get();

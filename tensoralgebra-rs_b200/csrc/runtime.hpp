@@ -245,6 +245,13 @@ constexpr int GROUP_POLICIES = 4;
 // another device kind are skipped; a malformed file is an error).
 std::string tuning_text(const Executor& ex);
 void load_tuning_text(Executor& ex, const std::string& text);
+// A parsed cache file: the header's SM count and device tag, and its entries.
+struct TuningFile {
+  int sms = 0;
+  std::string device;
+  std::map<std::string, TuneEntry> singles, lists;
+};
+TuningFile parse_tuning_text(const std::string& text);
 std::string tuning_json(const Executor& ex);
 std::string choice_name(const PlainChoice& c, int dtype);
 

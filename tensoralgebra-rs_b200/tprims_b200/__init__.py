@@ -75,7 +75,7 @@ ABI_SYMBOLS = [
     "tprims_b200_network_set_precision", "tprims_b200_network_set_autotune", "tprims_b200_network_workspace_size",
     "tprims_b200_network_report", "tprims_b200_network_execute", "tprims_b200_networks_execute",
     "tprims_b200_device_allocations", "tprims_b200_executor_inject_launch_failure", "tprims_b200_product_check_raw",
-    "tprims_b200_contract_batched_sharded", "tprims_b200_balance",
+    "tprims_b200_contract_batched_sharded", "tprims_b200_balance", "tprims_b200_tuning_file_info",
 ]
 
 _i64p = C.POINTER(C.c_int64)
@@ -142,6 +142,8 @@ lib.tprims_b200_product_set_autotune.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_save_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_load_tuning.argtypes = [_ip, C.c_char_p]
 lib.tprims_b200_executor_clear_tuning.argtypes = [_ip]
+lib.tprims_b200_tuning_file_info.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.c_char_p, C.c_size_t,
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int)]
 lib.tprims_b200_executor_tuning.argtypes = [_ip, C.c_char_p, C.c_size_t]
 lib.tprims_b200_executor_tuning.restype = C.c_size_t
 lib.tprims_b200_executor_inject_launch_failure.argtypes = [_ip, C.c_int]
@@ -901,6 +903,15 @@ def einsum(subscripts: str, *operands, exec_: Optional[Executor] = None, out=Non
     finally:
         net.close()
     return out
+
+
+def tuning_file_info(path: str) -> dict:
+    """Header and entry counts of an autotuner cache file (no GPU needed)."""
+    sms, singles, lists = C.c_int(0), C.c_int(0), C.c_int(0)
+    dev = C.create_string_buffer(256)
+    check(lib.tprims_b200_tuning_file_info(os.fsencode(path), C.byref(sms), dev, 256, C.byref(singles),
+                                           C.byref(lists)))
+    return {"sms": sms.value, "device": dev.value.decode(), "single": singles.value, "list": lists.value}
 
 
 def balance(costs, part_devices, homes=None):

@@ -463,3 +463,44 @@ def test_scatter_vectors_reproduce_the_contraction(tp, orc, seed):
     orc.label_contract(1.0, orc.View(A, a["ext"], a["str"], a["lab"], oa), orc.View(B, b["ext"], b["str"], b["lab"], ob),
                        0.0, None, orc.View(want, d["ext"], d["str"], d["lab"], od))
     np.testing.assert_allclose(D, want, rtol=1e-12, atol=1e-12)
+
+
+def test_tuning_file_format_is_checked_without_a_gpu(tp, tmp_path):
+    """The autotuner cache file (versioned text): header, single-contraction and
+    list entries; malformed lines and other versions are refused."""
+    sig = _gemm_product(tp, 64, 64, 64).report()["signature"] + ";plain;c=0"
+    good = tmp_path / "tune.txt"
+    good.write_text("tprims-b200-tune 1 148 NVIDIA_B200\n"
+                    f"single {sig} 3 1 0 0 1 0.0123 4\n"
+                    f"single {sig}-split 3 4 1024 0 1 0.5 7\n"
+                    "single tiny-signature 0 1 0 1 0 0 0\n"
+                    "\n"
+                    "list list-0123456789abcdef-n3 2 1 1.5 3\n")
+    assert tp.tuning_file_info(str(good)) == {"sms": 148, "device": "NVIDIA_B200", "single": 3, "list": 1}
+    bad_lines = [
+        "single sig 10 1 0 0 1 0.1 1",    # no kernel family 10
+        "single sig 3 2 0 0 1 0.1 1",     # split without a chunk
+        "single sig 3 65 64 0 1 0.1 1",   # more than 64 chunks
+        "single sig 3 1 0 0 1 0.1",       # a field short
+        "single sig 3 1 0 0 1 0.1 1 9",   # a field too many
+        "list sig 4 1 0.1 1",             # no list policy 4
+        "pair sig 1 1 0.1 1",             # unknown kind
+    ]
+    for i, line in enumerate(bad_lines):
+        p = tmp_path / f"bad{i}.txt"
+        p.write_text("tprims-b200-tune 1 148 NVIDIA_B200\n" + line + "\n")
+        with pytest.raises(tp.TprimsError) as ei:
+            tp.tuning_file_info(str(p))
+        assert ei.value.status == tp.ERR_INVALID_ARGUMENT and "line 2" in ei.value.message, line
+    other = tmp_path / "v2.txt"
+    other.write_text("tprims-b200-tune 2 148 NVIDIA_B200\n")
+    with pytest.raises(tp.TprimsError) as ei:
+        tp.tuning_file_info(str(other))
+    assert ei.value.status == tp.ERR_UNSUPPORTED
+    for text in ["", "something else 1 148 x\n"]:
+        p = tmp_path / "junk.txt"
+        p.write_text(text)
+        with pytest.raises(tp.TprimsError):
+            tp.tuning_file_info(str(p))
+    with pytest.raises(tp.TprimsError):
+        tp.tuning_file_info(str(tmp_path / "missing.txt"))

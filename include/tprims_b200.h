@@ -47,7 +47,18 @@ typedef int TAPP_prectype;
 typedef int TAPP_element_op;
 
 /* tapp/datatype.h */
-enum { TAPP_F32 = 0, TAPP_F64 = 1, TAPP_C32 = 2, TAPP_C64 = 3, TAPP_F16 = 4, TAPP_BF16 = 5 };
+enum {
+  TAPP_F32 = 0,
+  TAPP_F64 = 1,
+  TAPP_C32 = 2,
+  TAPP_C64 = 3,
+  TAPP_F16 = 4,
+  TAPP_BF16 = 5,
+  TAPP_FLOAT = TAPP_F32,
+  TAPP_DOUBLE = TAPP_F64,
+  TAPP_SCOMPLEX = TAPP_C32,
+  TAPP_DCOMPLEX = TAPP_C64
+};
 enum {
   TAPP_DEFAULT_PREC = -1,
   TAPP_F32F32_ACCUM_F32 = 0,
@@ -154,7 +165,7 @@ typedef struct DLManagedTensorVersioned {
 
 /* crates/tprims-capi/include/tprims/core.h: a borrowed operand, never freed here. */
 typedef struct { DLTensor* view; uint64_t flags; } tprims_tensor;
-TPRIMS_B200_EXPORT tprims_tensor tprims_tensor_borrow_versioned(DLManagedTensorVersioned* m); /* tensor.rs:26 */
+TPRIMS_B200_EXPORT tprims_tensor tprims_tensor_borrow_versioned(struct DLManagedTensorVersioned* m); /* tensor.rs:26 */
 TPRIMS_B200_EXPORT tprims_tensor tprims_tensor_borrow_raw(DLTensor* t, uint64_t flags);       /* tensor.rs:55 */
 TPRIMS_B200_EXPORT const char* tprims_last_error(void);                                      /* status.rs:168 */
 TPRIMS_B200_EXPORT uint32_t tprims_abi_version(void);                                        /* lib.rs:143 */
@@ -418,15 +429,18 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_vjp(TAPP_tensor_product plan, 
    A, B, C and D must be in the current device's memory (else
    TPRIMS_ERR_DEVICE). Runs on `stream` (a cudaStream_t as an integer; 0 = the
    legacy default stream) of the current device and returns after that stream
-   has drained.
+   has drained; a stream that has not drained within 60 s (it waits on an event
+   nobody records, say) gives TPRIMS_ERR_INTERNAL instead of blocking forever.
    Its scratch is one fixed 64 MiB device array inside this library, held on
    every GPU that loads the library until the process exits; a contraction
    that needs more (about M = N = K = 2048 at bf16x6 fits) is refused with
    TPRIMS_ERR_SHAPE before anything runs. The first call on a device looks
    the array's address up (this may load the library's device code), so make
-   it before any stream capture on that device. All calls share the array:
-   calls that overlap on one GPU, from two streams or two threads, race on it
-   and give wrong results. */
+   it before any stream capture on that device; the address is looked up
+   again when the device's current context changes (after a cudaDeviceReset),
+   but a reset while a call is in flight is not supported. All calls share
+   the array: calls that overlap on one GPU, from two streams or two threads,
+   race on it and give wrong results. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_execute_product_noalloc(TAPP_tensor_product plan, uintptr_t stream,
                                                                   const void* alpha, const void* A, const void* B,
                                                                   const void* beta, const void* C, void* D);

@@ -154,6 +154,20 @@ size_t plain_scratch(const PlainChoice& c, const Product& p) {
   return (size_t)c.splits * p.view.H * p.view.M * p.view.N * dtype_size(p.problem.dtype) + 256;
 }
 
+bool choice_fits(const PlainChoice& c, const Product& p) {
+  const int64_t M = p.view.M, N = p.view.N, K = p.view.K, H = p.view.H;
+  if (c.tiny) return dev::use_tiny_batched(M, N, K, H) && c.splits == 1;
+  static const int fams[4][3] = {{dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, 0},
+                                 {dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_F64_DMMA_32x32, dev::PLAIN_F64_DMMA_128x32},
+                                 {dev::PLAIN_C32_SIMT_64x64, 0, 0},
+                                 {dev::PLAIN_C64_DMMA_64x32, dev::PLAIN_C64_DMMA_32x32, dev::PLAIN_C64_DMMA_128x32}};
+  bool fam_ok = false;
+  for (int f : fams[(int)p.problem.dtype & 3]) fam_ok = fam_ok || (f != 0 && f == c.kernel);
+  if (!fam_ok || c.splits < 1) return false;
+  if (c.splits == 1) return c.chunk == 0 || c.chunk >= K;
+  return c.chunk > 0 && c.chunk % 64 == 0 && (K + c.chunk - 1) / c.chunk == c.splits;
+}
+
 int grouped_family(const Product& p, int policy) {
   if (p.kernel_pin) return p.kernel_pin;
   const int dt = (int)p.problem.dtype;

@@ -11,8 +11,11 @@
 // library holds it until the process exits. Every call shares it and it keeps
 // the last call's contents; calls whose work overlaps on the same GPU (from two
 // streams or two host threads) race on it and produce wrong results.
+#include <chrono>
+#include <cuda.h>
 #include <mutex>
 #include <string>
+#include <thread>
 
 #include "kernels.cuh"
 #include "runtime.hpp"
@@ -32,20 +35,47 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 // cudaGetSymbolAddress returns for the current device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
+// Upper bound of the wait for the caller's stream to drain (the executor's
+// default drain limit); a stream that has not drained by then is reported as
+// TPRIMS_ERR_INTERNAL instead of blocking the caller forever.
+constexpr int NOALLOC_DRAIN_LIMIT_S = 60;
+
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+CUcontext g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// The device address of the scratch array on `device` (the current device),
-// looked up once per device. cudaGetSymbolAddress may load this library's
-// module on the device the first time, which is why the first call on a
-// device should not happen during a stream capture.
+// The current context through the runtime's driver entry point (no link
+// against libcuda); null when it cannot be queried.
+CUcontext current_context() {
+  typedef CUresult (*GetCurrentFn)(CUcontext*);
+  static GetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<GetCurrentFn>(p);
+  });
+  CUcontext c = nullptr;
+  if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
+
+// The device address of the scratch array on `device` (the current device).
+// It is looked up once per device and context: cudaGetSymbolAddress may load
+// this library's module on the device the first time, which is why the first
+// call on a device should not happen during a stream capture. When the
+// current context is no longer the one the address came from (the caller
+// reset the device and a new primary context exists), it is looked up again.
 unsigned char* scratch_on(int device) {
   if (device < 0 || device >= NOALLOC_MAX_DEVICES)
     throw Error(ERR_DEVICE, "no-allocation entry point: device " + std::to_string(device) + " out of range");
+  const CUcontext ctx = current_context();
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
+  if (!g_noalloc_addr[device] || g_noalloc_ctx[device] != ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -54,8 +84,24 @@ unsigned char* scratch_on(int device) {
                                   cudaGetErrorString(e));
     }
     g_noalloc_addr[device] = p;
+    g_noalloc_ctx[device] = ctx;
   }
   return static_cast<unsigned char*>(g_noalloc_addr[device]);
+}
+
+// Waits for `stream` to drain, giving up after NOALLOC_DRAIN_LIMIT_S.
+void drain_bounded(cudaStream_t stream) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t q = cudaStreamQuery(stream);
+    if (q == cudaSuccess) return;
+    if (q != cudaErrorNotReady) check_cuda(q, "kernel execution");
+    const auto waited = std::chrono::steady_clock::now() - t0;
+    if (waited > std::chrono::seconds(NOALLOC_DRAIN_LIMIT_S))
+      throw Error(ERR_INTERNAL, "no-allocation entry point: the stream did not drain within " +
+                                    std::to_string(NOALLOC_DRAIN_LIMIT_S) + " s");
+    if (waited > std::chrono::microseconds(200)) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
 }
 
 bool on_device(const void* p, int device) {
@@ -152,10 +198,12 @@ void execute_split_noalloc(Product& pr, cudaStream_t stream, Scalar alpha, Scala
     check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, stream), "tcgen05 contraction launch");
   }
 
-  // Synchronous: read the status word back on the same stream and wait.
+  // Synchronous: wait (bounded) for the stream to drain, then read the status
+  // word back on the same, now idle, stream.
+  drain_bounded(stream);
   unsigned word = 0;
   check_cuda(cudaMemcpyAsync(&word, status, sizeof(word), cudaMemcpyDeviceToHost, stream), "status read");
-  check_cuda(cudaStreamSynchronize(stream), "kernel execution");
+  check_cuda(cudaStreamSynchronize(stream), "status read");
   if (word & dev::STATUS_WAIT_TIMEOUT)
     throw Error(ERR_INTERNAL, "a kernel gave up on a bounded wait (device status word " + std::to_string(word) + ")");
   if (word != 0) throw Error(ERR_INTERNAL, "a kernel reported device status word " + std::to_string(word));

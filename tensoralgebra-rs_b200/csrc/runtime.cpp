@@ -789,8 +789,13 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
       key = tune_key(pr, c_read);
       const auto hit = ex.tune.find(key);
       if (hit != ex.tune.end()) {
-        pc = hit->second.choice;
-        src = hit->second.tuned ? ChoiceSource::Cached : ChoiceSource::Model;
+        // A loaded entry that does not fit this product (a stale or edited
+        // file: another family's kernel, or K chunks that would skip part of
+        // K) keeps the model's choice.
+        if (choice_fits(hit->second.choice, pr)) {
+          pc = hit->second.choice;
+          src = hit->second.tuned ? ChoiceSource::Cached : ChoiceSource::Model;
+        }
       } else {
         tune = true;
       }

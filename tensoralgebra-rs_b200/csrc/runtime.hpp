@@ -237,6 +237,11 @@ std::vector<PlainChoice> plain_candidates(int dtype, int64_t M, int64_t N, int64
 PlainChoice model_choice(const Product& p, int num_sms);
 // Scratch bytes a plain choice needs (split-K partials).
 size_t plain_scratch(const PlainChoice& c, const Product& p);
+// Whether a choice (from a tuning-cache file, say) is valid for a product: a
+// family of the product's dtype, the tiny kernel only where it applies, and
+// split-K chunks in whole 64-deep blocks whose count is exactly `splits`
+// (so that every k is covered once).
+bool choice_fits(const PlainChoice& c, const Product& p);
 // Tile family of a grouped item under a list tile policy (0: model, 1: large
 // tiles, 2: small tiles, 3: tall 128 x 32 tiles for narrow f64/c64 outputs).
 int grouped_family(const Product& p, int policy);

@@ -9,7 +9,7 @@ replay draws seeded inputs of these shapes.
 The reference tree is read in place here; the fixture is what travels to the
 machines that run the GPU tests and bench.py (--config corpus).
 
-Run: python tests/golden/make_corpus.py [corpus-dir]
+Run: python tests/golden/make_corpus.py <reference-root>/benchmarks/benchmarks/tprims/corpus
 """
 import glob
 import json
@@ -17,11 +17,12 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT = "/root/reference/benchmarks/benchmarks/tprims/corpus"
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else DEFAULT
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_corpus.py <reference-root>/benchmarks/benchmarks/tprims/corpus")
+    src = sys.argv[1]
     out = {"source": "benchmarks/benchmarks/tprims/corpus/*.json of the reference", "files": [], "entries": []}
     for path in sorted(glob.glob(os.path.join(src, "*.json"))):
         with open(path) as f:

@@ -30,6 +30,27 @@ def test_library_exports_every_declared_symbol(tp):
     assert set(tp.ABI_SYMBOLS) == decl
 
 
+def test_header_matches_the_reference_headers_as_the_compiler_sees_them():
+    """Every prototype (types after typedefs, parameter names dropped), enum
+    value, status code and DLPack struct size of the reference's pinned
+    headers (crates/tprims-capi/include/tapp.h, tprims/tprims.h; fixture
+    tests/golden/tapp_abi.json by tests/golden/make_abi_golden.py) is the same
+    in include/tprims_b200.h, compiled by gcc."""
+    import sys
+
+    sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+    from abi_extract import extract
+
+    ref = json.load(open(os.path.join(REPO, "tests", "golden", "tapp_abi.json")))
+    hdr = os.path.join(REPO, "include", "tprims_b200.h")
+    ours = extract([os.path.join(REPO, "include")], ["tprims_b200.h"], [hdr])
+    assert len(ref["prototypes"]) >= 30 and len(ref["values"]) >= 30
+    for name, proto in ref["prototypes"].items():
+        assert ours["prototypes"].get(name) == proto, (name, proto, ours["prototypes"].get(name))
+    for name, value in ref["values"].items():
+        assert ours["values"].get(name) == value, (name, value, ours["values"].get(name))
+
+
 def test_identity_queries(tp):
     assert tp.lib.tprims_abi_version() == 100
     assert tp.lib.tprims_has_part(b"core") == 1 and tp.lib.tprims_has_part(b"tapp") == 1

@@ -323,6 +323,85 @@ def corpus_case(tp, torch, e, seed):
     return plan, bufs, ptrs
 
 
+TCCG_PUBLISHED = {"f32": 74.8, "f64": 44.7, "c32": 121.0, "c64": 62.0}  # results.md:90-93, GF/s, 1 core
+
+
+def tccg_cases():
+    """The TCCG corpus of the reference's harness (tests/golden/tccg.json)."""
+    with open(os.path.join(REPO, "tests", "golden", "tccg.json")) as f:
+        return json.load(f)["cases"]
+
+
+def tccg_size_mib(key):
+    with open(os.path.join(REPO, "tests", "golden", "tccg.json")) as f:
+        return json.load(f)["sizes_mib"][key]
+
+
+def tccg_layout(labels, ext):
+    dims = [ext[ch] for ch in labels]
+    st, acc = [], 1
+    for d in dims:
+        st.append(acc)
+        acc *= d
+    return dims, st, acc
+
+
+def tccg_case(tp, torch, case, dt, size, seed):
+    """Plan (Problem::from_labels, column-major operands) and seeded device
+    operands of one TCCG case at the sizing `size` ('tccg64' or 'small');
+    returns (plan, tensors a, b, c, MAC count)."""
+    code, npdt = CORPUS_DT[dt]
+    ext = case["extents"][size]
+    lab = lambda s: [ord(ch) for ch in s]
+    lay = lambda s: tp.LayoutSpec(*tccg_layout(s, ext)[:2])
+    plan = tp.Plan(tp.Problem.from_labels(code, tp.OperandSpec(lay(case["a"])), tp.OperandSpec(lay(case["b"])),
+                                          tp.OperandSpec(lay(case["c"])), lab(case["a"]), lab(case["b"]),
+                                          lab(case["c"])))
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    real = torch.float32 if dt in ("f32", "c32") else torch.float64
+    t = {}
+    for k in ("a", "b"):
+        n = tccg_layout(case[k], ext)[2]
+        x = torch.rand(n, dtype=real, device="cuda", generator=gen) * 2 - 1
+        if dt[0] == "c":
+            x = torch.complex(x, torch.rand(n, dtype=real, device="cuda", generator=gen) * 2 - 1)
+        t[k] = x
+    t["c"] = torch.zeros(tccg_layout(case["c"], ext)[2], dtype=t["a"].dtype, device="cuda")
+    macs = 1
+    for v in ext.values():
+        macs *= v
+    return plan, t, macs
+
+
+def tccg_sampled_error(torch, case, dt, t, size, n_samples=32, seed=0):
+    """Relative Frobenius error of n sampled outputs of a TCCG case against
+    float64 (complex128) sums over its contracted labels, on the device."""
+    ext = case["extents"][size]
+    la, lb, lc = case["a"], case["b"], case["c"]
+    st = {k: dict(zip(case[k], tccg_layout(case[k], ext)[1])) for k in ("a", "b", "c")}
+    contracted = [ch for ch in la if ch in lb and ch not in lc]
+    ca = np.zeros(1, dtype=np.int64)
+    cb = np.zeros(1, dtype=np.int64)
+    for ch in contracted:
+        r = np.arange(ext[ch], dtype=np.int64)
+        ca = (ca[:, None] + r[None, :] * st["a"][ch]).ravel()
+        cb = (cb[:, None] + r[None, :] * st["b"][ch]).ravel()
+    g = np.random.default_rng(seed)
+    idx = {ch: g.integers(0, ext[ch], size=n_samples) for ch in lc}
+    off = {k: np.zeros(n_samples, dtype=np.int64) for k in ("a", "b", "c")}
+    for ch in lc:
+        for k in ("a", "b", "c"):
+            if ch in case[k]:
+                off[k] += idx[ch] * st[k][ch]
+    wide = torch.complex128 if dt[0] == "c" else torch.float64
+    av = torch.take(t["a"], torch.from_numpy(off["a"][:, None] + ca[None, :]).cuda()).to(wide)
+    bv = torch.take(t["b"], torch.from_numpy(off["b"][:, None] + cb[None, :]).cuda()).to(wide)
+    ref = (av * bv).sum(dim=1)
+    got = torch.take(t["c"], torch.from_numpy(off["c"]).cuda()).to(wide)
+    den = torch.linalg.norm(ref).item()
+    return torch.linalg.norm(got - ref).item() / den if den > 0 else torch.linalg.norm(got - ref).item()
+
+
 def corpus_sampled_error(torch, e, bufs, n_samples=64, seed=0):
     """Relative Frobenius error of n sampled outputs against float64 (complex128)
     sums over the contracted index set, computed on the device."""
@@ -369,10 +448,39 @@ def corpus_sampled_error(torch, e, bufs, n_samples=64, seed=0):
     return num / den if den > 0 else num
 
 
+def cpu_median_rate(run_once, flop, target_s):
+    """Median FLOP/s of repeated runs of `run_once` (returns seconds) filling
+    about `target_s` seconds, at least three runs."""
+    rates = []
+    t_end = time.perf_counter() + target_s
+    while len(rates) < 3 or (time.perf_counter() < t_end and len(rates) < 50):
+        rates.append(flop / run_once())
+    return float(np.median(rates))
+
+
+def cpu_pair(make_run, flop, sample, target_s=2.0):
+    """The restated packed CPU driver on a bounded sample, timed at one thread
+    and at every host thread in the same session (the reference measures each
+    case at one and N threads, PERFORMANCE_TIPS.md:247)."""
+    n = os.cpu_count() or 1
+    one = cpu_median_rate(lambda: make_run(1), flop, target_s)
+    full = cpu_median_rate(lambda: make_run(n), flop, target_s)
+    return {"value": full / 1e12, "unit": "TFLOP/s", "cores": n, "kind": "port", "threads_1": one / 1e12,
+            "threads_all": full / 1e12, "sample": sample}
+
+
+def timed_call(fn):
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
+
+
 def run_config(args, tp, torch, ex):
-    """Timing lines for the other configurations (parity-test cases in the test
-    suite): C1 (f64, extents 24, beta 0.5), C3 (c64 batched, conj(A), batch
-    innermost) and C5 (f64 forward + Plan::vjp with a repeated index)."""
+    """Timing record of one of the other configurations (each also a parity-test
+    case): C1 (f64, extents 24, beta 0.5), C3 (c64 batched, conj(A), batch
+    innermost), C4 / C4c (the uneven list of environment updates, f64 / c64),
+    C5 (f64 forward + Plan::vjp with a repeated index), the reference's corpus,
+    or a plain square GEMM. Returns the record (None when it was printed)."""
     import oracle
 
     def col_major(ext):
@@ -428,8 +536,7 @@ def run_config(args, tp, torch, ex):
         out["plain"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms_per_step": ms, "kernels": kt,
                         "family": plan.report()["family"], "pipe_peak_tflops": peak,
                         "frac": flop / (ms * 1e-3) / 1e12 / peak}
-        print(json.dumps(out), flush=True)
-        return
+        return out
     if cfg == "corpus":
         # The reference's dot_general corpus replayed through Problem::from_dot_general
         # and execute_into (plain precision), seeded inputs; each entry timed alone.
@@ -454,24 +561,68 @@ def run_config(args, tp, torch, ex):
         out["call_weighted_tflops"] = tot_f / tot_t / 1e12
         out["worst_rel_err"] = max(r["rel_err_sampled"] for r in rows)
         out["entries"] = rows
-        print(json.dumps(out), flush=True)
-        return
+        return out
+    if cfg == "tccg":
+        # The reference's TCCG corpus (49 contractions) at its published nominal
+        # size, plain precision, each case and dtype timed alone; GF/s with 2
+        # flops per real MAC and 8 per complex MAC, summarised per dtype
+        # (min / median / geomean / max) beside the reference's single-core
+        # numbers (docs/archive/tensorprimitives/results.md:90-93).
+        rows = []
+        for dt in ("f32", "f64", "c32", "c64"):
+            for i, case in enumerate(tccg_cases()):
+                plan, t, macs = tccg_case(tp, torch, case, dt, args.tccg_size, 20261203 + 9000 + i)
+                fn = lambda: plan.execute_into(ex, 1.0, t["a"].data_ptr(), t["b"].data_ptr(), t["c"].data_ptr())
+                flop = (8.0 if dt[0] == "c" else 2.0) * macs
+                reps = max(3, min(args.steps, int(5e11 // max(flop, 1.0))))
+                ms, _ = timed(fn, reps, 2)
+                err = tccg_sampled_error(torch, case, dt, t, args.tccg_size, seed=i)
+                rows.append({"name": case["name"], "group": case["group"], "dtype": dt, "ms": ms,
+                             "gflops": flop / (ms * 1e-3) / 1e9, "rel_err_sampled": err,
+                             "family": plan.report()["family"]})
+                del t, plan
+            torch.cuda.empty_cache()
+        out["workload"] = (f"TCCG corpus, {len(tccg_cases())} contractions (tests/golden/tccg.json), nominal "
+                           f"{tccg_size_mib(args.tccg_size)} MiB tensors, column-major, plain precision, seeded "
+                           "uniform inputs")
+        summary = {}
+        for dt in ("f32", "f64", "c32", "c64"):
+            g = np.array([r["gflops"] for r in rows if r["dtype"] == dt])
+            summary[dt] = {"min": float(g.min()), "median": float(np.median(g)),
+                           "geomean": float(np.exp(np.log(g).mean())), "max": float(g.max()),
+                           "reference_1core_median": TCCG_PUBLISHED[dt]}
+        out["gflops_by_dtype"] = summary
+        out["worst_rel_err"] = max(r["rel_err_sampled"] for r in rows)
+        out["entries"] = rows
+        return out
     # Pipe peaks measured on this GPU (register-only probe kernels), and the
     # INT8 tensor peak taken as twice the measured dense BF16 burst peak.
     peaks, peak_src = measured_peaks()
-    pipe = {"fp64_dmma": ex.probe_peak(0), "fp32_ffma": ex.probe_peak(1),
-            "int8_tcgen05": 2.0 * peaks["bf16_tflops"]}
-    out["pipe_peaks_tflops"] = dict(pipe, source="probe kernels (fp64/fp32, measured here); int8 = 2 x " + peak_src)
+    pipe = {"fp64_dmma": ex.probe_peak(0), "fp32_ffma": ex.probe_peak(1), "int8_tcgen05": ex.probe_peak(2),
+            "bf16_tcgen05": ex.probe_peak(3)}
+    out["pipe_peaks_tflops"] = dict(pipe, source="probe kernels measured here (register-only DMMA / FFMA chains; "
+                                                 "dense 128x256 tcgen05.mma from shared memory into TMEM)",
+                                    bf16_measured_peaks_file=peaks.get("bf16_tflops"), bf16_file_source=peak_src)
+    want_cpu = not getattr(args, "no_cpu_baseline", False)
 
-    def roofline(entry, kernel, pipe_flop_per_step, peak_name):
-        """Pipe fraction of the dominant kernel: executed pipe flops / its CUDA-event time / measured peak."""
+    def dmma_pipe_flops(family, useful):
+        """FP64 pipe flops the family executes for `useful` flops (8 per complex
+        MAC): 3m runs three real products per complex MAC, planar four."""
+        return useful * 0.75 if ".3m." in family else useful
+
+    def roofline(entry, kernel, pipe_flop_per_step, peak_name, steps=None):
+        """Pipe fraction of the dominant kernel: executed pipe flops / its CUDA-event time / measured peak,
+        with the kernel's DRAM bytes per launch from the committed ncu summaries when one covers it."""
         kt = entry["kernels"].get(kernel)
         if not kt:
             return
-        k_ms = kt["ms"] / kt["launches"] * (kt["launches"] / args.steps)
+        k_ms = kt["ms"] / (steps or args.steps)
+        traffic, src = profiled_traffic(kernel)
         entry["roofline"] = {"kernel": kernel, "pipe": peak_name, "achieved": pipe_flop_per_step / (k_ms * 1e-3) / 1e12,
                              "peak": pipe[peak_name], "unit": "TFLOP/s",
-                             "frac": pipe_flop_per_step / (k_ms * 1e-3) / 1e12 / pipe[peak_name]}
+                             "frac": pipe_flop_per_step / (k_ms * 1e-3) / 1e12 / pipe[peak_name],
+                             "kernel_ms_per_step": k_ms, "launches_per_step": kt["launches"] / (steps or args.steps),
+                             "traffic": traffic, "traffic_source": src}
 
     def ozaki_products(entry):
         fam = entry.get("family", "")
@@ -508,7 +659,14 @@ def run_config(args, tp, torch, ex):
             if code:
                 roofline(out[scheme], "ozaki_gemm", ozaki_products(out[scheme]) * flop, "int8_tcgen05")
             else:
-                roofline(out[scheme], out[scheme]["family"], flop, "fp64_dmma")
+                roofline(out[scheme], out[scheme]["family"], dmma_pipe_flops(out[scheme]["family"], flop),
+                         "fp64_dmma")
+        if want_cpu:
+            dc = np.zeros(e ** 4)
+            cv = [oracle.View(x, *sp) for x, sp in zip((a, b, c, dc), specs)]
+            out["cpu_baseline"] = cpu_pair(
+                lambda t: timed_call(lambda: oracle.packed_contract(1.0, cv[0], cv[1], 0.5, cv[2], cv[3], nthreads=t)),
+                flop, "restated packed CPU driver (oracle/oracle.c), the whole C1 contraction (separate C)")
     elif cfg == "c3":
         nb, n = 64, 384
         ext = [nb, n, n]
@@ -548,7 +706,18 @@ def run_config(args, tp, torch, ex):
                 emb = 2.0 * (2 * n) * n * (2 * n) * nb
                 roofline(out[scheme], "ozaki_gemm", ozaki_products(out[scheme]) * emb, "int8_tcgen05")
             else:
-                roofline(out[scheme], out[scheme]["family"], flop, "fp64_dmma")
+                roofline(out[scheme], out[scheme]["family"], dmma_pipe_flops(out[scheme]["family"], flop),
+                         "fp64_dmma")
+        if want_cpu:
+            nbs = 8  # batch entries 0..7 of 64: the same strides, an eighth of the work
+            es = [nbs, n, n]
+            dc = np.zeros(nb * n * n, dtype=np.complex128)
+            va = oracle.View(a, es, cm, [9, 2, 0], conj=True)
+            vb, vd = oracle.View(b, es, cm, [9, 2, 1]), oracle.View(dc, es, cm, [9, 0, 1])
+            out["cpu_baseline"] = cpu_pair(
+                lambda t: timed_call(lambda: oracle.packed_contract(1.0, va, vb, 0.0, None, vd, nthreads=t)),
+                8.0 * nbs * n ** 3, f"restated packed CPU driver (oracle/oracle.c, planar c64), batch entries "
+                                    f"0..{nbs - 1} of {nb} in the C3 layout")
     elif cfg in ("c4", "c4c"):
         dt = "complex128" if cfg == "c4c" else "float64"
         tdt = tp.C64 if cfg == "c4c" else tp.F64
@@ -650,6 +819,24 @@ def run_config(args, tp, torch, ex):
         for n in nets:
             n.close()
         del net_out
+        if want_cpu:
+            sample = items[:16]
+
+            def cpu_list(t):
+                for it in sample:
+                    ext = c4_extents(it)
+                    bufs = {k: it[k] for k in ("E", "Ma", "W", "Mb")}
+                    for xa, la, xb, lb, xd, ld, cj in C4_STEPS:
+                        ed_ = [ext[x] for x in ld]
+                        bufs[xd] = np.zeros(int(np.prod(ed_)), dtype=bufs["E"].dtype)
+                        va = oracle.View(bufs[xa], [ext[x] for x in la], col_major([ext[x] for x in la]), la)
+                        vb = oracle.View(bufs[xb], [ext[x] for x in lb], col_major([ext[x] for x in lb]), lb, conj=cj)
+                        oracle.packed_contract(1.0, va, vb, 0.0, None, oracle.View(bufs[xd], ed_, col_major(ed_), ld),
+                                               nthreads=t)
+
+            out["cpu_baseline"] = cpu_pair(lambda t: timed_call(lambda: cpu_list(t)), c4_flops(sample, cfg == "c4c"),
+                                           f"restated packed CPU driver (oracle/oracle.c), items 0..15 of "
+                                           f"{len(items)}, three binary steps each, one packed call per step")
     elif cfg == "c5":
         i, k, l = 512, 128, 256
         ea, eb, ed = [i, k, k, l], [l, i, k], [i, i]
@@ -678,7 +865,38 @@ def run_config(args, tp, torch, ex):
                                     "achieved": 3 * flop / (gemm_ms * 1e-3) / 1e12, "peak": pipe["fp64_dmma"],
                                     "unit": "TFLOP/s",
                                     "frac": 3 * flop / (gemm_ms * 1e-3) / 1e12 / pipe["fp64_dmma"]}
-    print(json.dumps(out), flush=True)
+        fill = {n_: v for n_, v in kt.items() if n_ == "zero_fill"}
+        if fill:
+            f_ms = sum(v["ms"] for v in fill.values()) / args.steps
+            out["plain"]["dA_zero_fill"] = {"ms_per_step": f_ms, "bytes": 8 * i * k * k * l,
+                                            "gbs": 8 * i * k * k * l / (f_ms * 1e-3) / 1e9, "hbm_peak_gbs":
+                                            peaks["hbm_gbs"]}
+        del A, B, dA, dB, dD, D
+        torch.cuda.empty_cache()
+        if want_cpu:
+            # The packed driver reads only A's diagonal (through the scatter
+            # vectors), so the CPU runs on a dense copy of it, Ad[i,k,l] =
+            # A[i,k,k,l], with l restricted to 0..63: the three contractions of
+            # the step (forward, dA's diagonal, dB) on a quarter of the work.
+            ls = 64
+            rg = np.random.default_rng(20261203 + 5000 + 10)
+            ad, bh, ddh = rg.standard_normal(i * k * ls), rg.standard_normal(ls * i * k), rg.standard_normal(i * i)
+            out_d, out_da, out_db = np.zeros(i * i), np.zeros(i * k * ls), np.zeros(ls * i * k)
+            V = oracle.View
+            eadd, ebs = [i, k, ls], [ls, i, k]
+
+            def cpu_step(t):
+                oracle.packed_contract(1.0, V(ad, eadd, col_major(eadd), [0, 2, 3]), V(bh, ebs, col_major(ebs), [3, 1, 2]),
+                                       0.0, None, V(out_d, ed, col_major(ed), [0, 1]), nthreads=t)
+                oracle.packed_contract(1.0, V(ddh, ed, col_major(ed), [0, 1]), V(bh, ebs, col_major(ebs), [3, 1, 2]),
+                                       0.0, None, V(out_da, eadd, col_major(eadd), [0, 2, 3]), nthreads=t)
+                oracle.packed_contract(1.0, V(ad, eadd, col_major(eadd), [0, 2, 3]), V(ddh, ed, col_major(ed), [0, 1]),
+                                       0.0, None, V(out_db, ebs, col_major(ebs), [3, 1, 2]), nthreads=t)
+
+            out["cpu_baseline"] = cpu_pair(lambda t: timed_call(lambda: cpu_step(t)), 3 * 2.0 * i * i * k * ls,
+                                           "restated packed CPU driver (oracle/oracle.c): forward, dA diagonal and dB "
+                                           "of C5 with l in 0..63 of 256, A's diagonal as a dense copy")
+    return out
 
 
 def main():
@@ -690,12 +908,15 @@ def main():
     ap.add_argument("--scheme", default="bf16x6", choices=list(SCHEMES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="time the metric's workload only (no C1, C3-C5 records)")
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
     ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
     ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus", "gemm"],
+    ap.add_argument("--tccg-size", default="tccg64", choices=["tccg64", "small"], help="sizing of --config tccg")
+    ap.add_argument("--config", default="c2",
+                    choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus", "gemm", "tccg"],
                     help="c2 is the metric's workload; c1/c3/c5 print timing lines of the other configurations")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -721,7 +942,9 @@ def main():
         ex = tp.Executor(device=local)
         ex.set_sync(False)
         ex.set_profiling(True)
-        run_config(args, tp, torch, ex)
+        out = run_config(args, tp, torch, ex)
+        if out is not None:
+            print(json.dumps(out), flush=True)
         return
 
     a_h, b_h = host_inputs()
@@ -835,9 +1058,34 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, s, runs = cpu_rate(threads, 12.0)
+        rate1, s1, runs1 = cpu_rate(1, 6.0)
         cpu = {"value": rate / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": f"restated packed CPU driver (oracle/oracle.c, AVX-512 48x8 f32 micro-kernel), n2 in "
-                         f"[0,{s}) of 64 (M=4096, N={E * s}, K=4096), median of {runs} runs"}
+                         f"[0,{s}) of 64 (M=4096, N={E * s}, K=4096), median of {runs} runs",
+               "threads_1": rate1 / 1e12, "threads_all": rate / 1e12,
+               "sample_threads_1": f"n2 in [0,{s1}) of 64, median of {runs1} runs, 1 thread"}
+
+    # The other configurations (parity-test cases), each with its own timing,
+    # error, dominant-kernel roofline and CPU baseline at 1 and all threads.
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        import copy
+
+        configs = {}
+        cex = tp.Executor(device=local)
+        cex.set_sync(False)
+        cex.set_profiling(True)
+        for cfg, cap in (("c1", 50), ("c3", 10), ("c4", 5), ("c4c", 5), ("c5", 5)):
+            a2 = copy.copy(args)
+            a2.config, a2.steps, a2.warmup = cfg, min(args.steps, cap), 3
+            t_cfg = time.perf_counter()
+            try:
+                configs[cfg] = run_config(a2, tp, torch, cex)
+            except Exception as err:  # a config that fails is recorded, the headline line still prints
+                configs[cfg] = {"error": f"{type(err).__name__}: {err}"}
+            configs[cfg]["wall_s"] = time.perf_counter() - t_cfg
+            torch.cuda.empty_cache()
+        cex.close()
 
     if world > 1:
         dist.destroy_process_group()
@@ -863,6 +1111,8 @@ def main():
     }
     if head != "plain" and "plain" in others:
         line["speedup_vs_plain"] = value / others["plain"]["tflops"]
+    if configs is not None:
+        line["configs"] = configs
     print(json.dumps(line), flush=True)
 
 

@@ -227,8 +227,10 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_inject_launch_failure(TAPP_ex
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor exec, uint64_t limit_ns);
 /* Measured pipe peak for roofline denominators (diagnostics): which = 0 runs
    the FP64 DMMA pipe (mma.sync m8n8k4), 1 the FP32 FFMA pipe, with
-   register-only operation chains on every SM; *tflops receives the best of a
-   few timed launches (CUDA events on the executor's stream). */
+   register-only operation chains on every SM; 2 the INT8 and 3 the BF16
+   tensor pipe (dense 128 x 256 tcgen05.mma products from shared memory into
+   TMEM, one CTA per SM); *tflops receives the best of a few timed launches
+   (CUDA events on the executor's stream), in TFLOP/s or TOP/s. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int which, double* tflops);
 /* The executor's autotuner cache, persisted as a versioned text file (the
    reference has no tuning state to persist; this is the build's only

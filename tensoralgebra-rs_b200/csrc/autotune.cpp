@@ -53,6 +53,13 @@ std::string device_tag(const Executor& ex) {
   return n;
 }
 
+// The single-launch tile families of each dtype (direct, then packed).
+const int kFamilies[4][4] = {
+    {dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, dev::PLAIN_F32_PACKED_128x128, 0},
+    {dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_F64_DMMA_32x32, dev::PLAIN_F64_DMMA_128x32, dev::PLAIN_F64_PACKED_64x64},
+    {dev::PLAIN_C32_SIMT_64x64, dev::PLAIN_C32_PACKED_1M_64x128, 0, 0},
+    {dev::PLAIN_C64_DMMA_64x32, dev::PLAIN_C64_DMMA_32x32, dev::PLAIN_C64_DMMA_128x32, dev::PLAIN_C64_PACKED_3M_64x32}};
+
 }  // namespace
 
 std::string problem_signature(const Product& p) {
@@ -96,12 +103,8 @@ std::vector<PlainChoice> plain_candidates(int dtype, int64_t M, int64_t N, int64
     t.tiny = true;
     add(t);
   }
-  static const int fams[4][3] = {{dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, 0},
-                                 {dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_F64_DMMA_32x32, dev::PLAIN_F64_DMMA_128x32},
-                                 {dev::PLAIN_C32_SIMT_64x64, 0, 0},
-                                 {dev::PLAIN_C64_DMMA_64x32, dev::PLAIN_C64_DMMA_32x32, dev::PLAIN_C64_DMMA_128x32}};
-  for (int f : fams[dtype & 3]) {
-    if (!f) continue;
+  for (int f : kFamilies[dtype & 3]) {
+    if (!f || (dev::is_packed_kernel(f) && !dev::packed_fits(f, M, N, K, H))) continue;
     PlainChoice c;
     c.kernel = f;
     add(c);
@@ -150,26 +153,29 @@ PlainChoice model_choice(const Product& p, int num_sms) {
 }
 
 size_t plain_scratch(const PlainChoice& c, const Product& p) {
-  if (c.tiny || c.splits <= 1) return 0;
-  return (size_t)c.splits * p.view.H * p.view.M * p.view.N * dtype_size(p.problem.dtype) + 256;
+  if (c.tiny) return 0;
+  size_t s = 0;
+  if (dev::is_packed_kernel(c.kernel))
+    s += dev::packed_workspace_bytes(dev::packed_layout(c.kernel, p.view.M, p.view.N, p.view.K, p.view.H)) + 512;
+  if (c.splits > 1) s += (size_t)c.splits * p.view.H * p.view.M * p.view.N * dtype_size(p.problem.dtype) + 256;
+  return s;
 }
 
 bool choice_fits(const PlainChoice& c, const Product& p) {
   const int64_t M = p.view.M, N = p.view.N, K = p.view.K, H = p.view.H;
   if (c.tiny) return dev::use_tiny_batched(M, N, K, H) && c.splits == 1;
-  static const int fams[4][3] = {{dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, 0},
-                                 {dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_F64_DMMA_32x32, dev::PLAIN_F64_DMMA_128x32},
-                                 {dev::PLAIN_C32_SIMT_64x64, 0, 0},
-                                 {dev::PLAIN_C64_DMMA_64x32, dev::PLAIN_C64_DMMA_32x32, dev::PLAIN_C64_DMMA_128x32}};
   bool fam_ok = false;
-  for (int f : fams[(int)p.problem.dtype & 3]) fam_ok = fam_ok || (f != 0 && f == c.kernel);
+  for (int f : kFamilies[(int)p.problem.dtype & 3]) fam_ok = fam_ok || (f != 0 && f == c.kernel);
   if (!fam_ok || c.splits < 1) return false;
+  if (dev::is_packed_kernel(c.kernel) && !dev::packed_fits(c.kernel, M, N, K, H)) return false;
   if (c.splits == 1) return c.chunk == 0 || c.chunk >= K;
   return c.chunk > 0 && c.chunk % 64 == 0 && (K + c.chunk - 1) / c.chunk == c.splits;
 }
 
 int grouped_family(const Product& p, int policy) {
-  if (p.kernel_pin) return p.kernel_pin;
+  // A packed family pinned on the plan serves its single launches; inside a
+  // grouped list the item takes a direct family.
+  if (p.kernel_pin && !dev::is_packed_kernel(p.kernel_pin)) return p.kernel_pin;
   const int dt = (int)p.problem.dtype;
   static const int large[4] = {dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_C32_SIMT_64x64,
                                dev::PLAIN_C64_DMMA_64x32};

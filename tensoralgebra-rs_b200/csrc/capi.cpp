@@ -1030,7 +1030,9 @@ extern "C" TAPP_error tprims_b200_executor_selftest_wait(TAPP_executor exec, uin
 extern "C" TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int which, double* tflops) {
   return ffi([&] {
     if (!tflops) null_arg("tflops out-parameter");
-    if (which != 0 && which != 1) throw Error(ERR_INVALID_ARGUMENT, "probe must be 0 (FP64 DMMA) or 1 (FP32 FFMA)");
+    if (which < 0 || which > 3)
+      throw Error(ERR_INVALID_ARGUMENT,
+                  "probe must be 0 (FP64 DMMA), 1 (FP32 FFMA), 2 (INT8 tcgen05) or 3 (BF16 tcgen05)");
     Executor& ex = resolve_exec(exec)->get();
     std::lock_guard<std::mutex> lk(ex.mu);
     int prev = -1;
@@ -1046,12 +1048,17 @@ extern "C" TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int wh
     cudaEvent_t e0, e1;
     check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
-    const int blocks = ex.num_sms * (which == 0 ? 8 : 8);
-    const int iters = which == 0 ? 4096 : 65536;
+    const bool tc = which >= 2;
+    const int blocks = tc ? ex.num_sms : ex.num_sms * 8;
+    const int iters = which == 0 ? 4096 : (tc ? 20000 : 65536);
     double best = 0, flops = 0;
     for (int rep = 0; rep < 5; ++rep) {
       check_cuda(cudaEventRecord(e0, ex.stream), "cudaEventRecord");
-      check_cuda(dev::launch_probe(which, sink, blocks, iters, ex.stream, &flops), "probe launch");
+      if (tc)
+        check_cuda(dev::launch_tc_probe(which == 2 ? 1 : 0, blocks, iters, ex.status, ex.stream, &flops),
+                   "tensor probe launch");
+      else
+        check_cuda(dev::launch_probe(which, sink, blocks, iters, ex.stream, &flops), "probe launch");
       check_cuda(cudaEventRecord(e1, ex.stream), "cudaEventRecord");
       check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
       float ms = 0;
@@ -1060,6 +1067,7 @@ extern "C" TAPP_error tprims_b200_executor_probe_peak(TAPP_executor exec, int wh
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    finish(ex);  // a tensor probe that gave up on its bounded wait reports here
     *tflops = best;
   });
 }

@@ -777,5 +777,65 @@ cudaError_t launch_ozaki_gemm(const GemmArgs& g, const OzakiLayout& L, const voi
   return gemm_dispatch<false>(g, L, ap, bp, ea, eb, kb0, kb1, st);
 }
 
+namespace {
+
+// Tensor-pipe probe: one CTA per SM, one thread issuing `iters` dense
+// 128 x 256 tcgen05.mma products (kind::i8 with K = 32, or kind::f16 BF16
+// with K = 16) from one shared-memory operand pair into one TMEM accumulator,
+// then a commit and a bounded wait. No memory traffic beyond the CTA's own
+// shared memory: the measured rate is the pipe's.
+__global__ void __launch_bounds__(128, 1) tc_probe_kernel(int int8, int iters, unsigned* status) {
+  __shared__ __align__(1024) uint8_t ops[8192 + 16384];  // A: 128 rows x 64 B, B: 256 rows x 64 B
+  __shared__ uint64_t bar;
+  __shared__ uint32_t slot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < (8192 + 16384) / 16; i += 128) reinterpret_cast<uint4*>(ops)[i] = make_uint4(0, 0, 0, 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    tmem_alloc(&slot, 256);
+    tmem_relinquish();
+  }
+  if (tid == 32) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = slot;
+  if (tid == 0) {
+    const uint64_t ad = sdesc_sw64(smem_u32(ops)), bd = sdesc_sw64(smem_u32(ops + 8192));
+    const uint32_t idesc = int8 ? idesc_i8(128, 256) : ((1u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) |
+                                                         ((128u >> 4) << 24));
+    for (int it = 0; it < iters; ++it) {
+      const uint64_t k = (uint64_t)(2 * (it & 1));  // the two 32-byte K steps of the 64-byte rows
+      if (int8)
+        umma_i8(tmem, ad + k, bd + k, idesc, it > 0 ? 1u : 0u);
+      else
+        umma_bf16(tmem, ad + k, bd + k, idesc, it > 0 ? 1u : 0u);
+    }
+    umma_commit(&bar);
+    if (!mbar_wait(&bar, 0)) atomicOr(status, STATUS_WAIT_TIMEOUT);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_tc_probe(int int8, int blocks, int iters, unsigned* status, cudaStream_t st, double* ops) {
+  // Unused dynamic shared memory keeps one CTA per SM.
+  constexpr int kPad = 160 * 1024;
+  const cudaError_t e = cudaFuncSetAttribute(tc_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPad);
+  if (e != cudaSuccess) return e;
+  tc_probe_kernel<<<blocks, 128, kPad, st>>>(int8, iters, status);
+  *ops = (double)blocks * iters * 2.0 * 128 * 256 * (int8 ? 32 : 16);
+  return cudaGetLastError();
+}
+
 }  // namespace dev
 }  // namespace tprims

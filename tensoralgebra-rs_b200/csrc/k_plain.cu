@@ -1054,13 +1054,35 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
     case PLAIN_F64_DMMA_128x32: return "sm100.f64.dmma884.128x32x16";
     case PLAIN_C64_DMMA_128x32: return "sm100.c64.dmma884.planar.128x32x8";
+    case PLAIN_F32_PACKED_128x128: return "sm100.f32.simt.tma.packed.128x128x16";
+    case PLAIN_C32_PACKED_1M_64x128: return "sm100.c32.simt.tma.1m.64x128x16";
+    case PLAIN_F64_PACKED_64x64: return "sm100.f64.dmma884.tma.packed.64x64x16";
+    case PLAIN_C64_PACKED_3M_64x32: return "sm100.c64.dmma884.tma.3m.64x32x16";
   }
   return "auto";
 }
 
+// Whether the packed families can take a shape: the pack grid's limits (batch
+// and row tiles of 32 in a grid dimension) and the TMA maps' 32-bit rows.
+bool packed_fits(int kernel, int64_t M, int64_t N, int64_t K, int64_t H) {
+  const PackedLayout L = packed_layout(kernel, M, N, K, H);
+  const int64_t rows = L.m_pad > L.n_pad ? L.m_pad : L.n_pad;
+  return H <= 65535 && rows / 32 <= 65535 && (int64_t)L.planes * H * rows < ((int64_t)1 << 31) &&
+         H * L.k_pad < ((int64_t)1 << 31) && K > 0;
+}
+
 int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, int num_sms) {
   auto tiles = [&](int bm, int bn) { return ((M + bm - 1) / bm) * ((N + bn - 1) / bn) * H; };
-  (void)K;
+  // At least a full wave of packed tiles and some depth: the pack pass (one
+  // read and one write of each operand) is then small beside the tiles' work.
+  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x128,
+                                PLAIN_C64_PACKED_3M_64x32};
+  {
+    const int pk = packed[dtype & 3];
+    int bm = 0, bn = 0;
+    plain_tile_shape(pk, &bm, &bn);
+    if (K >= 64 && tiles(bm, bn) >= num_sms && packed_fits(pk, M, N, K, H)) return pk;
+  }
   switch (dtype) {
     case 0: return tiles(128, 128) >= num_sms ? PLAIN_F32_SIMT_128x128 : PLAIN_F32_SIMT_64x64;
     case 1: return tiles(64, 64) >= num_sms ? PLAIN_F64_DMMA_64x64 : PLAIN_F64_DMMA_32x32;
@@ -1104,10 +1126,14 @@ void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K,
   };
   static const int large[4] = {PLAIN_F32_SIMT_128x128, PLAIN_F64_DMMA_64x64, PLAIN_C32_SIMT_64x64,
                                PLAIN_C64_DMMA_64x32};
+  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x128,
+                                PLAIN_C64_PACKED_3M_64x32};
   *splits = 1;
   *k_chunk = 0;
   const int64_t min_chunk = 512;  // K per split
-  const int k = pinned ? pinned : large[dtype & 3];
+  // Deep contractions split along K take the packed family when it fits.
+  const int big = packed_fits(packed[dtype & 3], M, N, K, H) ? packed[dtype & 3] : large[dtype & 3];
+  const int k = pinned ? pinned : big;
   const int64_t t = tiles(k);
   if (t < num_sms && K >= 2 * min_chunk) {
     int64_t s = (2 * num_sms + t - 1) / t;
@@ -1243,6 +1269,10 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_C64_DMMA_32x32: *bm = 32; *bn = 32; return;
     case PLAIN_F64_DMMA_128x32: *bm = 128; *bn = 32; return;
     case PLAIN_C64_DMMA_128x32: *bm = 128; *bn = 32; return;
+    case PLAIN_F32_PACKED_128x128: *bm = 128; *bn = 128; return;
+    case PLAIN_C32_PACKED_1M_64x128: *bm = 64; *bn = 128; return;
+    case PLAIN_F64_PACKED_64x64: *bm = 64; *bn = 64; return;
+    case PLAIN_C64_PACKED_3M_64x32: *bm = 64; *bn = 32; return;
   }
   *bm = *bn = 0;
 }

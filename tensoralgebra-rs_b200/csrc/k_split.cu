@@ -109,6 +109,26 @@ struct Pairs<3> {
   __device__ static inline int b(int p) { return p == 0 ? 0 : (p == 1 ? 1 : (p == 2 ? 0 : (p == 3 ? 2 : (p == 4 ? 1 : 0)))); }
 };
 
+// Tile order: within a batch entry, tiles go in groups of TILE_GROUP_M m-tiles
+// (the last group may be narrower); inside a group the m-tile is fastest, then
+// the n-tile. A wave of 148 CTAs then covers a block of about 16 A row panels
+// by 9 B column panels instead of 9 row panels by every column panel, so the
+// B planes a wave reads stay in L2 for the next wave of the same group.
+constexpr int TILE_GROUP_M = 16;
+
+__host__ __device__ inline void tile_coords(int64_t tile, int64_t tiles_m, int64_t tiles_n, int64_t& h, int64_t& mt,
+                                            int64_t& nt) {
+  const int64_t per_h = tiles_m * tiles_n;
+  h = tile / per_h;
+  const int64_t t = tile % per_h;
+  const int64_t group = t / (TILE_GROUP_M * tiles_n);
+  const int64_t first_m = group * TILE_GROUP_M;
+  const int64_t gm = tiles_m - first_m < TILE_GROUP_M ? tiles_m - first_m : TILE_GROUP_M;
+  const int64_t local = t - group * TILE_GROUP_M * tiles_n;
+  mt = first_m + local % gm;
+  nt = local / gm;
+}
+
 template <int S, int BN>
 struct TcCfg {
   static constexpr int A_TILE = TC_BM * TC_BK * 2;  // bytes of one A plane tile
@@ -169,8 +189,9 @@ tc_bf16_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     kb_lo = part * per;
     kb_hi = kb_lo + per < nk_all ? kb_lo + per : nk_all;
   }
-  const int64_t h = tile / (tiles_n * tiles_m);
-  const int64_t m0 = ((tile / tiles_n) % tiles_m) * TC_BM, n0 = (tile % tiles_n) * BN;
+  int64_t h, mt, nt;
+  tile_coords(tile, tiles_m, tiles_n, h, mt, nt);
+  const int64_t m0 = mt * TC_BM, n0 = nt * BN;
   const int nk = kb_hi - kb_lo;  // k-blocks of this CTA (>= 1)
   const int nchunks = (nk + CK - 1) / CK;
 
@@ -342,8 +363,9 @@ __global__ void __launch_bounds__(256) split_tail_reduce_kernel(GemmArgs g, cons
     const int64_t t = idx / (TC_BM * BN), within = idx % (TC_BM * BN);
     const int row = (int)(within % TC_BM), col = (int)(within / TC_BM);
     const int64_t tile = whole + t;
-    const int64_t h = tile / (tiles_n * tiles_m);
-    const int64_t m = ((tile / tiles_n) % tiles_m) * TC_BM + row, n = (tile % tiles_n) * BN + col;
+    int64_t h, mt, nt;
+    tile_coords(tile, tiles_m, tiles_n, h, mt, nt);
+    const int64_t m = mt * TC_BM + row, n = nt * BN + col;
     if (m >= g.M || n >= g.N) continue;
     float v = 0.f;
     for (int p = 0; p < parts; ++p) v += partial[(t * parts + p) * (int64_t)(TC_BM * BN) + within];

@@ -66,7 +66,13 @@ enum PlainKernel : int {
   PLAIN_C64_DMMA_32x32 = 7,
   PLAIN_F64_DMMA_128x32 = 8,  // tall tiles for N <= 32 (grouped lists)
   PLAIN_C64_DMMA_128x32 = 9,
-  PLAIN_LAST = 9,
+  // Packed families: a pack pass writes dense panels, a TMA-fed tile reads them
+  // (single launches only, never inside a grouped list).
+  PLAIN_F32_PACKED_128x128 = 10,
+  PLAIN_C32_PACKED_1M_64x128 = 11,  // 1m: the complex product as a 2M x N x 2K real one
+  PLAIN_F64_PACKED_64x64 = 12,
+  PLAIN_C64_PACKED_3M_64x32 = 13,   // 3m: three real products per complex MAC
+  PLAIN_LAST = 13,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).
@@ -88,6 +94,9 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
                            unsigned long long* counter, unsigned* status, int num_sms, cudaStream_t st);
 // Register-only pipe probes (0: FP64 DMMA, 1: FP32 FFMA); *flops = work launched.
 cudaError_t launch_probe(int which, void* sink, int blocks, int iters, cudaStream_t st, double* flops);
+// Tensor-pipe probe (one CTA per SM): dense 128 x 256 tcgen05.mma products,
+// kind::i8 (int8 = 1) or BF16 kind::f16 (int8 = 0); *ops = work launched.
+cudaError_t launch_tc_probe(int int8, int blocks, int iters, unsigned* status, cudaStream_t st, double* ops);
 // Bounded wait on a flag that stays zero: sets STATUS_WAIT_TIMEOUT after limit_ns.
 cudaError_t launch_wait_selftest(const unsigned* flag, unsigned* status, uint64_t limit_ns, cudaStream_t st);
 // Zero every element of a strided layout (origin = element of index 0).
@@ -117,6 +126,45 @@ void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K,
                          int* splits, int64_t* k_chunk);
 // Sum of the split-K partials (fixed order) and the epilogue into D.
 cudaError_t launch_splitk_reduce(int dtype, const GemmArgs& g, int splits, cudaStream_t st);
+
+// ---- packed plain families (pack pass + TMA-fed tiles) ----------------------
+//
+// The operands are first gathered through their scatter vectors into dense
+// panels (the reference's packed panels, crates/tprims-kernel/src/pack/
+// pack.rs:152-270, once per call for the whole operand), then a tile kernel
+// streams the panels into shared memory with TMA tiled loads:
+//   f32:     A' as [H][k_pad][m_pad], B' as [H][k_pad][n_pad] (rows fastest);
+//            FFMA, 128 x 128 tiles.
+//   c32 1m:  the complex product as a real one of 2M x N x 2K (the reference's
+//            induced 1m method, kernels/reference/induced.rs:67): A' element
+//            (m, k) becomes the real 2 x 2 block [[re, -im], [im, re]] at rows
+//            2m, 2m+1 and depths 2k, 2k+1; B' element (k, n) the pair [re; im]
+//            at depths 2k, 2k+1; output rows 2m, 2m+1 are Re and Im of row m.
+//   f64:     A' as [H][m_pad][k_pad], B' as [H][n_pad][k_pad] (k fastest,
+//            128-byte rows swizzled by TMA); DMMA, 64 x 64 tiles.
+//   c64 3m:  three planes per operand, [re, im, re + im] (pack/pack.rs:70-72,
+//            conjugation folded into the signs), three DMMA products M1 = Ar Br,
+//            M2 = Ai Bi, M3 = (Ar + Ai)(Br + Bi) recombined as
+//            (M1 - M2) + i (M3 - M1 - M2) (kernels/reference/scalar.rs:136,
+//            pack/writeback.rs:86-92); 64 x 32 tiles.
+// Split-K (k_chunk, partial) works as in the direct kernels.
+struct PackedLayout {
+  int kernel = 0;
+  int planes = 1;
+  int64_t m_pad = 0, n_pad = 0, k_pad = 0;  // of the (embedded) real problem
+  int64_t H = 0;
+};
+bool is_packed_kernel(int kernel);
+// The dtype (TAPP numbering) a packed family computes in.
+int packed_dtype(int kernel);
+// Whether a packed family can take a shape (grid and TMA coordinate limits).
+bool packed_fits(int kernel, int64_t M, int64_t N, int64_t K, int64_t H);
+PackedLayout packed_layout(int kernel, int64_t M, int64_t N, int64_t K, int64_t H);
+size_t packed_workspace_bytes(const PackedLayout& L);
+// Pack both operands into `panels` (packed_workspace_bytes of device memory).
+cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* panels, cudaStream_t st);
+// The tile kernel over the panels (with the epilogue, or split-K partials).
+cudaError_t launch_packed_gemm(const GemmArgs& g, const PackedLayout& L, const void* panels, cudaStream_t st);
 
 // ---- split precision (tensor cores) ----------------------------------------
 

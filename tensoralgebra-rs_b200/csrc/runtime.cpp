@@ -436,6 +436,39 @@ void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const Plain
     check_cuda(dev::launch_tiny_batched(dt, g, pr.tiny_h, ex.num_sms, ex.stream), "tiny batched launch");
     return;
   }
+  if (dev::is_packed_kernel(c.kernel)) {
+    // Pack pass into dense panels, then the TMA-fed tile (split-K partials
+    // after the panels when split).
+    if (dev::packed_dtype(c.kernel) != dt)
+      throw Error(ERR_INVALID_ARGUMENT, std::string("kernel family ") + dev::plain_kernel_name(c.kernel) +
+                                            " does not take " + dtype_name(pr.problem.dtype) + " operands");
+    if (!dev::packed_fits(c.kernel, g.M, g.N, g.K, g.H))
+      throw Error(ERR_UNSUPPORTED, std::string("kernel family ") + dev::plain_kernel_name(c.kernel) +
+                                       " cannot take this shape (batch, rows or depth beyond its grid)");
+    const dev::PackedLayout L = dev::packed_layout(c.kernel, g.M, g.N, g.K, g.H);
+    const size_t panels = dev::packed_workspace_bytes(L);
+    const size_t part = c.splits > 1 ? (size_t)c.splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype) + 256 : 0;
+    if (panels + part + 256 > scratch_bytes) throw Error(ERR_INTERNAL, "packed workspace too small");
+    char* pp = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
+    dev::GemmArgs gs = g;
+    if (c.splits > 1) {
+      gs.k_chunk = c.chunk;
+      gs.partial = reinterpret_cast<void*>(align_up((uintptr_t)(pp + panels), 256));
+    }
+    {
+      Timed t(ex, "plain_pack");
+      check_cuda(dev::launch_packed_pack(gs, L, pp, ex.stream), "plain pack launch");
+    }
+    {
+      Timed t(ex, dev::plain_kernel_name(c.kernel));
+      check_cuda(dev::launch_packed_gemm(gs, L, pp, ex.stream), "packed contraction launch");
+    }
+    if (c.splits > 1) {
+      Timed t(ex, "splitk_reduce");
+      check_cuda(dev::launch_splitk_reduce(dt, gs, c.splits, ex.stream), "split-K reduce launch");
+    }
+    return;
+  }
   if (c.splits > 1) {
     // Split-K: partial tiles into the scratch, then the reduce + epilogue.
     const size_t need = (size_t)c.splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype);
@@ -1338,6 +1371,7 @@ void zero_layout(Executor& ex, DType dt, const Operand& op, void* origin) {
   const bool dense = n == hi - lo + 1;
   if (classify(origin, ex.device) == Where::Device) {
     char* base = static_cast<char*>(origin);
+    Timed t(ex, "zero_fill");
     if (dense)
       check_cuda(cudaMemsetAsync(base + (int64_t)lo * (int64_t)elem, 0, (size_t)n * elem, ex.stream), "zero fill");
     else

@@ -130,17 +130,20 @@ inline EncodeTiledFn encode_fn() {
 }
 
 // A 2D tiled map over a row-major [rows][inner] array of `elem`-byte
-// elements, box [box_rows][box_inner], SWIZZLE_64B (box_inner * elem == 64).
+// elements, box [box_rows][box_inner], SWIZZLE_64B (box_inner * elem == 64)
+// unless another swizzle is given (128B: box_inner * elem == 128; NONE: any
+// multiple of 16 bytes up to 256 elements).
 inline bool make_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int elem, int64_t inner,
-                        int64_t rows, int box_inner, int box_rows) {
+                        int64_t rows, int box_inner, int box_rows,
+                        CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_64B) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)(inner * elem)};
   cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 

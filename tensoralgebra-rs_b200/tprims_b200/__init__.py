@@ -351,7 +351,8 @@ class Executor:
         return lib.tprims_b200_executor_selftest_wait(self.h, int(limit_ns))
 
     def probe_peak(self, which: int) -> float:
-        """Measured TFLOP/s of the FP64 DMMA (0) or FP32 FFMA (1) pipe on this device."""
+        """Measured TFLOP/s (TOP/s) of the FP64 DMMA (0), FP32 FFMA (1), INT8
+        tcgen05 (2) or BF16 tcgen05 (3) pipe on this device."""
         v = C.c_double(0)
         check(lib.tprims_b200_executor_probe_peak(self.h, int(which), C.byref(v)))
         return v.value

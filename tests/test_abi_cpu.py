@@ -367,7 +367,9 @@ def test_autotune_candidates(tp):
     assert {"sm100.f64.dmma884.64x64x16", "sm100.f64.dmma884.32x32x16", "sm100.f64.dmma884.128x32x16"} <= set(c1)
     assert any("+splitk" in c for c in c1) and len(c1) == len(set(c1))
     big = _gemm_product(tp, 4096, 4096, 4096, dt=0).report()["autotune_candidates"]
-    assert sorted(big) == ["sm100.f32.simt.128x128x16", "sm100.f32.simt.64x64x16"]  # enough tiles: no split
+    assert big[0] == "sm100.f32.simt.tma.packed.128x128x16"  # the model: packed, a full wave of tiles
+    assert sorted(big) == ["sm100.f32.simt.128x128x16", "sm100.f32.simt.64x64x16",
+                           "sm100.f32.simt.tma.packed.128x128x16"]  # enough tiles: no split
     shallow = _gemm_product(tp, 64, 64, 128).report()["autotune_candidates"]
     assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
     c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]
@@ -499,7 +501,7 @@ def test_tuning_file_format_is_checked_without_a_gpu(tp, tmp_path):
                     "list list-0123456789abcdef-n3 2 1 1.5 3\n")
     assert tp.tuning_file_info(str(good)) == {"sms": 148, "device": "NVIDIA_B200", "single": 3, "list": 1}
     bad_lines = [
-        "single sig 10 1 0 0 1 0.1 1",    # no kernel family 10
+        "single sig 14 1 0 0 1 0.1 1",    # no kernel family 14
         "single sig 3 2 0 0 1 0.1 1",     # split without a chunk
         "single sig 3 65 64 0 1 0.1 1",   # more than 64 chunks
         "single sig 3 1 0 0 1 0.1",       # a field short

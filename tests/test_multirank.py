@@ -47,6 +47,85 @@ def test_two_gloo_ranks_shard_and_reduce(n):
     assert all(res[r][2] == 3.5 for r in range(world))
 
 
+def _contract_share(tp, items, share):
+    """Each item of `share` through the three binary steps of the C4 update,
+    planned by the library (Problem::from_labels, Plan::new on the CPU) and
+    executed on the host through the plan's own scatter vectors, the way the
+    kernels address memory (A' = A[h_a + a_m + a_k], B' = B[h_b + b_k + b_n],
+    D[h_d + d_m + d_n] = A' B')."""
+    import numpy as np
+
+    results = {}
+    for q in share:
+        it = items[q]
+        ext = bench.c4_extents(it)
+        bufs = {k: it[k].astype(np.complex128) for k in ("E", "Ma", "W", "Mb")}
+        code = tp.C64 if it["E"].dtype == np.complex128 else tp.F64
+        for xa, la, xb, lb, xd, ld, cj in bench.C4_STEPS:
+            ea, eb, ed = ([ext[x] for x in ls] for ls in (la, lb, ld))
+            plan = tp.Plan(tp.Problem.from_labels(code, tp.OperandSpec(tp.LayoutSpec.col_major(ea)),
+                                                  tp.OperandSpec(tp.LayoutSpec.col_major(eb), cj),
+                                                  tp.OperandSpec(tp.LayoutSpec.col_major(ed)), la, lb, ld))
+            sc = {n: np.array(tp.product_scatter(plan.product, n), dtype=np.int64) for n in tp.SCATTER_NAMES}
+            one = np.zeros(1, np.int64)
+            h_a, h_b, h_d = (sc[n] if len(sc[n]) else one for n in ("h_a", "h_b", "h_d"))
+            out = np.zeros(int(np.prod(ed)), dtype=np.complex128)
+            A, B = bufs[xa], (np.conj(bufs[xb]) if cj else bufs[xb])
+            for h in range(max(len(sc["h_d"]), 1)):
+                Am = A[h_a[h] + sc["a_m"][:, None] + sc["a_k"][None, :]]
+                Bn = B[h_b[h] + sc["b_k"][:, None] + sc["b_n"][None, :]]
+                out[h_d[h] + sc["d_m"][:, None] + sc["d_n"][None, :]] = Am @ Bn
+            bufs[xd] = out
+        results[q] = bufs["Ep"]
+    return results
+
+
+def _rank_contracts(rank, world, port, dt, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    import tprims_b200 as tp
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    items = bench.c4_items(12, dt, seed=4321)
+    costs = [it["a"] * it["s"] * it["b"] * it["p"] * it["a"] for it in items]
+    part = tp.balance(costs, [0] * world)  # the same longest-first assignment on every rank
+    mine = [q for q in range(len(items)) if part[q] == rank]
+    res = _contract_share(tp, items, mine)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, sorted(res))
+    dist.barrier()
+    out[rank] = (gathered, {q: v.tolist() for q, v in res.items()})
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dt", ["float64", "complex128"])
+def test_two_gloo_ranks_contract_disjoint_shares_of_a_list(tp, dt):
+    """Two gloo ranks each plan and contract their own share of an uneven list
+    of environment updates (no exchange step on the data path); the shares are
+    disjoint, cover the list, and every result equals the four-tensor
+    contraction in complex128."""
+    import numpy as np
+
+    world = 2
+    with mp.get_context("spawn").Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_rank_contracts, args=(world, _free_port(), dt, out), nprocs=world, join=True)
+        res = dict(out)
+    items = bench.c4_items(12, dt, seed=4321)
+    shares = [set(res[r][1]) for r in range(world)]
+    assert shares[0].isdisjoint(shares[1]) and shares[0] | shares[1] == set(range(len(items)))
+    assert all(s for s in shares), "a rank received no items"
+    assert res[0][0] == res[1][0] == [sorted(s) for s in shares]
+    for r in range(world):
+        for q, v in res[r][1].items():
+            it = items[q]
+            got = np.array(v).reshape((it["a"], it["s"], it["b"]), order="F")
+            want = bench.c4_reference(it)
+            assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-12, (r, q)
+
+
 def test_shard_is_balanced():
     for n in (10, 4096, 3):
         sizes = [bench.shard(n, r, 8)[1] - bench.shard(n, r, 8)[0] for r in range(8)]

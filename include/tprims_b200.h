@@ -212,6 +212,17 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_synchronize(TAPP_executor exe
    device memory run as one persistent grouped launch per kernel family,
    replayed from a cached CUDA graph; with 0 every item is its own launch. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int on);
+/* Streamed execution of host operands (no counterpart in the reference, whose
+   operands are always host memory): with `on` != 0 (the default) a single
+   contraction of at least 32 MiB whose A, B and D are all host memory, whose
+   C is not read and which writes every element of D is split into chunks
+   along the outermost column axis of its output; the copy in of one chunk,
+   the kernels of the previous one and the copy out of the one before run at
+   once on the executor's stream and two copy streams. The call stays
+   synchronous and the result is the same as unstreamed (the kernels are the
+   same). Layouts whose chunks cannot be moved as whole pitched copies (not
+   nested, or negative strides) run unstreamed. 0 = always unstreamed. */
+TPRIMS_B200_EXPORT TAPP_error tprims_b200_executor_set_streaming(TAPP_executor exec, int on);
 /* Failure detection without a GPU fault. tprims_b200_executor_set_workspace_limit
    caps the executor's workspace arena (0 = no cap): a call that needs more is
    refused with TPRIMS_ERR_INTERNAL before anything runs (allocation-failure
@@ -279,8 +290,14 @@ enum {
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan, int scheme, int slices);
 /* Pin the plain-path tile family (0 = chosen per shape). Rows x cols of the
    oriented M/N tile: 1 f32 128x128, 2 f32 64x64, 3 f64 64x64, 4 f64 32x32,
-   5 c32 64x64, 6 c64 64x32, 7 c64 32x32, 8 f64 128x32, 9 c64 128x32. A family
-   of another dtype is refused at execution (TPRIMS_ERR_INTERNAL). */
+   5 c32 64x64, 6 c64 64x32, 7 c64 32x32, 8 f64 128x32, 9 c64 128x32 (direct
+   tiles: the gather is part of the tile); packed families (a pack pass into
+   dense panels, then TMA-fed tiles; single contractions only, a grouped list
+   runs its items on direct tiles): 10 f32 128x128, 11 c32 64x128 as 1m (the
+   2M x N x 2K real embedding), 12 f64 64x64, 13 c64 64x32 as 3m (three real
+   products per complex MAC). A direct family of another dtype is refused at
+   execution with TPRIMS_ERR_INTERNAL, a packed one with
+   TPRIMS_ERR_INVALID_ARGUMENT. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);
 /* Plan::check_raw (crates/tprims-contract/src/plan/mod.rs:384): the aliasing
    preflight of a call from its origins alone (nothing is dereferenced; a NULL

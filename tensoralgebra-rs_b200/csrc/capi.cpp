@@ -998,6 +998,14 @@ extern "C" TAPP_error tprims_b200_executor_set_grouping(TAPP_executor exec, int 
   });
 }
 
+extern "C" TAPP_error tprims_b200_executor_set_streaming(TAPP_executor exec, int on) {
+  return ffi([&] {
+    Executor& ex = resolve_exec(exec)->get();
+    std::lock_guard<std::mutex> lk(ex.mu);
+    ex.streaming = on != 0;
+  });
+}
+
 extern "C" TAPP_error tprims_b200_executor_set_workspace_limit(TAPP_executor exec, size_t bytes) {
   return ffi([&] {
     Executor& ex = resolve_exec(exec)->get();

@@ -73,7 +73,9 @@ template <class R, bool CPLX, int MODE>
 __global__ void __launch_bounds__(256) plain_pack_kernel(const typename Elem<R, CPLX>::type* __restrict__ X,
                                                          const int64_t* __restrict__ rows_scat,
                                                          const int64_t* __restrict__ k_scat,
-                                                         const int64_t* __restrict__ h_scat, int64_t nrows, int64_t K,
+                                                         const int64_t* __restrict__ h_scat,
+                                                         const int64_t* __restrict__ rows_blk,
+                                                         const int64_t* __restrict__ k_blk, int64_t nrows, int64_t K,
                                                          int kfast, int conj, PanelArgs o) {
   using T = typename Elem<R, CPLX>::type;
   __shared__ R tre[32][33];
@@ -81,18 +83,61 @@ __global__ void __launch_bounds__(256) plain_pack_kernel(const typename Elem<R, 
   const int tid = threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32, h = blockIdx.z;
   const T* base = X + h_scat[h];
+  // A whole tile on regular blocks of both vectors (block size 32 = the
+  // tile): one base offset and two strides, 16-byte vectors along a
+  // unit-stride fast index when aligned.
+  int64_t rs = SCATTER_IRREGULAR, ks = SCATTER_IRREGULAR;
+  if (rows_blk && k_blk && r0 + 32 <= nrows && k0 + 32 <= K) {
+    rs = rows_blk[blockIdx.y];
+    ks = k_blk[blockIdx.x];
+  }
+  if (rs != SCATTER_IRREGULAR && ks != SCATTER_IRREGULAR) {
+    const T* tb = base + rows_scat[r0] + k_scat[k0];
+    const int64_t fs = kfast ? ks : rs, ss = kfast ? rs : ks;  // strides of the fast and the slow index
+    constexpr int VEC = 16 / (int)sizeof(T);
+    if (VEC > 1 && fs == 1 && (reinterpret_cast<uintptr_t>(tb) & 15) == 0 && ((ss * (int64_t)sizeof(T)) & 15) == 0) {
+      constexpr int TPR = 32 / (VEC > 1 ? VEC : 1);  // threads per slow index
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int a = tid & 31, b = (tid >> 5) + 8 * j;
-    const int rr = kfast ? b : a, kk = kfast ? a : b;
-    const int64_t r = r0 + rr, k = k0 + kk;
-    R re = R(0), im = R(0);
-    if (r < nrows && k < K) {
-      Elem<R, CPLX>::load(base + rows_scat[r] + k_scat[k], re, im);
-      if (conj) im = -im;
+      for (int j = 0; j < 32 * TPR / 256; ++j) {
+        const int a0 = (tid % TPR) * VEC, b = tid / TPR + j * (256 / TPR);
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(tb + b * ss + a0));
+        const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+          R re, im;
+          Elem<R, CPLX>::load(e + q, re, im);
+          if (conj) im = -im;
+          const int rr = kfast ? b : a0 + q, kk = kfast ? a0 + q : b;
+          tre[rr][kk] = re;
+          if (CPLX) tim[rr][kk] = im;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int a = tid & 31, b = (tid >> 5) + 8 * j;
+        R re, im;
+        Elem<R, CPLX>::load(tb + a * fs + b * ss, re, im);
+        if (conj) im = -im;
+        const int rr = kfast ? b : a, kk = kfast ? a : b;
+        tre[rr][kk] = re;
+        if (CPLX) tim[rr][kk] = im;
+      }
     }
-    tre[rr][kk] = re;
-    if (CPLX) tim[rr][kk] = im;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int a = tid & 31, b = (tid >> 5) + 8 * j;
+      const int rr = kfast ? b : a, kk = kfast ? a : b;
+      const int64_t r = r0 + rr, k = k0 + kk;
+      R re = R(0), im = R(0);
+      if (r < nrows && k < K) {
+        Elem<R, CPLX>::load(base + rows_scat[r] + k_scat[k], re, im);
+        if (conj) im = -im;
+      }
+      tre[rr][kk] = re;
+      if (CPLX) tim[rr][kk] = im;
+    }
   }
   __syncthreads();
   R* out = static_cast<R*>(o.out);
@@ -525,14 +570,17 @@ size_t elem_bytes_of(int kernel) {
 }
 
 template <class R, bool CPLX, int MODE>
-cudaError_t run_pack(const void* X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
-                     int64_t nrows, int64_t K, int kfast, int conj, const PanelArgs& o, int64_t src_rows,
-                     int64_t src_k, cudaStream_t st) {
+cudaError_t run_pack(const GemmArgs& g, int which, const PanelArgs& o, int64_t src_rows, int64_t src_k,
+                     cudaStream_t st) {
   const int64_t gy = (src_rows + 31) / 32, gx = (src_k + 31) / 32;
   if (gy > 65535 || o.H > 65535 || gx > 0x7fffffff) return cudaErrorInvalidConfiguration;
   dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)o.H);
-  plain_pack_kernel<R, CPLX, MODE><<<grid, 256, 0, st>>>(static_cast<const typename Elem<R, CPLX>::type*>(X),
-                                                         rows_scat, k_scat, h_scat, nrows, K, kfast, conj, o);
+  using T = typename Elem<R, CPLX>::type;
+  const bool a = which == 0;
+  plain_pack_kernel<R, CPLX, MODE><<<grid, 256, 0, st>>>(
+      static_cast<const T*>(a ? g.A : g.B), a ? g.s.a_m : g.s.b_n, a ? g.s.a_k : g.s.b_k, a ? g.s.h_a : g.s.h_b,
+      a ? g.s.blk_a_m : g.s.blk_b_n, a ? g.s.blk_a_k : g.s.blk_b_k, a ? g.M : g.N, g.K, a ? g.a_kfast : g.b_kfast,
+      CPLX ? (a ? g.conj_a : g.conj_b) : 0, o);
   return cudaGetLastError();
 }
 
@@ -599,29 +647,21 @@ cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* p
   cudaError_t r;
   switch (L.kernel) {
     case PLAIN_F32_PACKED_128x128:
-      r = run_pack<float, false, PM_ROWS_FAST>(g.A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, g.a_kfast, 0, oa, L.m_pad,
-                                               L.k_pad, st);
+      r = run_pack<float, false, PM_ROWS_FAST>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<float, false, PM_ROWS_FAST>(g.B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, g.b_kfast, 0, ob, L.n_pad,
-                                                  L.k_pad, st);
+      return run_pack<float, false, PM_ROWS_FAST>(g, 1, ob, L.n_pad, L.k_pad, st);
     case PLAIN_C32_PACKED_1M_64x128:
-      r = run_pack<float, true, PM_1M_A>(g.A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, g.a_kfast, g.conj_a, oa,
-                                         L.m_pad / 2, (L.k_pad + 1) / 2, st);
+      r = run_pack<float, true, PM_1M_A>(g, 0, oa, L.m_pad / 2, (L.k_pad + 1) / 2, st);
       if (r != cudaSuccess) return r;
-      return run_pack<float, true, PM_1M_B>(g.B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, g.b_kfast, g.conj_b, ob,
-                                            L.n_pad, (L.k_pad + 1) / 2, st);
+      return run_pack<float, true, PM_1M_B>(g, 1, ob, L.n_pad, (L.k_pad + 1) / 2, st);
     case PLAIN_F64_PACKED_64x64:
-      r = run_pack<double, false, PM_K_FAST>(g.A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, g.a_kfast, 0, oa, L.m_pad,
-                                             L.k_pad, st);
+      r = run_pack<double, false, PM_K_FAST>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<double, false, PM_K_FAST>(g.B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, g.b_kfast, 0, ob, L.n_pad,
-                                                L.k_pad, st);
+      return run_pack<double, false, PM_K_FAST>(g, 1, ob, L.n_pad, L.k_pad, st);
     case PLAIN_C64_PACKED_3M_64x32:
-      r = run_pack<double, true, PM_3M>(g.A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, g.a_kfast, g.conj_a, oa, L.m_pad,
-                                        L.k_pad, st);
+      r = run_pack<double, true, PM_3M>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<double, true, PM_3M>(g.B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, g.b_kfast, g.conj_b, ob,
-                                           L.n_pad, L.k_pad, st);
+      return run_pack<double, true, PM_3M>(g, 1, ob, L.n_pad, L.k_pad, st);
   }
   return cudaErrorInvalidValue;
 }

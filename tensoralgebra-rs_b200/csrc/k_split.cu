@@ -54,27 +54,73 @@ __device__ inline void split3(float x, __nv_bfloat16& p0, __nv_bfloat16& p1, __n
 // Gather + split + K-major write of one 32-row x 64-k tile.
 __global__ void __launch_bounds__(256) split_pack_kernel(const float* __restrict__ X, const int64_t* __restrict__ rows_scat,
                                                          const int64_t* __restrict__ k_scat,
-                                                         const int64_t* __restrict__ h_scat, int64_t nrows, int64_t K,
+                                                         const int64_t* __restrict__ h_scat,
+                                                         const int64_t* __restrict__ rows_blk,
+                                                         const int64_t* __restrict__ k_blk, int64_t nrows, int64_t K,
                                                          int64_t rows_pad, int64_t k_pad, int64_t H, int kfast,
                                                          int planes, __nv_bfloat16* __restrict__ out) {
   __shared__ float tile[32][65];
   const int tid = threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 64, h = blockIdx.z;
   const float* base = X + h_scat[h];
+  // A whole tile on regular blocks (32 rows; two 32-deep k blocks of one
+  // arithmetic run): addressed from one base offset and two strides, with
+  // float4 loads along a unit-stride fast index when aligned.
+  int64_t rs = SCATTER_IRREGULAR, ks = SCATTER_IRREGULAR;
+  if (rows_blk && k_blk && r0 + 32 <= nrows && k0 + 64 <= K) {
+    rs = rows_blk[blockIdx.y];
+    const int64_t k1 = k_blk[2 * blockIdx.x], k2 = k_blk[2 * blockIdx.x + 1];
+    if (k1 != SCATTER_IRREGULAR && k1 == k2 && k_scat[k0 + 32] - k_scat[k0] == 32 * k1) ks = k1;
+  }
+  if (rs != SCATTER_IRREGULAR && ks != SCATTER_IRREGULAR) {
+    const float* tb = base + rows_scat[r0] + k_scat[k0];
+    const int64_t fs = kfast ? ks : rs, ss = kfast ? rs : ks;
+    if (fs == 1 && (reinterpret_cast<uintptr_t>(tb) & 15) == 0 && (ss & 3) == 0) {
+      // kfast: 16 threads per row (64 k); otherwise 8 threads per k column (32 rows).
+      const int tpr = kfast ? 16 : 8;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    int rr, kk;
-    if (kfast) {
-      rr = tid / 64 + 4 * j;
-      kk = tid % 64;
+      for (int j = 0; j < 2; ++j) {
+        const int a0 = (tid % tpr) * 4, b = tid / tpr + j * (256 / tpr);
+        const float4 v = __ldg(reinterpret_cast<const float4*>(tb + b * ss + a0));
+        const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (kfast)
+            tile[b][a0 + q] = e[q];
+          else
+            tile[a0 + q][b] = e[q];
+        }
+      }
     } else {
-      rr = tid % 32;
-      kk = tid / 32 + 8 * j;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        int rr, kk;
+        if (kfast) {
+          rr = tid / 64 + 4 * j;
+          kk = tid % 64;
+        } else {
+          rr = tid % 32;
+          kk = tid / 32 + 8 * j;
+        }
+        tile[rr][kk] = __ldg(tb + rr * rs + kk * ks);
+      }
     }
-    const int64_t r = r0 + rr, k = k0 + kk;
-    float v = 0.f;
-    if (r < nrows && k < K) v = base[rows_scat[r] + k_scat[k]];
-    tile[rr][kk] = v;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int rr, kk;
+      if (kfast) {
+        rr = tid / 64 + 4 * j;
+        kk = tid % 64;
+      } else {
+        rr = tid % 32;
+        kk = tid / 32 + 8 * j;
+      }
+      const int64_t r = r0 + rr, k = k0 + kk;
+      float v = 0.f;
+      if (r < nrows && k < K) v = base[rows_scat[r] + k_scat[k]];
+      tile[rr][kk] = v;
+    }
   }
   __syncthreads();
   const int64_t plane_stride = H * rows_pad * k_pad;
@@ -455,7 +501,8 @@ cudaError_t launch_split_pack_f32(const GemmArgs& g, int which, const SplitLayou
   dim3 grid((unsigned)(L.k_pad / 64), (unsigned)(rows_pad / 32), (unsigned)L.H);
   if (L.H > 65535 || rows_pad / 32 > 65535) return cudaErrorInvalidConfiguration;
   split_pack_kernel<<<grid, 256, 0, st>>>(static_cast<const float*>(a ? g.A : g.B), a ? g.s.a_m : g.s.b_n,
-                                          a ? g.s.a_k : g.s.b_k, a ? g.s.h_a : g.s.h_b, a ? g.M : g.N, g.K, rows_pad,
+                                          a ? g.s.a_k : g.s.b_k, a ? g.s.h_a : g.s.h_b, a ? g.s.blk_a_m : g.s.blk_b_n,
+                                          a ? g.s.blk_a_k : g.s.blk_b_k, a ? g.M : g.N, g.K, rows_pad,
                                           L.k_pad, L.H, a ? g.a_kfast : g.b_kfast, L.planes,
                                           static_cast<__nv_bfloat16*>(planes));
   return cudaGetLastError();

@@ -15,8 +15,22 @@
 namespace tprims {
 namespace dev {
 
+// Block scatters of the operand vectors (the reference's block scatter,
+// crates/tprims-kernel/src/pack/scatter.rs:148-171, IRREGULAR sentinel :43):
+// entry j of blk_x is the common difference of x[32 j .. 32 j + 31] (0 for a
+// one-entry block) or SCATTER_IRREGULAR when the block is not an arithmetic
+// run. A pack pass whose 32-row x 32-k tile sits on regular blocks of both of
+// its vectors addresses the tile from one base offset and two strides (no
+// per-element index loads), and loads 16-byte vectors along a unit-stride
+// run. Null when absent (the kernels then read the scatter vectors); the
+// struct is an aggregate, so an initializer list of the first 12 vectors (or
+// value-initialization) leaves them null.
+constexpr int SCATTER_BLOCK = 32;
+constexpr int64_t SCATTER_IRREGULAR = INT64_MIN;
+
 struct Scatters {
   const int64_t *a_m, *a_k, *b_k, *b_n, *c_m, *c_n, *d_m, *d_n, *h_a, *h_b, *h_c, *h_d;
+  const int64_t *blk_a_m, *blk_a_k, *blk_b_k, *blk_b_n;
 };
 
 // D = op_D(alpha * acc + beta * op_C(C)); beta_zero means C is never read.

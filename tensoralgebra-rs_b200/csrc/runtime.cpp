@@ -104,6 +104,11 @@ Executor::~Executor() {
   }
   if (ws) cudaFree(ws);
   if (status) cudaFree(status);
+  if (copy_in) cudaStreamSynchronize(copy_in);
+  if (copy_out) cudaStreamSynchronize(copy_out);
+  for (cudaEvent_t e : stream_events) cudaEventDestroy(e);
+  if (copy_in) cudaStreamDestroy(copy_in);
+  if (copy_out) cudaStreamDestroy(copy_out);
   if (own_stream && stream) cudaStreamDestroy(stream);
   if (capture_stream) cudaStreamDestroy(capture_stream);
   if (prev >= 0) cudaSetDevice(prev);
@@ -163,11 +168,18 @@ const dev::Scatters& Product::scatters(int device, cudaStream_t stream) {
   std::lock_guard<std::mutex> lk(mu);
   auto it = dev.find(device);
   if (it != dev.end()) return it->second.s;
-  const std::vector<int64_t>* vs[12] = {&view.a_m, &view.a_k, &view.b_k, &view.b_n, &view.c_m, &view.c_n,
-                                        &view.d_m, &view.d_n, &view.h_a, &view.h_b, &view.h_c, &view.h_d};
+  // The 12 scatter vectors, then the block scatters (blocks of
+  // dev::SCATTER_BLOCK) of a_m, a_k, b_k and b_n for the pack passes.
+  const std::vector<int64_t> blk[4] = {
+      build_block_scatter(view.a_m, dev::SCATTER_BLOCK), build_block_scatter(view.a_k, dev::SCATTER_BLOCK),
+      build_block_scatter(view.b_k, dev::SCATTER_BLOCK), build_block_scatter(view.b_n, dev::SCATTER_BLOCK)};
+  static_assert(IRREGULAR == dev::SCATTER_IRREGULAR, "one sentinel for irregular blocks");
+  const std::vector<int64_t>* vs[16] = {&view.a_m, &view.a_k, &view.b_k, &view.b_n, &view.c_m, &view.c_n,
+                                        &view.d_m, &view.d_n, &view.h_a, &view.h_b, &view.h_c, &view.h_d,
+                                        &blk[0],   &blk[1],   &blk[2],   &blk[3]};
   std::vector<int64_t> host;
-  size_t offs[12];
-  for (int i = 0; i < 12; ++i) {
+  size_t offs[16];
+  for (int i = 0; i < 16; ++i) {
     offs[i] = host.size();
     host.insert(host.end(), vs[i]->begin(), vs[i]->end());
     host.push_back(0);  // never empty
@@ -188,6 +200,10 @@ const dev::Scatters& Product::scatters(int device, cudaStream_t stream) {
   const int64_t* b = ds.buf;
   ds.s = dev::Scatters{b + offs[0], b + offs[1], b + offs[2],  b + offs[3],  b + offs[4],  b + offs[5],
                        b + offs[6], b + offs[7], b + offs[8], b + offs[9], b + offs[10], b + offs[11]};
+  ds.s.blk_a_m = b + offs[12];
+  ds.s.blk_a_k = b + offs[13];
+  ds.s.blk_b_k = b + offs[14];
+  ds.s.blk_b_n = b + offs[15];
   return dev.emplace(device, ds).first->second.s;
 }
 
@@ -777,10 +793,243 @@ TuneEntry autotune_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, char
   return best;
 }
 
-// Enqueue one item; returns whether host copies were involved (the caller
-// must then drain the stream before returning to the host).
 int dt_code(const Product& pr) { return (int)pr.problem.dtype; }
 
+// ---- streamed host execution
+//
+// With A, B and D in host memory, a synchronous call spends most of its time
+// on the host link: every operand is copied in, the kernels run, D is copied
+// out. Split along the outermost column axis of the oriented product (the
+// last folded axis of N'), chunk c of the output needs all of A' but only
+// chunk c of B' (and writes chunk c of D), so the copy of B' chunk c + 1, the
+// kernels of chunk c and the copy out of chunk c - 1 run at once on three
+// streams. A' is copied and (for the split schemes) packed once.
+
+// One copy of a chunk region: `rows` rows of `width` bytes, `pitch` bytes
+// apart, starting `off` bytes from the operand's origin.
+struct ChunkCopy {
+  int64_t off;
+  size_t width, rows, pitch;
+};
+
+// The copies that move exactly the elements of an operand whose chunk-axis
+// index lies in [lo, hi). `axes` are the operand's other axes as (extent,
+// stride); those with a stride below `sc` must fit inside one chunk-axis
+// step, those above must each span the whole block below them (a nested
+// layout), and every stride must be positive. The smallest outer axis gives
+// the rows of one pitched copy, further outer axes are looped (at most 4096
+// copies).
+bool chunk_copies(const std::vector<std::pair<int64_t, int64_t>>& axes, int64_t sc, int64_t ec, int64_t lo,
+                  int64_t hi, int64_t elem, std::vector<ChunkCopy>& out) {
+  if (sc <= 0 || lo >= hi) return false;
+  int64_t inner_max = 0;
+  std::vector<std::pair<int64_t, int64_t>> outer;  // (stride, extent)
+  for (const auto& a : axes) {
+    if (a.first <= 1 || a.second == 0) continue;
+    if (a.second < 0 || a.second == sc) return false;
+    if (a.second < sc)
+      inner_max += (a.first - 1) * a.second;
+    else
+      outer.push_back({a.second, a.first});
+  }
+  if (inner_max >= sc) return false;
+  std::sort(outer.begin(), outer.end());
+  int64_t reach = (ec - 1) * sc + inner_max;  // last offset of the block below the next outer axis
+  for (const auto& o : outer) {
+    if (o.first <= reach) return false;
+    reach += (o.second - 1) * o.first;
+  }
+  const int64_t seg0 = lo * sc, seg_len = (hi - 1) * sc + inner_max + 1 - seg0;
+  int64_t combos = 1;
+  for (size_t i = 1; i < outer.size(); ++i) combos *= outer[i].second;
+  if (combos > 4096) return false;
+  for (int64_t c = 0; c < combos; ++c) {
+    int64_t base = 0, rem = c;
+    for (size_t i = 1; i < outer.size(); ++i) {
+      base += (rem % outer[i].second) * outer[i].first;
+      rem /= outer[i].second;
+    }
+    ChunkCopy cc;
+    cc.off = (base + seg0) * elem;
+    cc.width = (size_t)(seg_len * elem);
+    cc.rows = outer.empty() ? 1 : (size_t)outer[0].second;
+    cc.pitch = outer.empty() ? cc.width : (size_t)(outer[0].first * elem);
+    out.push_back(cc);
+  }
+  return true;
+}
+
+// Runs the item streamed when it qualifies (see above): returns false, with
+// nothing enqueued, when it does not.
+bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
+  const Problem& p = pr.problem;
+  const OrientedView& v = pr.view;
+  const PlanStats& stt = pr.packed.stats;
+  const int64_t elem = (int64_t)dtype_size(p.dtype);
+  const int sx = v.swapped ? SA : SB;  // the operand that plays B'
+  const std::vector<Axis>& nax = v.swapped ? stt.m_axes : stt.n_axes;
+  if (nax.empty() || v.H > 65535) return false;
+  const Axis& ca = nax.back();
+  const int64_t E = ca.extent;
+  if (E < 2) return false;
+  const int nchunks = (int)std::min<int64_t>(E, 4);
+  const int64_t inner_n = v.N / E;
+  if (v.N / nchunks < 256) return false;
+  const auto stride_in = [](const Axis& a, int slot) {
+    return slot == SA ? a.sa : slot == SB ? a.sb : slot == SC ? a.sc : a.sd;
+  };
+  const auto others = [&](int slot) {
+    std::vector<std::pair<int64_t, int64_t>> out;
+    for (const std::vector<Axis>* role : {&stt.m_axes, &stt.n_axes, &stt.k_axes, &stt.h_axes})
+      for (const Axis& a : *role)
+        if (&a != &ca) out.push_back({a.extent, stride_in(a, slot)});
+    return out;
+  };
+  std::vector<std::vector<ChunkCopy>> bcp(nchunks), dcp(nchunks);
+  std::vector<int64_t> lo(nchunks), hi(nchunks);
+  for (int c = 0; c < nchunks; ++c) {
+    lo[c] = E * c / nchunks;
+    hi[c] = E * (c + 1) / nchunks;
+    if (!chunk_copies(others(sx), stride_in(ca, sx), E, lo[c], hi[c], elem, bcp[c]) ||
+        !chunk_copies(others(SD), stride_in(ca, SD), E, lo[c], hi[c], elem, dcp[c]))
+      return false;
+  }
+  // Kernel configuration per chunk (the plain path: one launch each, no split-K).
+  const bool split = pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6;
+  std::vector<PlainChoice> pcs(nchunks);
+  size_t scratch = 0;
+  if (split) {
+    const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
+    int64_t ncmax = 0;
+    for (int c = 0; c < nchunks; ++c) ncmax = std::max(ncmax, (hi[c] - lo[c]) * inner_n);
+    const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, v.M, ncmax, v.K, v.H);
+    scratch = align_up((size_t)L.planes * L.H * L.m_pad * L.k_pad * 2, 256) +
+              align_up((size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2, 256) + dev::split_tail_bytes(L, ex.num_sms) +
+              1024;
+  } else if (pr.scheme == Scheme::Plain) {
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t nc = (hi[c] - lo[c]) * inner_n;
+      PlainChoice& pc = pcs[c];
+      if (dev::use_tiny_batched(v.M, nc, v.K, v.H)) return false;
+      dev::choose_plain_launch((int)p.dtype, pr.kernel_pin, v.M, nc, v.K, v.H, ex.num_sms, &pc.kernel, &pc.splits,
+                               &pc.chunk);
+      if (pc.splits > 1) return false;
+      if (dev::is_packed_kernel(pc.kernel))
+        scratch = std::max(scratch, dev::packed_workspace_bytes(dev::packed_layout(pc.kernel, v.M, nc, v.K, v.H)) + 512);
+    }
+  } else {
+    return false;
+  }
+
+  // Workspace: the staged spans of A, B and D, then the kernels' scratch.
+  Staged st[4];
+  const void* origins[4] = {it.a, it.b, nullptr, it.d};
+  size_t total = 0;
+  for (int s : {SA, SB, SD}) {
+    st[s].host = origins[s];
+    st[s].staged = true;
+    span_bytes(p, s, &st[s].lo_bytes, &st[s].bytes);
+    total = align_up(total, 256) + st[s].bytes;
+  }
+  injected_failure_check(ex);
+  char* ws = static_cast<char*>(ex.workspace(align_up(total, 256) + align_up(scratch, 256) + 1024));
+  size_t off = 0;
+  for (int s : {SA, SB, SD}) {
+    off = align_up(off, 256);
+    st[s].buf = ws + off;
+    st[s].dev_origin = st[s].buf - st[s].lo_bytes;
+    off += st[s].bytes;
+  }
+  char* scratch_ptr = reinterpret_cast<char*>(align_up((uintptr_t)(ws + off), 256));
+  if (!ex.copy_in) check_cuda(cudaStreamCreateWithFlags(&ex.copy_in, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!ex.copy_out) check_cuda(cudaStreamCreateWithFlags(&ex.copy_out, cudaStreamNonBlocking), "cudaStreamCreate");
+  while ((int)ex.stream_events.size() < 2 * nchunks + 3) {
+    cudaEvent_t e;
+    check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    ex.stream_events.push_back(e);
+  }
+  cudaEvent_t* ev = ex.stream_events.data();
+  // The copy streams start behind everything already on the executor's stream.
+  check_cuda(cudaEventRecord(ev[2 * nchunks + 2], ex.stream), "cudaEventRecord");
+  check_cuda(cudaStreamWaitEvent(ex.copy_in, ev[2 * nchunks + 2], 0), "cudaStreamWaitEvent");
+  check_cuda(cudaStreamWaitEvent(ex.copy_out, ev[2 * nchunks + 2], 0), "cudaStreamWaitEvent");
+
+  // In: the whole of the A' operand, then B' chunk by chunk.
+  const int sy = v.swapped ? SB : SA;
+  check_cuda(cudaMemcpyAsync(st[sy].buf, static_cast<const char*>(st[sy].host) + st[sy].lo_bytes, st[sy].bytes,
+                             cudaMemcpyHostToDevice, ex.copy_in),
+             "host-to-device copy");
+  check_cuda(cudaEventRecord(ev[0], ex.copy_in), "cudaEventRecord");
+  for (int c = 0; c < nchunks; ++c) {
+    for (const ChunkCopy& cc : bcp[c])
+      check_cuda(cudaMemcpy2DAsync(st[sx].dev_origin + cc.off, cc.pitch,
+                                   static_cast<const char*>(st[sx].host) + cc.off, cc.pitch, cc.width, cc.rows,
+                                   cudaMemcpyHostToDevice, ex.copy_in),
+                 "host-to-device chunk copy");
+    check_cuda(cudaEventRecord(ev[1 + c], ex.copy_in), "cudaEventRecord");
+  }
+
+  // Kernels, chunk by chunk, on the executor's stream.
+  check_cuda(cudaStreamWaitEvent(ex.stream, ev[0], 0), "cudaStreamWaitEvent");
+  const dev::GemmArgs g = build_args(pr, ex, alpha, Scalar{}, false, st[SA].dev_origin, st[SB].dev_origin, nullptr,
+                                     st[SD].dev_origin);
+  dev::SplitLayout L{};
+  char* ap = scratch_ptr;
+  if (split) {
+    L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
+    Timed t(ex, "split_pack");
+    check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
+  }
+  char* bp = ap + align_up((size_t)L.planes * L.H * L.m_pad * L.k_pad * 2, 256);
+  for (int c = 0; c < nchunks; ++c) {
+    check_cuda(cudaStreamWaitEvent(ex.stream, ev[1 + c], 0), "cudaStreamWaitEvent");
+    dev::GemmArgs gc = g;
+    const int64_t n0 = lo[c] * inner_n;
+    gc.N = (hi[c] - lo[c]) * inner_n;
+    gc.s.b_n += n0;
+    gc.s.c_n += n0;
+    gc.s.d_n += n0;
+    gc.s.blk_b_n = (n0 % dev::SCATTER_BLOCK == 0) ? g.s.blk_b_n + n0 / dev::SCATTER_BLOCK : nullptr;
+    if (split) {
+      const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, v.M, gc.N, v.K, v.H);
+      char* tail = reinterpret_cast<char*>(
+          align_up((uintptr_t)(bp + (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2), 256));
+      {
+        Timed t(ex, "split_pack");
+        check_cuda(dev::launch_split_pack_f32(gc, 1, Lc, bp, ex.stream), "split pack B");
+      }
+      Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
+      check_cuda(dev::launch_tc_bf16_gemm(gc, Lc, ap, bp, (int)pr.scheme, ex.stream, tail),
+                 "tcgen05 contraction launch");
+    } else {
+      launch_plain(pr, ex, gc, pcs[c], scratch_ptr, scratch);
+    }
+    check_cuda(cudaEventRecord(ev[1 + nchunks + c], ex.stream), "cudaEventRecord");
+  }
+  if (!split) {
+    std::lock_guard<std::mutex> lk(pr.mu);
+    pr.last = pcs[0];
+    pr.last_source = (pr.kernel_pin || pr.split_pin) ? ChoiceSource::Pinned : ChoiceSource::Model;
+    pr.executed = true;
+  }
+
+  // Out: D chunk by chunk as each is written; the executor's stream then
+  // waits for the last copy, so draining it covers the whole call.
+  for (int c = 0; c < nchunks; ++c) {
+    check_cuda(cudaStreamWaitEvent(ex.copy_out, ev[1 + nchunks + c], 0), "cudaStreamWaitEvent");
+    for (const ChunkCopy& cc : dcp[c])
+      check_cuda(cudaMemcpy2DAsync(const_cast<char*>(static_cast<const char*>(st[SD].host)) + cc.off, cc.pitch,
+                                   st[SD].dev_origin + cc.off, cc.pitch, cc.width, cc.rows, cudaMemcpyDeviceToHost,
+                                   ex.copy_out),
+                 "device-to-host chunk copy");
+  }
+  check_cuda(cudaEventRecord(ev[2 * nchunks + 1], ex.copy_out), "cudaEventRecord");
+  check_cuda(cudaStreamWaitEvent(ex.stream, ev[2 * nchunks + 1], 0), "cudaStreamWaitEvent");
+  return true;
+}
+
+// Enqueue one item; returns whether host copies were involved (the caller
+// must then drain the stream before returning to the host).
 bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const Item& it) {
   const Problem& p = pr.problem;
   if (p.out_empty) return false;
@@ -808,6 +1057,12 @@ bool enqueue_item(Product& pr, Executor& ex, Scalar alpha, Scalar beta, const It
     span_bytes(p, s, &st[s].lo_bytes, &st[s].bytes);
     total = align_up(total, 256) + st[s].bytes;
   }
+  // Large contractions of host operands that write all of D and read no C
+  // run streamed (copies in and out overlap the kernels chunk by chunk).
+  if (ex.streaming && need_ab && !c_read && st[SA].staged && st[SB].staged && st[SD].staged && !pr.autotune &&
+      pr.split_pin <= 1 && fully_written(pr) &&
+      st[SA].bytes + st[SB].bytes + st[SD].bytes >= (size_t(32) << 20) && enqueue_streamed(pr, ex, alpha, it))
+    return true;
   // The plain path's configuration: the pins, else (autotune) the executor's
   // tuning cache or a measurement now, else the model.
   PlainChoice pc{};

@@ -107,6 +107,13 @@ struct Executor {
   std::map<std::string, TuneEntry> tune;
   std::map<std::string, TuneEntry> list_tune;
   std::string device_name;
+  // Streamed host execution (host operands split into chunks along the
+  // output's outermost column axis; copies in, kernels and copies out of
+  // successive chunks overlap): switch, copy streams and events, the latter
+  // created on first use.
+  bool streaming = true;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> stream_events;
 
   static Executor* create(int device, uintptr_t stream);
   ~Executor();

@@ -67,7 +67,7 @@ ABI_SYMBOLS = [
     "tprims_b200_product_set_tile", "tprims_b200_product_report", "tprims_b200_product_from_dot_general",
     "tprims_b200_execute_product_dlpack", "tprims_b200_contract_batched", "tprims_b200_product_vjp",
     "tprims_b200_product_scatter", "tprims_b200_executor_set_profiling", "tprims_b200_executor_kernel_times",
-    "tprims_b200_executor_set_grouping", "tprims_b200_executor_set_workspace_limit",
+    "tprims_b200_executor_set_grouping", "tprims_b200_executor_set_streaming", "tprims_b200_executor_set_workspace_limit",
     "tprims_b200_executor_selftest_wait", "tprims_b200_executor_probe_peak",
     "tprims_b200_execute_product_noalloc", "tprims_b200_product_set_split_k", "tprims_b200_product_set_autotune",
     "tprims_b200_executor_save_tuning", "tprims_b200_executor_load_tuning", "tprims_b200_executor_clear_tuning",
@@ -106,6 +106,7 @@ lib.tprims_b200_executor_set_sync.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_synchronize.argtypes = [_ip]
 lib.tprims_b200_executor_set_profiling.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_set_grouping.argtypes = [_ip, C.c_int]
+lib.tprims_b200_executor_set_streaming.argtypes = [_ip, C.c_int]
 lib.tprims_b200_executor_set_workspace_limit.argtypes = [_ip, C.c_size_t]
 lib.tprims_b200_executor_selftest_wait.argtypes = [_ip, C.c_uint64]
 lib.tprims_b200_executor_probe_peak.argtypes = [_ip, C.c_int, C.POINTER(C.c_double)]
@@ -337,6 +338,11 @@ class Executor:
     def set_grouping(self, on: bool):
         """Grouped persistent launches (cached in CUDA graphs) for lists; off = one launch per item."""
         check(lib.tprims_b200_executor_set_grouping(self.h, 1 if on else 0))
+
+    def set_streaming(self, on: bool):
+        """Streamed execution of large host-operand contractions (chunked copies
+        overlapping the kernels); off = copy in, run, copy out."""
+        check(lib.tprims_b200_executor_set_streaming(self.h, 1 if on else 0))
 
     def set_workspace_limit(self, nbytes: int):
         """Cap the workspace arena (0 = no cap); larger requests are refused."""

@@ -1135,9 +1135,13 @@ void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K,
   const int big = packed_fits(packed[dtype & 3], M, N, K, H) ? packed[dtype & 3] : large[dtype & 3];
   const int k = pinned ? pinned : big;
   const int64_t t = tiles(k);
-  if (t < num_sms && K >= 2 * min_chunk) {
+  // Packed tiles stream their K range through a TMA ring, so shorter chunks
+  // (at least 128 deep) still keep the pipe busy: a moderately deep
+  // contraction with less than a wave of tiles splits too.
+  const int64_t chunk_min = is_packed_kernel(k) ? 128 : min_chunk;
+  if (t < num_sms && K >= 2 * chunk_min) {
     int64_t s = (2 * num_sms + t - 1) / t;
-    s = s < K / min_chunk ? s : K / min_chunk;
+    s = s < K / chunk_min ? s : K / chunk_min;
     s = s < 64 ? s : 64;
     if (s > 1) {
       const int64_t chunk = ((K + s - 1) / s + 63) / 64 * 64;  // whole 64-deep blocks

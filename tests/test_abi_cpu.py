@@ -265,7 +265,8 @@ def test_executor_handles_without_a_gpu(tp):
 
 def test_planner_splits_k_only_for_deep_contractions_with_few_tiles(tp):
     """The launch choice (reported per plan, for 148 SMs): split-K when the
-    large-tile grid has fewer tiles than SMs and K is deep; never otherwise."""
+    large-tile grid has fewer tiles than SMs and K is deep (packed tiles: at
+    least two chunks of 128); never otherwise."""
     def report(m, n, k, dt=1):
         h = tp.Handle()
         infos = [tp.TensorInfo(dt, [m, k], [1, m]), tp.TensorInfo(dt, [k, n], [1, k]),
@@ -277,7 +278,9 @@ def test_planner_splits_k_only_for_deep_contractions_with_few_tiles(tp):
     deep = report(512, 512, 32768)
     assert deep["split_k"] > 1 and "64x64" in deep["family"]
     assert report(4096, 4096, 4096, dt=0)["split_k"] == 1  # enough tiles
-    assert report(64, 64, 512)["split_k"] == 1  # shallow
+    assert report(64, 64, 192)["split_k"] == 1  # shallow
+    c1_like = report(576, 576, 576)  # 81 packed tiles, K = 576: three chunks of 192
+    assert c1_like["split_k"] == 3 and ".tma." in c1_like["family"], c1_like
 
 
 def test_launch_choices_reported_per_plan(tp):
@@ -363,7 +366,7 @@ def test_autotune_candidates(tp):
     tile family of the dtype, split-K only while tiles x splits <= 4 x SMs and
     the chunks stay at least 128 deep."""
     c1 = _gemm_product(tp, 576, 576, 576).report()["autotune_candidates"]
-    assert c1[0] == _gemm_product(tp, 576, 576, 576).report()["family"]
+    assert c1[0].startswith(_gemm_product(tp, 576, 576, 576).report()["family"])  # the model's choice first
     assert {"sm100.f64.dmma884.64x64x16", "sm100.f64.dmma884.32x32x16", "sm100.f64.dmma884.128x32x16"} <= set(c1)
     assert any("+splitk" in c for c in c1) and len(c1) == len(set(c1))
     big = _gemm_product(tp, 4096, 4096, 4096, dt=0).report()["autotune_candidates"]
@@ -373,7 +376,8 @@ def test_autotune_candidates(tp):
     shallow = _gemm_product(tp, 64, 64, 128).report()["autotune_candidates"]
     assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
     c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]
-    assert c32[0].startswith("sm100.c32.simt.ring")
+    assert c32[0].startswith("sm100.c32.simt.tma.1m")  # packed 1m, K split in two (15 tiles)
+    assert any(c.startswith("sm100.c32.simt.ring") for c in c32)
 
 
 def test_plain_c_consumer_compiles_links_and_runs(tmp_path):
@@ -401,7 +405,11 @@ def test_report_tile_ctas_and_scratch(tp):
     launch (tiles x K chunks) and the workspace the scheme needs."""
     r = _gemm_product(tp, 576, 576, 576).report()
     bm, bn = r["tile"]
-    assert r["ctas"] == -(-576 // bm) * -(-576 // bn) and r["scratch_bytes"] == 0
+    assert r["ctas"] == -(-576 // bm) * -(-576 // bn) * r["split_k"]
+    # The packed family's panels (576 x 576 of A and B, f64) plus the split-K partials.
+    assert r["scratch_bytes"] >= 2 * 576 * 576 * 8 + r["split_k"] * 576 * 576 * 8
+    small = _gemm_product(tp, 96, 96, 96).report()  # direct tiles, no split: no scratch
+    assert small["split_k"] == 1 and small["scratch_bytes"] == 0 and ".tma." not in small["family"]
     deep = _gemm_product(tp, 512, 512, 32768).report()
     assert deep["split_k"] > 1 and deep["ctas"] == 64 * deep["split_k"]
     assert deep["scratch_bytes"] >= deep["split_k"] * 512 * 512 * 8  # the split-K partials

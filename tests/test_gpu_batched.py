@@ -1,8 +1,10 @@
 """contract_batched on the GPU: the config-4 list of environment updates (three
 binary steps per item over uneven extents), run as grouped persistent launches
-replayed from cached CUDA graphs, against the same list run one launch per item
-(bitwise identical: the same tile body and family) and against the four-tensor
-contraction in complex128."""
+replayed from cached CUDA graphs (a replay bitwise equal to the captured run),
+against the same list run one launch per item (each item on the single-launch
+family the model picks for it, a packed 3m or DMMA tile where the grouped list
+runs a direct one: equal within the plain bound 1e-13) and against the
+four-tensor contraction in complex128."""
 import numpy as np
 import pytest
 
@@ -52,7 +54,8 @@ def test_grouped_list_matches_per_item_and_the_full_contraction(tp, torch_cuda, 
     grouped = run(True)   # captures the graphs
     replay = run(True)    # replays them
     for s, g, r in zip(single, grouped, replay):
-        assert np.array_equal(s, g) and np.array_equal(g, r)
+        assert np.array_equal(g, r)
+        assert np.linalg.norm(s - g) <= 1e-13 * np.linalg.norm(g)
     # New input values behind the same pointers: the replayed graph reads them.
     for d in dev:
         d["W"].mul_(2.0)

@@ -523,7 +523,7 @@ def run_config(args, tp, torch, ex):
         lay = tp.LayoutSpec([n, n], [1, n])
         prob = tp.Problem.from_labels(code, tp.OperandSpec(lay), tp.OperandSpec(lay), tp.OperandSpec(lay),
                                       [2, 0], [2, 1], [0, 1])
-        plan = tp.Plan(prob)
+        plan = tp.Plan(prob, tp.PlanConfig(kernel=args.kernel))
         gen = torch.Generator(device="cuda").manual_seed(20261203 + 8000)
         A = torch.randn(n * n, dtype=tdt, device="cuda", generator=gen)
         B = torch.randn(n * n, dtype=tdt, device="cuda", generator=gen)
@@ -914,6 +914,7 @@ def main():
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
     ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
     ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")
+    ap.add_argument("--kernel", type=int, default=0, help="tile family pinned for --config gemm (0 = the model's)")
     ap.add_argument("--tccg-size", default="tccg64", choices=["tccg64", "small"], help="sizing of --config tccg")
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c3", "c4", "c4c", "c5", "corpus", "gemm", "tccg"],

@@ -295,7 +295,8 @@ TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_prod
    dense panels, then TMA-fed tiles; single contractions only, a grouped list
    runs its items on direct tiles): 10 f32 128x128, 11 c32 64x128 as 1m (the
    2M x N x 2K real embedding), 12 f64 64x64, 13 c64 64x32 as 3m (three real
-   products per complex MAC). A direct family of another dtype is refused at
+   products per complex MAC), 14 f32 128x64 and 15 c32 64x64 as 1m (half-width
+   tiles, two CTAs per SM). A direct family of another dtype is refused at
    execution with TPRIMS_ERR_INTERNAL, a packed one with
    TPRIMS_ERR_INVALID_ARGUMENT. */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_tile(TAPP_tensor_product plan, int kernel_id);

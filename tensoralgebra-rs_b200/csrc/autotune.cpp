@@ -55,9 +55,10 @@ std::string device_tag(const Executor& ex) {
 
 // The single-launch tile families of each dtype (direct, then packed).
 const int kFamilies[4][4] = {
-    {dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, dev::PLAIN_F32_PACKED_128x128, 0},
+    {dev::PLAIN_F32_SIMT_128x128, dev::PLAIN_F32_SIMT_64x64, dev::PLAIN_F32_PACKED_128x128,
+     dev::PLAIN_F32_PACKED_128x64},
     {dev::PLAIN_F64_DMMA_64x64, dev::PLAIN_F64_DMMA_32x32, dev::PLAIN_F64_DMMA_128x32, dev::PLAIN_F64_PACKED_64x64},
-    {dev::PLAIN_C32_SIMT_64x64, dev::PLAIN_C32_PACKED_1M_64x128, 0, 0},
+    {dev::PLAIN_C32_SIMT_64x64, dev::PLAIN_C32_PACKED_1M_64x128, dev::PLAIN_C32_PACKED_1M_64x64, 0},
     {dev::PLAIN_C64_DMMA_64x32, dev::PLAIN_C64_DMMA_32x32, dev::PLAIN_C64_DMMA_128x32, dev::PLAIN_C64_PACKED_3M_64x32}};
 
 }  // namespace

@@ -190,10 +190,19 @@ __global__ void __launch_bounds__(256) plain_pack_kernel(const typename Elem<R, 
 
 // ------------------------------------------------------------ FFMA tile (f32)
 
-constexpr int SP_BM = 128, SP_BN = 128, SP_BK = 16, SP_STAGES = 4, SP_FLUSH = 4;
-constexpr int SP_A = SP_BK * SP_BM * 4, SP_B = SP_BK * SP_BN * 4, SP_STAGE = SP_A + SP_B;
-constexpr int SP_COMPUTE = 256, SP_THREADS = SP_COMPUTE + 32;
-constexpr int SP_SMEM = 1024 + SP_STAGES * SP_STAGE + (2 * SP_BM + 2 * SP_BN) * 8 + 2 * SP_STAGES * 8 + 16;
+// Tile shapes of the FFMA kernel: 128 rows x BN columns, 16-deep stages, 256
+// compute threads each with 8 rows x BN/16 columns (groups of four columns
+// 64 apart), one producer warp. BN = 128 runs one CTA per SM (168 registers),
+// BN = 64 two (half the accumulators, twice the warps to hide latency).
+template <int BN>
+struct SpCfg {
+  static constexpr int BM = 128, BK = 16, STAGES = BN == 128 ? 4 : 6, FLUSH = 4;
+  static constexpr int TN = BN / 16, CG = TN / 4;  // columns per thread, groups of four
+  static constexpr int A = BK * BM * 4, B = BK * BN * 4, STAGE = A + B;
+  static constexpr int COMPUTE = 256, THREADS = COMPUTE + 32;
+  static constexpr int MINB = BN == 128 ? 1 : 2;
+  static constexpr int SMEM = 1024 + STAGES * STAGE + (2 * BM + 2 * BN) * 8 + 2 * STAGES * 8 + 16;
+};
 
 // Stores four consecutive rows of one column when D's rows are consecutive in
 // memory and the address is 16-byte aligned (the reference's unit-stride
@@ -209,37 +218,39 @@ __device__ inline bool store4_f32(const Epilogue& e, float* d0, const int64_t* d
   return true;
 }
 
-template <bool ONEM>
-__global__ void __launch_bounds__(SP_THREADS, 1)
+template <bool ONEM, int BN>
+__global__ void __launch_bounds__(SpCfg<BN>::THREADS, SpCfg<BN>::MINB)
 simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g,
                    int64_t k_pad, int64_t tiles_m, int64_t tiles_n, int64_t kchunk, int splits) {
+  using Cfg = SpCfg<BN>;
+  constexpr int BM = Cfg::BM, BK = Cfg::BK, STAGES = Cfg::STAGES, TN = Cfg::TN, CG = Cfg::CG;
   using T = typename Elem<float, ONEM>::type;
-  constexpr int EROWS = ONEM ? SP_BM / 2 : SP_BM;  // output rows per tile
+  constexpr int EROWS = ONEM ? BM / 2 : BM;  // output rows per tile
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* ring = smem;
-  int64_t* dm_s = reinterpret_cast<int64_t*>(smem + SP_STAGES * SP_STAGE);
-  int64_t* cm_s = dm_s + SP_BM;
-  int64_t* dn_s = cm_s + SP_BM;
-  int64_t* cn_s = dn_s + SP_BN;
-  uint64_t* full = reinterpret_cast<uint64_t*>(cn_s + SP_BN);
-  uint64_t* empty = full + SP_STAGES;
-  int* stop = reinterpret_cast<int*>(empty + SP_STAGES);
+  int64_t* dm_s = reinterpret_cast<int64_t*>(smem + STAGES * Cfg::STAGE);
+  int64_t* cm_s = dm_s + BM;
+  int64_t* dn_s = cm_s + BM;
+  int64_t* cn_s = dn_s + BN;
+  uint64_t* full = reinterpret_cast<uint64_t*>(cn_s + BN);
+  uint64_t* empty = full + STAGES;
+  int* stop = reinterpret_cast<int*>(empty + STAGES);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t split = (int64_t)blockIdx.x % splits, tile = (int64_t)blockIdx.x / splits;
   int64_t h, mt, nt;
   packed_tile_coords(tile, tiles_m, tiles_n, h, mt, nt);
-  const int64_t m0 = mt * SP_BM, n0 = nt * SP_BN, em0 = ONEM ? m0 / 2 : m0;
-  const int64_t nkb_all = k_pad / SP_BK;
-  const int64_t kb_lo = kchunk ? split * (kchunk / SP_BK) : 0;
-  const int64_t kb_hi = kchunk ? min(nkb_all, kb_lo + kchunk / SP_BK) : nkb_all;
+  const int64_t m0 = mt * BM, n0 = nt * BN, em0 = ONEM ? m0 / 2 : m0;
+  const int64_t nkb_all = k_pad / BK;
+  const int64_t kb_lo = kchunk ? split * (kchunk / BK) : 0;
+  const int64_t kb_hi = kchunk ? min(nkb_all, kb_lo + kchunk / BK) : nkb_all;
   const int nk = (int)(kb_hi - kb_lo);
 
   if (warp == 8 && lane == 0) {
-    for (int s = 0; s < SP_STAGES; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], SP_COMPUTE / 32);
+      mbar_init(&empty[s], Cfg::COMPUTE / 32);
     }
     fence_barrier_init();
     *stop = nk;
@@ -252,7 +263,7 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
     dm_s[tid] = ok ? g.s.d_m[m] : 0;
     cm_s[tid] = (ok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
   }
-  if (tid < SP_BN) {
+  if (tid < BN) {
     const int64_t n = n0 + tid;
     const bool ok = n < g.N;
     dn_s[tid] = ok ? g.s.d_n[n] : 0;
@@ -264,59 +275,65 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
   if (warp == 8) {
     if (lane == 0) {
       for (int i = 0; i < nk; ++i) {
-        const int s = i % SP_STAGES;
-        const uint32_t round = (uint32_t)(i / SP_STAGES);
+        const int s = i % STAGES;
+        const uint32_t round = (uint32_t)(i / STAGES);
         if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) {
           atomicOr(g.status, STATUS_WAIT_TIMEOUT);
           break;
         }
-        mbar_arrive_expect_tx(&full[s], (uint32_t)SP_STAGE);
-        const int y = (int)(h * k_pad + (kb_lo + i) * SP_BK);
-        tma_load_2d(ring + s * SP_STAGE, &tmA, &full[s], (int)m0, y);
-        tma_load_2d(ring + s * SP_STAGE + SP_A, &tmB, &full[s], (int)n0, y);
+        mbar_arrive_expect_tx(&full[s], (uint32_t)Cfg::STAGE);
+        const int y = (int)(h * k_pad + (kb_lo + i) * BK);
+        tma_load_2d(ring + s * Cfg::STAGE, &tmA, &full[s], (int)m0, y);
+        tma_load_2d(ring + s * Cfg::STAGE + Cfg::A, &tmB, &full[s], (int)n0, y);
         issued = i + 1;
       }
     }
   } else {
     const int tx = tid & 15, ty = tid >> 4;
-    float tot[8][8], acc[8][8];
+    float tot[8][TN], acc[8][TN];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < TN; ++j) {
         tot[i][j] = 0.f;
         acc[i][j] = 0.f;
       }
     for (int i = 0; i < nk; ++i) {
-      const int s = i % SP_STAGES;
-      const uint32_t round = (uint32_t)(i / SP_STAGES);
+      const int s = i % STAGES;
+      const uint32_t round = (uint32_t)(i / STAGES);
       if (!mbar_wait(&full[s], round & 1u)) {
         atomicOr(g.status, STATUS_WAIT_TIMEOUT);
         atomicMin(stop, i);
         break;
       }
-      const float* As = reinterpret_cast<const float*>(ring + s * SP_STAGE);
-      const float* Bs = reinterpret_cast<const float*>(ring + s * SP_STAGE + SP_A);
+      const float* As = reinterpret_cast<const float*>(ring + s * Cfg::STAGE);
+      const float* Bs = reinterpret_cast<const float*>(ring + s * Cfg::STAGE + Cfg::A);
 #pragma unroll
-      for (int kk = 0; kk < SP_BK; ++kk) {
-        const float4 a0 = *reinterpret_cast<const float4*>(As + kk * SP_BM + tx * 4);
-        const float4 a1 = *reinterpret_cast<const float4*>(As + kk * SP_BM + 64 + tx * 4);
-        const float4 b0 = *reinterpret_cast<const float4*>(Bs + kk * SP_BN + ty * 4);
-        const float4 b1 = *reinterpret_cast<const float4*>(Bs + kk * SP_BN + 64 + ty * 4);
+      for (int kk = 0; kk < BK; ++kk) {
+        const float4 a0 = *reinterpret_cast<const float4*>(As + kk * BM + tx * 4);
+        const float4 a1 = *reinterpret_cast<const float4*>(As + kk * BM + 64 + tx * 4);
+        float br[TN];
+#pragma unroll
+        for (int c = 0; c < CG; ++c) {
+          const float4 b = *reinterpret_cast<const float4*>(Bs + kk * BN + 64 * c + ty * 4);
+          br[4 * c] = b.x;
+          br[4 * c + 1] = b.y;
+          br[4 * c + 2] = b.z;
+          br[4 * c + 3] = b.w;
+        }
         const float ar[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-        const float br[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii)
 #pragma unroll
-          for (int jj = 0; jj < 8; ++jj) acc[ii][jj] = fmaf(ar[ii], br[jj], acc[ii][jj]);
+          for (int jj = 0; jj < TN; ++jj) acc[ii][jj] = fmaf(ar[ii], br[jj], acc[ii][jj]);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-      if ((i + 1) % SP_FLUSH == 0) {
+      if ((i + 1) % Cfg::FLUSH == 0) {
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii)
 #pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
+          for (int jj = 0; jj < TN; ++jj) {
             tot[ii][jj] += acc[ii][jj];
             acc[ii][jj] = 0.f;
           }
@@ -325,15 +342,15 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
 #pragma unroll
     for (int ii = 0; ii < 8; ++ii)
 #pragma unroll
-      for (int jj = 0; jj < 8; ++jj) tot[ii][jj] += acc[ii][jj];
+      for (int jj = 0; jj < TN; ++jj) tot[ii][jj] += acc[ii][jj];
 
     // Epilogue. Thread rows: tx*4 + [0,4) and 64 + tx*4 + [0,4); columns
-    // ty*4 + [0,4) and 64 + ty*4 + [0,4).
+    // 64 c + ty*4 + [0,4) for each group c.
     const T* Cb = static_cast<const T*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
     T* Db = static_cast<T*>(g.D) + g.s.h_d[h];
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-      const int cc = (jj < 4) ? (ty * 4 + jj) : (64 + ty * 4 + jj - 4);
+    for (int jj = 0; jj < TN; ++jj) {
+      const int cc = 64 * (jj / 4) + ty * 4 + (jj % 4);
       const int64_t n = n0 + cc;
       if (n >= g.N) continue;
 #pragma unroll
@@ -379,7 +396,7 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
   __syncthreads();
   // Copies issued but not consumed (only after a timeout) land before exit.
   if (warp == 8 && lane == 0)
-    for (int i = *stop; i < issued; ++i) (void)mbar_wait(&full[i % SP_STAGES], (uint32_t)(i / SP_STAGES) & 1u);
+    for (int i = *stop; i < issued; ++i) (void)mbar_wait(&full[i % STAGES], (uint32_t)(i / STAGES) & 1u);
 }
 
 // ------------------------------------------------------------ DMMA tile (f64)
@@ -584,15 +601,41 @@ cudaError_t run_pack(const GemmArgs& g, int which, const PanelArgs& o, int64_t s
   return cudaGetLastError();
 }
 
+// The FFMA tile over f32 panels: [H * k_pad] rows of m_pad (n_pad) floats,
+// boxes of 16 rows x 128 (BN) floats.
+template <bool ONEM, int BN>
+cudaError_t run_simt_packed(const GemmArgs& g, const PackedLayout& L, const void* pa, const void* pb, int64_t splits,
+                            cudaStream_t st) {
+  using Cfg = SpCfg<BN>;
+  if (L.H * L.k_pad >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+  CUtensorMap ma, mb;
+  if (!make_map_2d(&ma, pa, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L.m_pad, L.H * L.k_pad, Cfg::BM, Cfg::BK,
+                   CU_TENSOR_MAP_SWIZZLE_NONE) ||
+      !make_map_2d(&mb, pb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L.n_pad, L.H * L.k_pad, BN, Cfg::BK,
+                   CU_TENSOR_MAP_SWIZZLE_NONE))
+    return cudaErrorInvalidValue;
+  const int64_t tiles = (L.m_pad / Cfg::BM) * (L.n_pad / BN) * L.H;
+  const int64_t kchunk = g.k_chunk ? (ONEM ? 2 * g.k_chunk : g.k_chunk) : 0;
+  if (tiles * splits >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+  auto kern = simt_packed_kernel<ONEM, BN>;
+  cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+  if (r != cudaSuccess) return r;
+  kern<<<(unsigned)(tiles * splits), Cfg::THREADS, Cfg::SMEM, st>>>(ma, mb, g, L.k_pad, L.m_pad / Cfg::BM,
+                                                                    L.n_pad / BN, kchunk, (int)splits);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
-bool is_packed_kernel(int kernel) { return kernel >= PLAIN_F32_PACKED_128x128 && kernel <= PLAIN_C64_PACKED_3M_64x32; }
+bool is_packed_kernel(int kernel) { return kernel >= PLAIN_F32_PACKED_128x128 && kernel <= PLAIN_C32_PACKED_1M_64x64; }
 
 int packed_dtype(int kernel) {
   switch (kernel) {
-    case PLAIN_F32_PACKED_128x128: return 0;
+    case PLAIN_F32_PACKED_128x128:
+    case PLAIN_F32_PACKED_128x64: return 0;
     case PLAIN_F64_PACKED_64x64: return 1;
-    case PLAIN_C32_PACKED_1M_64x128: return 2;
+    case PLAIN_C32_PACKED_1M_64x128:
+    case PLAIN_C32_PACKED_1M_64x64: return 2;
     case PLAIN_C64_PACKED_3M_64x32: return 3;
   }
   return -1;
@@ -604,14 +647,16 @@ PackedLayout packed_layout(int kernel, int64_t M, int64_t N, int64_t K, int64_t 
   L.H = H;
   switch (kernel) {
     case PLAIN_F32_PACKED_128x128:
-      L.m_pad = round_up(M, SP_BM);
-      L.n_pad = round_up(N, SP_BN);
-      L.k_pad = round_up(K, SP_BK);
+    case PLAIN_F32_PACKED_128x64:
+      L.m_pad = round_up(M, SpCfg<128>::BM);
+      L.n_pad = round_up(N, kernel == PLAIN_F32_PACKED_128x128 ? 128 : 64);
+      L.k_pad = round_up(K, SpCfg<128>::BK);
       break;
     case PLAIN_C32_PACKED_1M_64x128:
-      L.m_pad = round_up(2 * M, SP_BM);
-      L.n_pad = round_up(N, SP_BN);
-      L.k_pad = round_up(2 * K, SP_BK);
+    case PLAIN_C32_PACKED_1M_64x64:
+      L.m_pad = round_up(2 * M, SpCfg<128>::BM);
+      L.n_pad = round_up(N, kernel == PLAIN_C32_PACKED_1M_64x128 ? 128 : 64);
+      L.k_pad = round_up(2 * K, SpCfg<128>::BK);
       break;
     case PLAIN_F64_PACKED_64x64:
       L.m_pad = round_up(M, DpF64::BM);
@@ -647,10 +692,12 @@ cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* p
   cudaError_t r;
   switch (L.kernel) {
     case PLAIN_F32_PACKED_128x128:
+    case PLAIN_F32_PACKED_128x64:
       r = run_pack<float, false, PM_ROWS_FAST>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
       return run_pack<float, false, PM_ROWS_FAST>(g, 1, ob, L.n_pad, L.k_pad, st);
     case PLAIN_C32_PACKED_1M_64x128:
+    case PLAIN_C32_PACKED_1M_64x64:
       r = run_pack<float, true, PM_1M_A>(g, 0, oa, L.m_pad / 2, (L.k_pad + 1) / 2, st);
       if (r != cudaSuccess) return r;
       return run_pack<float, true, PM_1M_B>(g, 1, ob, L.n_pad, (L.k_pad + 1) / 2, st);
@@ -675,25 +722,11 @@ cudaError_t launch_packed_gemm(const GemmArgs& g, const PackedLayout& L, const v
   const int64_t splits = g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1;
   if (splits > 64) return cudaErrorInvalidValue;
   CUtensorMap ma, mb;
-  const bool onem = L.kernel == PLAIN_C32_PACKED_1M_64x128;
-  if (L.kernel == PLAIN_F32_PACKED_128x128 || onem) {
-    // [H * k_pad] rows of m_pad (n_pad) floats; boxes of 16 rows x 128 floats.
-    if (L.H * L.k_pad >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
-    if (!make_map_2d(&ma, pa, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L.m_pad, L.H * L.k_pad, SP_BM, SP_BK,
-                     CU_TENSOR_MAP_SWIZZLE_NONE) ||
-        !make_map_2d(&mb, pb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L.n_pad, L.H * L.k_pad, SP_BN, SP_BK,
-                     CU_TENSOR_MAP_SWIZZLE_NONE))
-      return cudaErrorInvalidValue;
-    const int64_t tiles = (L.m_pad / SP_BM) * (L.n_pad / SP_BN) * L.H;
-    const int64_t kchunk = g.k_chunk ? (onem ? 2 * g.k_chunk : g.k_chunk) : 0;
-    if (tiles * splits >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
-    auto kern = onem ? simt_packed_kernel<true> : simt_packed_kernel<false>;
-    cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SP_SMEM);
-    if (r != cudaSuccess) return r;
-    kern<<<(unsigned)(tiles * splits), SP_THREADS, SP_SMEM, st>>>(ma, mb, g, L.k_pad, L.m_pad / SP_BM,
-                                                                  L.n_pad / SP_BN, kchunk, (int)splits);
-    return cudaGetLastError();
-  }
+  const bool onem = L.kernel == PLAIN_C32_PACKED_1M_64x128 || L.kernel == PLAIN_C32_PACKED_1M_64x64;
+  if (L.kernel == PLAIN_F32_PACKED_128x128 || L.kernel == PLAIN_C32_PACKED_1M_64x128)
+    return onem ? run_simt_packed<true, 128>(g, L, pa, pb, splits, st) : run_simt_packed<false, 128>(g, L, pa, pb, splits, st);
+  if (L.kernel == PLAIN_F32_PACKED_128x64 || L.kernel == PLAIN_C32_PACKED_1M_64x64)
+    return onem ? run_simt_packed<true, 64>(g, L, pa, pb, splits, st) : run_simt_packed<false, 64>(g, L, pa, pb, splits, st);
   // K-major f64 panels: [planes * H * rows_pad] rows of k_pad doubles; boxes
   // of BM (BN) rows x 16 doubles (128 bytes), SWIZZLE_128B.
   const bool three = L.kernel == PLAIN_C64_PACKED_3M_64x32;

@@ -1058,6 +1058,8 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C32_PACKED_1M_64x128: return "sm100.c32.simt.tma.1m.64x128x16";
     case PLAIN_F64_PACKED_64x64: return "sm100.f64.dmma884.tma.packed.64x64x16";
     case PLAIN_C64_PACKED_3M_64x32: return "sm100.c64.dmma884.tma.3m.64x32x16";
+    case PLAIN_F32_PACKED_128x64: return "sm100.f32.simt.tma.packed.128x64x16";
+    case PLAIN_C32_PACKED_1M_64x64: return "sm100.c32.simt.tma.1m.64x64x16";
   }
   return "auto";
 }
@@ -1277,6 +1279,8 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_C32_PACKED_1M_64x128: *bm = 64; *bn = 128; return;
     case PLAIN_F64_PACKED_64x64: *bm = 64; *bn = 64; return;
     case PLAIN_C64_PACKED_3M_64x32: *bm = 64; *bn = 32; return;
+    case PLAIN_F32_PACKED_128x64: *bm = 128; *bn = 64; return;
+    case PLAIN_C32_PACKED_1M_64x64: *bm = 64; *bn = 64; return;
   }
   *bm = *bn = 0;
 }

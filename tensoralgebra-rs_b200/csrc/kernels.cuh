@@ -86,7 +86,9 @@ enum PlainKernel : int {
   PLAIN_C32_PACKED_1M_64x128 = 11,  // 1m: the complex product as a 2M x N x 2K real one
   PLAIN_F64_PACKED_64x64 = 12,
   PLAIN_C64_PACKED_3M_64x32 = 13,   // 3m: three real products per complex MAC
-  PLAIN_LAST = 13,
+  PLAIN_F32_PACKED_128x64 = 14,     // half-width FFMA tiles, two CTAs per SM
+  PLAIN_C32_PACKED_1M_64x64 = 15,
+  PLAIN_LAST = 15,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).

@@ -372,7 +372,8 @@ def test_autotune_candidates(tp):
     big = _gemm_product(tp, 4096, 4096, 4096, dt=0).report()["autotune_candidates"]
     assert big[0] == "sm100.f32.simt.tma.packed.128x128x16"  # the model: packed, a full wave of tiles
     assert sorted(big) == ["sm100.f32.simt.128x128x16", "sm100.f32.simt.64x64x16",
-                           "sm100.f32.simt.tma.packed.128x128x16"]  # enough tiles: no split
+                           "sm100.f32.simt.tma.packed.128x128x16",
+                           "sm100.f32.simt.tma.packed.128x64x16"]  # enough tiles: no split
     shallow = _gemm_product(tp, 64, 64, 128).report()["autotune_candidates"]
     assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
     c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]
@@ -509,7 +510,7 @@ def test_tuning_file_format_is_checked_without_a_gpu(tp, tmp_path):
                     "list list-0123456789abcdef-n3 2 1 1.5 3\n")
     assert tp.tuning_file_info(str(good)) == {"sms": 148, "device": "NVIDIA_B200", "single": 3, "list": 1}
     bad_lines = [
-        "single sig 14 1 0 0 1 0.1 1",    # no kernel family 14
+        "single sig 16 1 0 0 1 0.1 1",    # no kernel family 16
         "single sig 3 2 0 0 1 0.1 1",     # split without a chunk
         "single sig 3 65 64 0 1 0.1 1",   # more than 64 chunks
         "single sig 3 1 0 0 1 0.1",       # a field short

@@ -15,6 +15,7 @@ from test_gpu_parity import Op, make_product, oracle_ref, plain_tol, rnd, run
 pytestmark = pytest.mark.gpu
 
 PACKED = {"float32": 10, "complex64": 11, "float64": 12, "complex128": 13}
+HALF = {"float32": 14, "complex64": 15}  # the half-width FFMA tiles
 DTYPES = list(PACKED)
 
 
@@ -51,6 +52,45 @@ def test_packed_family_on_ragged_shapes(tp, ex, torch_cuda, orc, dt):
         assert st == 0, tp.last_error()
         assert p.report()["family"].startswith("sm100") and "tma" in p.report()["family"]
         assert orc.rel_frobenius(got, want) <= plain_tol(dt), (m, n, k, kfast)
+
+
+@pytest.mark.parametrize("dt", list(HALF))
+def test_half_width_ffma_tiles(tp, ex, torch_cuda, orc, dt):
+    """The 128 x 64 FFMA tiles (f32; c32 as 1m): ragged shapes of both operand
+    orders, conjugated A for c32, alpha / beta with C, and a split K."""
+    rng = np.random.default_rng(65)
+    for (m, n, k, kfast) in [(1, 1, 1, True), (65, 33, 17, False), (200, 129, 300, True), (129, 200, 33, False)]:
+        if kfast:
+            A = Op(rnd(rng, dt, m * k), [m, k], [k, 1], [0, 2], conj=dt == "complex64")
+            B = Op(rnd(rng, dt, k * n), [k, n], [1, k], [2, 1])
+        else:
+            A = Op(rnd(rng, dt, m * k), [m, k], [1, m], [0, 2])
+            B = Op(rnd(rng, dt, k * n), [k, n], [n, 1], [2, 1], conj=dt == "complex64")
+        C = Op(rnd(rng, dt, m * n), [m, n], [1, m], [0, 1])
+        d0 = np.zeros(m * n, dtype=dt)
+        D = Op(d0, [m, n], [1, m], [0, 1])
+        al, be = (complex(0.5, -0.25), complex(-1.5, 0.5)) if dt.startswith("complex") else (0.75, -1.5)
+        want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
+        st, got, p = run(tp, ex, torch_cuda, dt, A, B, C, D, al, be, kernel=HALF[dt])
+        assert st == 0, tp.last_error()
+        assert "x64x16" in p.report()["family"], p.report()["family"]
+        assert orc.rel_frobenius(got, want) <= plain_tol(dt), (m, n, k, kfast)
+    m, n, k = 96, 80, 1500
+    A = Op(rnd(rng, dt, m * k), [m, k], [1, m], [0, 2])
+    B = Op(rnd(rng, dt, k * n), [k, n], [1, k], [2, 1])
+    d0 = np.zeros(m * n, dtype=dt)
+    D = Op(d0, [m, n], [1, m], [0, 1])
+    want = oracle_ref(orc, dt, A, B, None, D, 1.0, 0.0, d0)
+    p = make_product(tp, dt, A, B, None, D)
+    p.set_kernel(HALF[dt])
+    p.set_split_k(3)
+    torch = torch_cuda
+    ta, tb = (torch.from_numpy(x.buf.copy()).cuda() for x in (A, B))
+    td = torch.from_numpy(d0.copy()).cuda()
+    assert p.execute(ex, 1.0, ta.data_ptr(), tb.data_ptr(), 0.0, None, td.data_ptr()) == 0, tp.last_error()
+    torch.cuda.synchronize()
+    assert p.report().get("split_k", 1) == 3
+    assert orc.rel_frobenius(td.cpu().numpy(), want) <= plain_tol(dt)
 
 
 @pytest.mark.parametrize("dt", DTYPES)

@@ -418,7 +418,10 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
   AsyncGather<double, CPLX, BM, BK, NT> ga;
   AsyncGather<double, CPLX, BN, BK, NT> gb;
 
-  double cr[TI][TJ][4], ci[CPLX ? TI : 1][CPLX ? TJ : 1][4];
+  // Complex tiles run 3m (kernels/reference/scalar.rs:136): cr = M1 = Ar Br,
+  // cm = M2 = Ai Bi, ci = M3 = (Ar + Ai)(Br + Bi), the sums formed from the
+  // fragments in registers; the epilogue takes (M1 - M2) + i (M3 - M1 - M2).
+  double cr[TI][TJ][4], ci[CPLX ? TI : 1][CPLX ? TJ : 1][4], cm[CPLX ? TI : 1][CPLX ? TJ : 1][4];
 #pragma unroll
   for (int i = 0; i < TI; ++i)
 #pragma unroll
@@ -426,7 +429,10 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         cr[i][j][q] = 0.0;
-        if (CPLX) ci[i][j][q] = 0.0;
+        if (CPLX) {
+          ci[i][j][q] = 0.0;
+          cm[i][j][q] = 0.0;
+        }
       }
 
   // This CTA's K range (the whole of K unless split).
@@ -467,7 +473,8 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
     const int buf = (int)(t % STAGES);
 #pragma unroll
     for (int ks = 0; ks < BK / 8; ++ks) {
-      double a_re[TI][4], b_re[TJ][2], a_im[CPLX ? TI : 1][4], na_im[CPLX ? TI : 1][4], b_im[CPLX ? TJ : 1][2];
+      double a_re[TI][4], b_re[TJ][2], a_im[CPLX ? TI : 1][4], a_sum[CPLX ? TI : 1][4], b_im[CPLX ? TJ : 1][2],
+          b_sum[CPLX ? TJ : 1][2];
 #pragma unroll
       for (int i = 0; i < TI; ++i)
 #pragma unroll
@@ -476,7 +483,7 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
           a_re[i][r] = As[buf][0][idx];
           if (CPLX) {
             a_im[i][r] = sa * As[buf][NPL - 1][idx];
-            na_im[i][r] = -a_im[i][r];
+            a_sum[i][r] = a_re[i][r] + a_im[i][r];
           }
         }
 #pragma unroll
@@ -485,7 +492,10 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
         for (int r = 0; r < 2; ++r) {
           const int idx = (ks * 8 + fk + 4 * r) * SB + wn0 + j * 8 + fr;
           b_re[j][r] = Bs[buf][0][idx];
-          if (CPLX) b_im[j][r] = sb * Bs[buf][NPL - 1][idx];
+          if (CPLX) {
+            b_im[j][r] = sb * Bs[buf][NPL - 1][idx];
+            b_sum[j][r] = b_re[j][r] + b_im[j][r];
+          }
         }
 #pragma unroll
       for (int i = 0; i < TI; ++i)
@@ -493,9 +503,8 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
         for (int j = 0; j < TJ; ++j) {
           dmma_1688(cr[i][j], a_re[i], b_re[j]);
           if (CPLX) {
-            dmma_1688(cr[i][j], na_im[i], b_im[j]);
-            dmma_1688(ci[i][j], a_re[i], b_im[j]);
-            dmma_1688(ci[i][j], a_im[i], b_re[j]);
+            dmma_1688(cm[i][j], a_im[i], b_im[j]);
+            dmma_1688(ci[i][j], a_sum[i], b_sum[j]);
           }
         }
     }
@@ -513,12 +522,13 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
         const int rr = wm0 + i * 16 + fr + 8 * (q >> 1);
         const int cc = wn0 + j * 8 + fk * 2 + (q & 1);
         if (m0 + rr >= g.M || n0 + cc >= g.N) continue;
+        const double re = CPLX ? cr[i][j][q] - cm[i][j][q] : cr[i][j][q];
+        const double im = CPLX ? ci[i][j][q] - cr[i][j][q] - cm[i][j][q] : 0.0;
         if (g.partial)
           Elem<double, CPLX>::store(static_cast<T*>(g.partial) + ((split * g.H + h) * g.N + n0 + cc) * g.M + m0 + rr,
-                                    cr[i][j][q], CPLX ? ci[i][j][q] : 0.0);
+                                    re, im);
         else
-          epilogue_store<double, CPLX>(g.e, cr[i][j][q], CPLX ? ci[i][j][q] : 0.0, Cb + cm_s[rr] + cn_s[cc],
-                                     Db + dm_s[rr] + dn_s[cc]);
+          epilogue_store<double, CPLX>(g.e, re, im, Cb + cm_s[rr] + cn_s[cc], Db + dm_s[rr] + dn_s[cc]);
       }
 }
 
@@ -912,9 +922,10 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_ring_gemm_kerne
 }
 
 // Three CTAs per SM (at most 170 registers a thread): twelve warps to hide the
-// gather and shared-memory latency around the DMMA pipe.
+// gather and shared-memory latency around the DMMA pipe; two for the tall
+// complex tile, whose three 3m accumulators need the registers.
 template <bool CPLX, int WM, int WN, int BK>
-__global__ void __launch_bounds__(128, 3) dmma_gemm_kernel(GemmArgs g) {
+__global__ void __launch_bounds__(128, (CPLX && WM == 64) ? 2 : 3) dmma_gemm_kernel(GemmArgs g) {
   constexpr int BM = 2 * WM, BN = 2 * WN;
   const int64_t tn = (g.N + BN - 1) / BN, tm = (g.M + BM - 1) / BM;
   const int64_t total = tn * tm * g.H * (g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1);

@@ -204,6 +204,28 @@ struct SpCfg {
   static constexpr int SMEM = 1024 + STAGES * STAGE + (2 * BM + 2 * BN) * 8 + 2 * STAGES * 8 + 16;
 };
 
+// Packed pairs of FP32 values (sm_100 f32x2 arithmetic; each half rounds as
+// its own IEEE operation).
+__device__ __forceinline__ unsigned long long f32x2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f32x2_unpack(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f32x2_fma(unsigned long long a, unsigned long long b,
+                                                        unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f32x2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
 // Stores four consecutive rows of one column when D's rows are consecutive in
 // memory and the address is 16-byte aligned (the reference's unit-stride
 // write-back, pack/writeback.rs:426-486); returns false when it did not.
@@ -290,13 +312,16 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
     }
   } else {
     const int tx = tid & 15, ty = tid >> 4;
-    float tot[8][TN], acc[8][TN];
+    // Accumulators in packed pairs of rows (fma.rn.f32x2: two IEEE FMAs per
+    // instruction, half the issue slots of scalar FFMA): pair p holds rows
+    // 2p and 2p + 1 of the thread's eight rows for one column.
+    unsigned long long totp[4][TN], accp[4][TN];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int p = 0; p < 4; ++p)
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
-        tot[i][j] = 0.f;
-        acc[i][j] = 0.f;
+        totp[p][j] = 0ull;
+        accp[p][j] = 0ull;
       }
     for (int i = 0; i < nk; ++i) {
       const int s = i % STAGES;
@@ -310,39 +335,40 @@ simt_packed_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
       const float* Bs = reinterpret_cast<const float*>(ring + s * Cfg::STAGE + Cfg::A);
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
-        const float4 a0 = *reinterpret_cast<const float4*>(As + kk * BM + tx * 4);
-        const float4 a1 = *reinterpret_cast<const float4*>(As + kk * BM + 64 + tx * 4);
-        float br[TN];
+        const ulonglong2 a0 = *reinterpret_cast<const ulonglong2*>(As + kk * BM + tx * 4);
+        const ulonglong2 a1 = *reinterpret_cast<const ulonglong2*>(As + kk * BM + 64 + tx * 4);
+        const unsigned long long ap[4] = {a0.x, a0.y, a1.x, a1.y};
+        unsigned long long bd[TN];  // each column value duplicated into both halves
 #pragma unroll
         for (int c = 0; c < CG; ++c) {
           const float4 b = *reinterpret_cast<const float4*>(Bs + kk * BN + 64 * c + ty * 4);
-          br[4 * c] = b.x;
-          br[4 * c + 1] = b.y;
-          br[4 * c + 2] = b.z;
-          br[4 * c + 3] = b.w;
+          bd[4 * c] = f32x2_pack(b.x, b.x);
+          bd[4 * c + 1] = f32x2_pack(b.y, b.y);
+          bd[4 * c + 2] = f32x2_pack(b.z, b.z);
+          bd[4 * c + 3] = f32x2_pack(b.w, b.w);
         }
-        const float ar[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
-        for (int ii = 0; ii < 8; ++ii)
+        for (int p = 0; p < 4; ++p)
 #pragma unroll
-          for (int jj = 0; jj < TN; ++jj) acc[ii][jj] = fmaf(ar[ii], br[jj], acc[ii][jj]);
+          for (int jj = 0; jj < TN; ++jj) accp[p][jj] = f32x2_fma(ap[p], bd[jj], accp[p][jj]);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
       if ((i + 1) % Cfg::FLUSH == 0) {
 #pragma unroll
-        for (int ii = 0; ii < 8; ++ii)
+        for (int p = 0; p < 4; ++p)
 #pragma unroll
           for (int jj = 0; jj < TN; ++jj) {
-            tot[ii][jj] += acc[ii][jj];
-            acc[ii][jj] = 0.f;
+            totp[p][jj] = f32x2_add(totp[p][jj], accp[p][jj]);
+            accp[p][jj] = 0ull;
           }
       }
     }
+    float tot[8][TN];
 #pragma unroll
-    for (int ii = 0; ii < 8; ++ii)
+    for (int p = 0; p < 4; ++p)
 #pragma unroll
-      for (int jj = 0; jj < TN; ++jj) tot[ii][jj] += acc[ii][jj];
+      for (int jj = 0; jj < TN; ++jj) f32x2_unpack(f32x2_add(totp[p][jj], accp[p][jj]), tot[2 * p][jj], tot[2 * p + 1][jj]);
 
     // Epilogue. Thread rows: tx*4 + [0,4) and 64 + tx*4 + [0,4); columns
     // 64 c + ty*4 + [0,4) for each group c.

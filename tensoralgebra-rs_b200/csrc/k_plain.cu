@@ -959,16 +959,19 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
   const int64_t total = tile_start[nitems];
   const uint64_t t_start = globaltimer_ns();
   constexpr uint64_t LIMIT_NS = 60000000000ull;  // 60 s for one grouped launch
+  // The claim of the next tile is issued before the current tile runs (its
+  // result is first used after the tile), so the atomic's round trip overlaps
+  // the tile instead of adding to it.
+  long long next = 0;
+  if (threadIdx.x == 0) next = (long long)atomicAdd(counter, 1ull);
   for (int64_t iter = 0;; ++iter) {
     if (threadIdx.x < 32) {
-      // Claim a tile, then find the item whose tile range holds it (the last
-      // index with tile_start <= claimed) by a 32-way search across the warp:
-      // each round probes 32 evenly spaced entries at once, so a list of n
-      // items costs about log32(n) dependent loads instead of log2(n).
+      // Find the item whose tile range holds the claimed tile (the last index
+      // with tile_start <= claimed) by a 32-way search across the warp: each
+      // round probes 32 evenly spaced entries at once, so a list of n items
+      // costs about log32(n) dependent loads instead of log2(n).
       const int lane = threadIdx.x;
-      long long c = 0;
-      if (lane == 0) c = (long long)atomicAdd(counter, 1ull);
-      c = __shfl_sync(0xffffffffu, c, 0);
+      const long long c = __shfl_sync(0xffffffffu, next, 0);
       int lo = 0, hi = nitems - 1;
       while (lo < hi) {
         const int step = (hi - lo + 32) / 32;
@@ -1001,6 +1004,7 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
     __syncthreads();
     const long long t = claimed;
     if (t >= total || stop) break;
+    if (threadIdx.x == 0) next = (long long)atomicAdd(counter, 1ull);
     const int it = item_s;
     if (it != sg_item) {  // uniform: both values were written before the barrier above
       const int4* src = reinterpret_cast<const int4*>(&items[it].g);

@@ -872,9 +872,20 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   const Axis& ca = nax.back();
   const int64_t E = ca.extent;
   if (E < 2) return false;
-  const int nchunks = (int)std::min<int64_t>(E, 4);
+  // Chunks that halve in size (E/2, E/4, ... down to about E/16, the rest
+  // last): the call ends with the kernels and the copy out of the last chunk
+  // only, so a small last chunk shortens that tail while the large first ones
+  // keep the kernels efficient. Every chunk keeps at least 256 columns.
   const int64_t inner_n = v.N / E;
-  if (v.N / nchunks < 256) return false;
+  std::vector<int64_t> bounds{0};
+  while (bounds.back() < E) {
+    const int64_t left = E - bounds.back();
+    int64_t take = left / 2;
+    if (take * 16 < E || take * inner_n < 256 || (left - take) * inner_n < 256) take = left;
+    bounds.push_back(bounds.back() + take);
+  }
+  const int nchunks = (int)bounds.size() - 1;
+  if (nchunks < 2 || nchunks > 8) return false;
   const auto stride_in = [](const Axis& a, int slot) {
     return slot == SA ? a.sa : slot == SB ? a.sb : slot == SC ? a.sc : a.sd;
   };
@@ -888,8 +899,8 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   std::vector<std::vector<ChunkCopy>> bcp(nchunks), dcp(nchunks);
   std::vector<int64_t> lo(nchunks), hi(nchunks);
   for (int c = 0; c < nchunks; ++c) {
-    lo[c] = E * c / nchunks;
-    hi[c] = E * (c + 1) / nchunks;
+    lo[c] = bounds[c];
+    hi[c] = bounds[c + 1];
     if (!chunk_copies(others(sx), stride_in(ca, sx), E, lo[c], hi[c], elem, bcp[c]) ||
         !chunk_copies(others(SD), stride_in(ca, SD), E, lo[c], hi[c], elem, dcp[c]))
       return false;

@@ -1065,10 +1065,10 @@ const char* plain_kernel_name(int k) {
     case PLAIN_F64_DMMA_64x64: return "sm100.f64.dmma884.64x64x16";
     case PLAIN_F64_DMMA_32x32: return "sm100.f64.dmma884.32x32x16";
     case PLAIN_C32_SIMT_64x64: return "sm100.c32.simt.ring.planar.64x64x16";
-    case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.planar.64x32x8";
-    case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.planar.32x32x8";
+    case PLAIN_C64_DMMA_64x32: return "sm100.c64.dmma884.3m.64x32x8";
+    case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.3m.32x32x8";
     case PLAIN_F64_DMMA_128x32: return "sm100.f64.dmma884.128x32x16";
-    case PLAIN_C64_DMMA_128x32: return "sm100.c64.dmma884.planar.128x32x8";
+    case PLAIN_C64_DMMA_128x32: return "sm100.c64.dmma884.3m.128x32x8";
     case PLAIN_F32_PACKED_128x128: return "sm100.f32.simt.tma.packed.128x128x16";
     case PLAIN_C32_PACKED_1M_64x128: return "sm100.c32.simt.tma.1m.64x128x16";
     case PLAIN_F64_PACKED_64x64: return "sm100.f64.dmma884.tma.packed.64x64x16";
@@ -1092,7 +1092,7 @@ int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, i
   auto tiles = [&](int bm, int bn) { return ((M + bm - 1) / bm) * ((N + bn - 1) / bn) * H; };
   // At least a full wave of packed tiles and some depth: the pack pass (one
   // read and one write of each operand) is then small beside the tiles' work.
-  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x128,
+  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x64,
                                 PLAIN_C64_PACKED_3M_64x32};
   {
     const int pk = packed[dtype & 3];
@@ -1143,7 +1143,7 @@ void choose_plain_launch(int dtype, int pinned, int64_t M, int64_t N, int64_t K,
   };
   static const int large[4] = {PLAIN_F32_SIMT_128x128, PLAIN_F64_DMMA_64x64, PLAIN_C32_SIMT_64x64,
                                PLAIN_C64_DMMA_64x32};
-  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x128,
+  static const int packed[4] = {PLAIN_F32_PACKED_128x128, PLAIN_F64_PACKED_64x64, PLAIN_C32_PACKED_1M_64x64,
                                 PLAIN_C64_PACKED_3M_64x32};
   *splits = 1;
   *k_chunk = 0;

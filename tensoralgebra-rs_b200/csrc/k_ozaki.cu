@@ -232,12 +232,12 @@ template <bool CPLX>
 __global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __restrict__ X, const int64_t* rows_scat,
                                                               const int64_t* k_scat, const int64_t* h_scat,
                                                               int64_t nrows, int64_t K, int64_t rows_pad, int64_t H,
-                                                              int64_t row0, int* __restrict__ out) {
+                                                              int* __restrict__ out) {
   // One CTA per (row, 32 batch entries); the 8 warps split k and combine in
-  // shared memory. Rows row0 + blockIdx.x.
+  // shared memory.
   __shared__ unsigned long long red[8][32];
   const int hl = threadIdx.x & 31, kp = threadIdx.x >> 5;
-  const int64_t r = row0 + blockIdx.x, h = (int64_t)blockIdx.y * 32 + hl;
+  const int64_t r = blockIdx.x, h = (int64_t)blockIdx.y * 32 + hl;
   unsigned long long best = 0ull;
   if (r < nrows && h < H) {
     const double* base = X + (CPLX ? 2 : 1) * (h_scat[h] + rows_scat[r]);
@@ -269,11 +269,10 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_kernel(const double* __
                                                                 const int64_t* k_scat, const int64_t* h_scat,
                                                                 const int* __restrict__ exps, int64_t nrows, int64_t K,
                                                                 int64_t rows_pad, int64_t exp_pad, int64_t k_pad,
-                                                                int64_t H, int S, int64_t row0,
-                                                                int8_t* __restrict__ out) {
+                                                                int64_t H, int S, int8_t* __restrict__ out) {
   __shared__ double tile[32][65];
   const int tid = threadIdx.x;
-  const int64_t k0 = (int64_t)blockIdx.x * 64, r = row0 + blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
+  const int64_t k0 = (int64_t)blockIdx.x * 64, r = blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
   {
     const int hl = tid & 31;
     const int64_t h = h0 + hl;
@@ -307,10 +306,10 @@ template <int WHICH>
 __global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
     const double* __restrict__ X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
     const int* __restrict__ exps, int64_t nrows, int64_t K, int64_t Kh, int64_t rows_pad, int64_t exp_pad,
-    int64_t k_pad, int64_t H, int conj, int S, int64_t row0, int8_t* __restrict__ out) {
+    int64_t k_pad, int64_t H, int conj, int S, int8_t* __restrict__ out) {
   __shared__ double t_re[32][65], t_im[32][65];
   const int tid = threadIdx.x;
-  const int64_t k0 = (int64_t)blockIdx.x * 64, r = row0 + blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
+  const int64_t k0 = (int64_t)blockIdx.x * 64, r = blockIdx.y, h0 = (int64_t)blockIdx.z * 32;
   {
     const int hl = tid & 31;
     const int64_t h = h0 + hl;
@@ -705,37 +704,22 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
                          int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
                          int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
   if (hfast) {
-    // The scan and the slicing both read the operand; they run on groups of
-    // rows whose source data (about 48 MB) stays in L2 between the two, so the
-    // slicing's read is served from L2 instead of HBM.
-    const int64_t crows = CPLX ? (which == 0 ? rows_pad / 2 : rows_pad) : rows_pad;  // sliced rows
-    const int64_t all = exp_pad > crows ? exp_pad : crows;
-    const int64_t row_bytes = K * L.H * (CPLX ? 16 : 8);
-    int64_t group = row_bytes > 0 ? ((int64_t)48 << 20) / row_bytes : all;
-    group = group < 1 ? 1 : (group > all ? all : group);
-    for (int64_t r0 = 0; r0 < all; r0 += group) {
-      const int64_t e1 = r0 + group < exp_pad ? r0 + group : exp_pad;
-      if (e1 > r0)
-        ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)(e1 - r0), (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
-            X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, r0, exps);
-      const int64_t s1 = r0 + group < crows ? r0 + group : crows;
-      if (s1 <= r0) continue;
-      if constexpr (CPLX) {
-        // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
-        const dim3 grid((unsigned)(L.k_half / 64), (unsigned)(s1 - r0), (unsigned)((L.H + 31) / 32));
-        if (which == 0)
-          ozaki_slice_hfast_c64_kernel<0><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half,
-                                                                 rows_pad, exp_pad, L.k_pad, L.H, conj, L.slices, r0,
-                                                                 planes);
-        else
-          ozaki_slice_hfast_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half,
-                                                                 rows_pad, exp_pad, L.k_pad, L.H, conj, L.slices, r0,
-                                                                 planes);
-      } else {
-        ozaki_slice_hfast_kernel<<<dim3((unsigned)(L.k_pad / 64), (unsigned)(s1 - r0), (unsigned)((L.H + 31) / 32)),
-                                   256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, rows_pad, exp_pad, L.k_pad, L.H,
-                                                 L.slices, r0, planes);
-      }
+    ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
+        X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);
+    if constexpr (CPLX) {
+      // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
+      const dim3 grid((unsigned)(L.k_half / 64), (unsigned)(which == 0 ? rows_pad / 2 : rows_pad),
+                      (unsigned)((L.H + 31) / 32));
+      if (which == 0)
+        ozaki_slice_hfast_c64_kernel<0><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                               exp_pad, L.k_pad, L.H, conj, L.slices, planes);
+      else
+        ozaki_slice_hfast_c64_kernel<1><<<grid, 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, L.k_half, rows_pad,
+                                                               exp_pad, L.k_pad, L.H, conj, L.slices, planes);
+    } else {
+      ozaki_slice_hfast_kernel<<<dim3((unsigned)(L.k_pad / 64), (unsigned)rows_pad, (unsigned)((L.H + 31) / 32)),
+                                 256, 0, st>>>(X, rows_s, k_s, h_s, exps, nrows, K, rows_pad, exp_pad, L.k_pad, L.H,
+                                               L.slices, planes);
     }
   } else {
     ozaki_exp_kernel<CPLX><<<dim3((unsigned)((nrows + 31) / 32), (unsigned)L.H), 256, 0, st>>>(

@@ -731,7 +731,7 @@ def run_config(args, tp, torch, ex):
                 prob = tp.Problem.from_labels(tdt, tp.OperandSpec(tp.LayoutSpec.col_major(ea)),
                                               tp.OperandSpec(tp.LayoutSpec.col_major(eb), conj_b),
                                               tp.OperandSpec(tp.LayoutSpec.col_major(ed)), la, lb, ld)
-                plans[key] = tp.Plan(prob)
+                plans[key] = tp.Plan(prob, tp.PlanConfig(autotune=not args.no_autotune))
             return plans[key]
 
         dev, lists = [], [[], [], []]
@@ -771,6 +771,12 @@ def run_config(args, tp, torch, ex):
             got = dev[i]["Ep"].cpu().numpy().reshape((it["a"], it["s"], it["b"]), order="F")
             worst = max(worst, float(np.linalg.norm(got - want) / np.linalg.norm(want)))
         out["rel_err_sampled_items"] = worst
+        if not args.no_autotune:
+            pol = {}
+            for e in ex.tuning().get("list", {}).values():
+                pol[str(e.get("policy"))] = pol.get(str(e.get("policy")), 0) + 1
+            out["grouped"]["autotune"] = {"list_policies": pol, "policy_names": {"0": "per-item model", "1": "large",
+                                                                                 "2": "small", "3": "tall for N<=32"}}
         out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
         # Per binary step (grouped), and the mixed roofline of the list: each
         # item-step bounded by max(flops / FP64 DMMA peak, bytes / HBM peak).
@@ -911,6 +917,7 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="time the metric's workload only (no C1, C3-C5 records)")
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
+    ap.add_argument("--no-autotune", action="store_true", help="config 4: the model's tiles instead of autotuned ones")
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
     ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
     ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")

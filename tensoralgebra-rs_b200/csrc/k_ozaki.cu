@@ -36,7 +36,8 @@ using namespace tc;
 
 constexpr int OZ_BM = 128;
 constexpr int OZ_BN = 64;
-constexpr int OZ_BK = 64;  // INT8 per stage row: 64 bytes = one SWIZZLE_64B atom
+constexpr int OZ_BK = 64;  // depth unit of the slice planes' padding and of the host's K chunks
+constexpr int OZ_SK = 64;  // INT8 depth of one ring stage: 64-byte rows (SWIZZLE_64B), two MMAs deep
 constexpr int EXP_NONFINITE = INT_MAX;
 
 __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
@@ -56,8 +57,8 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
 // exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
 // of x, are the slices: the same digits as repeatedly multiplying the scaled
 // value by 128 and removing the integer part. Digits are cut from the 32-bit
-// halves of |T| (a funnel shift across the boundary), packed four to a word,
-// and negated bytewise where x < 0: for a byte b <= 127,
+// halves of |T| (a funnel shift across the boundary), packed four to a word
+// by byte permutes, and negated bytewise where x < 0: for a byte b <= 127,
 // ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
 template <int S>
 __device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[8]) {
@@ -77,15 +78,17 @@ __device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[
 #pragma unroll
   for (int sl = 0; sl < S; ++sl) {
     const int sh = 7 * (S - 1 - sl);
-    uint32_t w = 0;
+    uint32_t d[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      uint32_t d;
-      if (sh + 7 <= 32) d = lo[q] >> sh;
-      else if (sh >= 32) d = hi[q] >> (sh - 32);
-      else d = __funnelshift_r(lo[q], hi[q], sh);
-      w |= (d & 127u) << (8 * q);
+      if (sh + 7 <= 32) d[q] = lo[q] >> sh;
+      else if (sh >= 32) d[q] = hi[q] >> (sh - 32);
+      else d[q] = __funnelshift_r(lo[q], hi[q], sh);
     }
+    // Low bytes of d[0..3] into one word (three byte permutes), then the
+    // 7-bit digits.
+    const uint32_t p01 = __byte_perm(d[0], d[1], 0x0040), p23 = __byte_perm(d[2], d[3], 0x0040);
+    const uint32_t w = __byte_perm(p01, p23, 0x5410) & 0x7f7f7f7fu;
     out[sl] = (w & ~negmask) | (neg_bytes(w) & negmask);
   }
 }
@@ -137,6 +140,17 @@ __device__ inline void write_slices(const double (&x)[4], int e, int S, int8_t* 
   }
 }
 
+// Bit pattern of |x|: ordered like |x| for finite values, and every inf or
+// NaN (of either part of a complex value) compares at or above 0x7ff0...0, so
+// one integer max over a row finds both its largest magnitude and whether it
+// holds a non-finite entry.
+__device__ __forceinline__ unsigned long long mag_bits(double x) {
+  return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+}
+__device__ __forceinline__ unsigned long long max_bits(unsigned long long a, unsigned long long b) {
+  return a > b ? a : b;
+}
+
 // Per row (complex: per complex row) exponent e with max |x| < 2^e; a row with
 // a non-finite entry gets EXP_NONFINITE. One CTA per 32 rows, looping over K.
 template <bool CPLX>
@@ -164,10 +178,8 @@ __global__ void __launch_bounds__(256) ozaki_exp_kernel(const double* __restrict
       const int64_t r = r0 + rr, k = k0 + kk;
       if (r < nrows && k < K) {
         const double* e = X + (CPLX ? 2 : 1) * (hoff + rows_scat[r] + k_scat[k]);
-        double m = fabs(e[0]);
-        if (CPLX) m = fmax(m, fabs(e[1]));
-        if (!(m <= 1.79769313486231570e308)) m = __longlong_as_double(0x7ff0000000000000ll);  // inf or NaN
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+        unsigned long long bits = mag_bits(e[0]);
+        if (CPLX) bits = max_bits(bits, mag_bits(e[1]));
         if (bits > local[j]) local[j] = bits;
       }
     }
@@ -244,10 +256,8 @@ __global__ void __launch_bounds__(256) ozaki_exp_hfast_kernel(const double* __re
 #pragma unroll 4
     for (int64_t k = kp; k < K; k += 8) {
       const double* e = base + (CPLX ? 2 : 1) * __ldg(k_scat + k);
-      double m = fabs(e[0]);
-      if (CPLX) m = fmax(m, fabs(e[1]));
-      if (!(m <= 1.79769313486231570e308)) m = __longlong_as_double(0x7ff0000000000000ll);  // inf or NaN
-      const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+      unsigned long long bits = mag_bits(e[0]);
+      if (CPLX) bits = max_bits(bits, mag_bits(e[1]));
       if (bits > best) best = bits;
     }
   }
@@ -354,6 +364,133 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
   }
 }
 
+// One pass over a batch-innermost operand: a CTA holds OZ_HB batch entries of
+// one row, all of K, in shared memory, takes their exponents there and slices
+// them, so the operand is read from HBM once instead of once by the scan and
+// once by the slicing. The row's k offsets are staged in shared memory first;
+// then every element copy of the CTA is issued at once (cp.async, 16 bytes
+// per complex element when the operand is 16-byte aligned) and waited for
+// together, so a CTA keeps its whole block in flight. Shared layout
+// t[hl][swz(k)] (complex: re, im interleaved): the copies (8 lanes on 8 batch
+// entries at each of 4 k) and the slicing reads (lanes on consecutive quads
+// of k) both fall on distinct bank slots up to the width of a wavefront; swz
+// only permutes k inside its aligned group of four.
+constexpr int OZ_HB = 8;
+constexpr int OZ_PACK_THREADS = 128;
+
+__device__ __forceinline__ int64_t oz_swz(int64_t k) { return k ^ ((k >> 4) & 3); }
+
+// Row stride of t in elements: odd for 16-byte complex elements (8 slots per
+// wavefront), 4 mod 16 for 8-byte real ones (16 slots).
+__host__ __device__ inline int64_t oz_hfast_stride(bool cplx, int64_t K) {
+  return cplx ? (K + 3) / 4 * 4 + 1 : (K + 15) / 16 * 16 + 4;
+}
+
+__device__ __forceinline__ void oz_cp16(void* s, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void oz_cp8(void* s, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(s)), "l"(g) : "memory");
+}
+
+template <bool CPLX, int WHICH>
+__global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
+    const double* __restrict__ X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
+    int64_t nrows, int64_t crows, int64_t K, int64_t kw, int64_t rows_pad, int64_t exp_pad, int64_t k_pad,
+    int64_t Kh, int64_t H, int conj, int S, int vec16, int* __restrict__ exps, int8_t* __restrict__ out) {
+  constexpr int EW = CPLX ? 2 : 1;  // doubles per element
+  constexpr int KL = OZ_PACK_THREADS / OZ_HB;  // k lanes of the copy phase
+  extern __shared__ __align__(16) double oz_t[];
+  __shared__ unsigned long long red[KL][OZ_HB];
+  __shared__ int ex_s[OZ_HB];
+  const int tid = threadIdx.x, hl = tid % OZ_HB, kp = tid / OZ_HB;
+  const int64_t ks = oz_hfast_stride(CPLX, K);
+  int64_t* koff = reinterpret_cast<int64_t*>(oz_t + EW * OZ_HB * ks);
+  const int64_t r = blockIdx.x, h0 = (int64_t)blockIdx.y * OZ_HB;
+  for (int64_t k = tid; k < K; k += OZ_PACK_THREADS) koff[k] = k_scat[k];
+  __syncthreads();
+  const bool live = r < nrows && h0 + hl < H;
+  if (live) {
+    const double* base = X + EW * (h_scat[h0 + hl] + rows_scat[r]);
+    double* trow = oz_t + EW * hl * ks;
+#pragma unroll 4
+    for (int64_t k = kp; k < K; k += KL) {
+      const double* e = base + EW * koff[k];
+      double* sd = trow + EW * oz_swz(k);
+      if (CPLX && vec16) {
+        oz_cp16(sd, e);
+      } else {
+        oz_cp8(sd, e);
+        if (CPLX) oz_cp8(sd + 1, e + 1);
+      }
+    }
+  }
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;\n" ::: "memory");
+  unsigned long long best = 0ull;
+  if (live) {
+    const double* trow = oz_t + EW * hl * ks;
+    for (int64_t k = kp; k < K; k += KL) {
+      const double* sd = trow + EW * oz_swz(k);
+      unsigned long long bits = mag_bits(sd[0]);
+      if constexpr (CPLX) bits = max_bits(bits, mag_bits(sd[1]));
+      best = bits > best ? bits : best;
+    }
+  }
+  red[kp][hl] = best;
+  __syncthreads();
+  if (tid < OZ_HB) {
+    unsigned long long b = red[0][tid];
+#pragma unroll
+    for (int j = 1; j < KL; ++j) b = red[j][tid] > b ? red[j][tid] : b;
+    int e = 0;
+    if (b >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
+    else if (b != 0ull) frexp(__longlong_as_double((long long)b), &e);
+    ex_s[tid] = e;
+    if (h0 + tid < H && r < exp_pad) exps[(h0 + tid) * exp_pad + r] = e;
+  }
+  __syncthreads();
+  if (r >= crows) return;
+  const int64_t nq = kw / 4, plane = H * rows_pad * k_pad;
+  const double sgn = conj ? -1.0 : 1.0;
+  for (int64_t it = tid; it < OZ_HB * nq; it += OZ_PACK_THREADS) {
+    const int hh = (int)(it / nq);
+    const int64_t kq = (it - hh * nq) * 4, h = h0 + hh;
+    if (h >= H) break;
+    const int e = ex_s[hh];
+    double re[4], im[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t k = kq + q;
+      const bool in = k < K && e != EXP_NONFINITE && r < nrows;
+      const double* sd = oz_t + EW * (hh * ks + oz_swz(k));
+      if constexpr (CPLX) {
+        const double2 v = in ? *reinterpret_cast<const double2*>(sd) : make_double2(0.0, 0.0);
+        re[q] = v.x;
+        im[q] = sgn * v.y;
+      } else {
+        re[q] = in ? sd[0] : 0.0;
+      }
+    }
+    if constexpr (!CPLX) {
+      write_slices(re, e, S, out + (h * rows_pad + r) * k_pad + kq, plane);
+    } else if constexpr (WHICH == 0) {
+      int8_t* o0 = out + (h * rows_pad + 2 * r) * k_pad + kq;
+      write_slices_a(re, im, e, S, o0, o0 + k_pad, Kh, plane);
+    } else {
+      int8_t* o0 = out + (h * rows_pad + r) * k_pad + kq;
+      write_slices(re, e, S, o0, plane);
+      write_slices(im, e, S, o0 + Kh, plane);
+    }
+  }
+}
+
+// Shared memory of the one-pass kernel (the block and the row's k offsets);
+// it runs when two CTAs fit on an SM (four at the C3 depth of 384).
+inline size_t oz_hfast_smem(bool cplx, int64_t K) {
+  return (size_t)(cplx ? 2 : 1) * OZ_HB * oz_hfast_stride(cplx, K) * 8 + (size_t)K * 8;
+}
+constexpr size_t OZ_HFAST_SMEM_MAX = 100 * 1024;
+
 // Complex slicing for the general layouts (rows or k unit-stride): one load
 // of a complex element writes all of its embedded values, as in the
 // batch-innermost kernel above. One CTA per (32 complex rows, 64 k, batch
@@ -415,10 +552,12 @@ __global__ void __launch_bounds__(256) ozaki_slice_c64_kernel(
 
 template <int S>
 struct OzCfg {
-  static constexpr int A_TILE = OZ_BM * OZ_BK;  // bytes of one A plane tile
-  static constexpr int B_TILE = OZ_BN * OZ_BK;
+  static constexpr int A_TILE = OZ_BM * OZ_SK;  // bytes of one A plane tile
+  static constexpr int B_TILE = OZ_BN * OZ_SK;
   static constexpr int STAGE = S * (A_TILE + B_TILE);
-  static constexpr int STAGES = (S <= 6) ? 3 : 2;
+  // As many stages as fit in about 200 KB (2 at seven slices; 32-deep
+  // stages of 32-byte rows, twice as many, measured slower on B200).
+  static constexpr int STAGES = (200 * 1024 / STAGE) < 6 ? (200 * 1024 / STAGE) : 6;
   static constexpr int RING = STAGES * STAGE;
   static constexpr int BAR = (2 * STAGES + 2) * 8 + 16;
   static constexpr int SMEM = 1024 + RING + BAR;
@@ -459,7 +598,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tmem_empty + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nk = kb1 - kb0;
+  const int nk = (kb1 - kb0) * (OZ_BK / OZ_SK);  // ring stages per tile
   const int64_t tiles_n = n_pad / OZ_BN, tiles_m = m_pad / OZ_BM;
   const int64_t ntiles = tiles_n * tiles_m * g.H;
 
@@ -499,7 +638,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
           }
           mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
           uint8_t* sbase = ring + st * Cfg::STAGE;
-          const int kx = (kb0 + i) * OZ_BK;
+          const int kx = kb0 * OZ_BK + i * OZ_SK;
 #pragma unroll
           for (int p = 0; p < S; ++p)
             tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + mt * OZ_BM));
@@ -512,7 +651,6 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t IDESC = idesc_i8(OZ_BM, OZ_BN);
       uint32_t it = 0, j = 0;
       bool alive = true;
       for (int64_t tile = blockIdx.x; alive && tile < ntiles; tile += gridDim.x, ++j) {
@@ -532,16 +670,24 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
           }
           tc_fence_after();
           const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+          // A slice t meets B slices u = 0 .. S-1-t, whose diagonals t + u
+          // are the consecutive TMEM column blocks from t * 64 on, and whose
+          // tiles are consecutive 64-row blocks of one K-major operand in
+          // the stage. So one MMA takes a run of up to four B slices (N up
+          // to 256): S(S+1)/2 products in about 2S instructions, each
+          // reading the A tile once for all the slices it meets. The t = 0
+          // MMAs cover every diagonal and start them on the first k-block.
 #pragma unroll
-          for (int gd = 0; gd < S; ++gd) {
+          for (int t = 0; t < S; ++t) {
+            const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
 #pragma unroll
-            for (int t = 0; t <= gd; ++t) {
-              const int u = gd - t;
-              const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
-              const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u * Cfg::B_TILE);
+            for (int u0 = 0; u0 < S - t; u0 += 4) {
+              const int cnt = (S - t - u0) < 4 ? (S - t - u0) : 4;
+              const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN * cnt);
+              const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u0 * Cfg::B_TILE);
 #pragma unroll
-              for (int kk = 0; kk < OZ_BK / 32; ++kk)
-                umma_i8(tmem + (uint32_t)(gd * OZ_BN), ad + 2 * kk, bd + 2 * kk, IDESC,
+              for (int kk = 0; kk < OZ_SK / 32; ++kk)
+                umma_i8(tmem + (uint32_t)((t + u0) * OZ_BN), ad + 2 * kk, bd + 2 * kk, idesc,
                         (i | t | kk) != 0 ? 1u : 0u);
             }
           }
@@ -639,9 +785,11 @@ cudaError_t run_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ap, co
                      const int* eb, int kb0, int kb1, cudaStream_t st) {
   using Cfg = OzCfg<S>;
   CUtensorMap ma, mb;
-  if (!make_map_2d(&ma, ap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.m_pad, OZ_BK, OZ_BM))
+  if (!make_map_2d(&ma, ap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.m_pad, OZ_SK, OZ_BM,
+                   CU_TENSOR_MAP_SWIZZLE_64B))
     return cudaErrorInvalidValue;
-  if (!make_map_2d(&mb, bp, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.n_pad, OZ_BK, OZ_BN))
+  if (!make_map_2d(&mb, bp, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L.k_pad, (int64_t)S * L.H * L.n_pad, OZ_SK, OZ_BN,
+                   CU_TENSOR_MAP_SWIZZLE_64B))
     return cudaErrorInvalidValue;
   cudaError_t e =
       cudaFuncSetAttribute(ozaki_gemm_kernel<S, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
@@ -703,7 +851,19 @@ template <bool CPLX>
 static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* k_s, const int64_t* h_s, int64_t nrows,
                          int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
                          int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
-  if (hfast) {
+  const size_t one_pass = oz_hfast_smem(CPLX, K);
+  if (hfast && one_pass <= OZ_HFAST_SMEM_MAX) {
+    // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
+    const int64_t crows = CPLX && which == 0 ? rows_pad / 2 : rows_pad;
+    const int64_t rows = exp_pad > crows ? exp_pad : crows;
+    const dim3 grid((unsigned)rows, (unsigned)((L.H + OZ_HB - 1) / OZ_HB));
+    const int64_t kw = CPLX ? L.k_half : L.k_pad;
+    const int vec16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0 ? 1 : 0;
+    auto kern = which == 0 ? ozaki_pack_hfast_kernel<CPLX, 0> : ozaki_pack_hfast_kernel<CPLX, 1>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one_pass);
+    kern<<<grid, OZ_PACK_THREADS, one_pass, st>>>(X, rows_s, k_s, h_s, nrows, crows, K, kw, rows_pad, exp_pad,
+                                                  L.k_pad, L.k_half, L.H, conj, L.slices, vec16, exps, planes);
+  } else if (hfast) {
     ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);
     if constexpr (CPLX) {

@@ -42,10 +42,25 @@ struct TileGather {
   R im[CPLX ? PER : 1];
   int64_t var[PER];  // kfast: row offsets; otherwise: k offsets of the next stage
   int64_t fixed;     // kfast: k offset of the next stage; otherwise: the row offset
+  // k-fast operands: a warp covers RS rows x KQ consecutive k (the same
+  // spread over the shared-memory banks as AsyncGather below).
+  static constexpr int KQ = sizeof(R) == 4 ? 8 : 4, RS = 32 / KQ;
+  static constexpr bool WIDE = BK % KQ == 0 && ROWS % RS == 0 && (NT / 32) % (BK / KQ) == 0;
 
   __device__ static inline void coords(int idx, int kfast, int& kk, int& rr) {
-    kk = kfast ? (idx % BK) : (idx / ROWS);
-    rr = kfast ? (idx / BK) : (idx % ROWS);
+    if (kfast) {
+      if constexpr (WIDE) {
+        const int w = idx / 32, l = idx % 32;
+        kk = (w % (BK / KQ)) * KQ + l % KQ;
+        rr = (w / (BK / KQ)) * RS + l / KQ;
+      } else {
+        kk = idx % BK;
+        rr = idx / BK;
+      }
+    } else {
+      kk = idx / ROWS;
+      rr = idx % ROWS;
+    }
   }
 
   // Row offsets of this tile (rows_s: the tile's row scatter in shared memory).
@@ -311,10 +326,28 @@ struct AsyncGather {
   static_assert(ROWS * BK % NT == 0 && NT % BK == 0 && NT % ROWS == 0, "one k or one row per thread");
   int64_t var[PER];
   int64_t fixed;
+  // k-fast operands: a warp covers RS rows x KQ consecutive k (32 bytes of
+  // each row for 8-byte elements, 32 for 4-byte ones), so its cp.async
+  // writes into the [k][row] stage (row stride = 4 mod 16 words) spread over
+  // the banks; 32 lanes on 16 or 32 k of one row would land on a quarter of
+  // them. The k of a thread stays the same across its PER elements.
+  static constexpr int KQ = sizeof(R) == 4 ? 8 : 4, RS = 32 / KQ;
+  static constexpr bool WIDE = BK % KQ == 0 && ROWS % RS == 0 && (NT / 32) % (BK / KQ) == 0;
 
   __device__ static inline void coords(int idx, int kfast, int& kk, int& rr) {
-    kk = kfast ? (idx % BK) : (idx / ROWS);
-    rr = kfast ? (idx / BK) : (idx % ROWS);
+    if (kfast) {
+      if constexpr (WIDE) {
+        const int w = idx / 32, l = idx % 32;
+        kk = (w % (BK / KQ)) * KQ + l % KQ;
+        rr = (w / (BK / KQ)) * RS + l / KQ;
+      } else {
+        kk = idx % BK;
+        rr = idx / BK;
+      }
+    } else {
+      kk = idx / ROWS;
+      rr = idx % ROWS;
+    }
   }
   __device__ inline void init(const int64_t* rows_s, int64_t row0, int64_t nrows, int kfast, int tid) {
     if (kfast) {

@@ -98,6 +98,7 @@ Executor::~Executor() {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  for (cudaStream_t fs : family_streams) cudaStreamSynchronize(fs);
   for (auto& kv : graphs) {
     cudaGraphExecDestroy(kv.second.exec);
     cudaFree(kv.second.buf);
@@ -111,6 +112,8 @@ Executor::~Executor() {
   if (copy_out) cudaStreamDestroy(copy_out);
   if (own_stream && stream) cudaStreamDestroy(stream);
   if (capture_stream) cudaStreamDestroy(capture_stream);
+  for (cudaEvent_t e : family_events) cudaEventDestroy(e);
+  for (cudaStream_t fs : family_streams) cudaStreamDestroy(fs);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -1238,8 +1241,23 @@ struct GroupSet {
 
 GroupSet build_group_set(Executor& ex, const std::vector<int>& idx, int policy, Product* const* plans,
                          const Scalar* alpha, const Scalar* beta, const Item* items) {
-  std::map<int, std::vector<int>> fam;
-  for (int i : idx) fam[grouped_family(*plans[i], policy)].push_back(i);
+  std::map<int, std::vector<int>> by_family;
+  for (int i : idx) by_family[grouped_family(*plans[i], policy)].push_back(i);
+  // Families in decreasing order of work (padded tile volume): the first one
+  // runs on the submitting stream and the others fill its tail.
+  std::vector<std::pair<int, std::vector<int>>> fam(by_family.begin(), by_family.end());
+  auto work = [&](const std::pair<int, std::vector<int>>& f) {
+    int bm = 0, bn = 0;
+    dev::plain_tile_shape(f.first, &bm, &bn);
+    double w = 0;
+    for (int i : f.second) {
+      const Product& pr = *plans[i];
+      w += (double)((pr.view.M + bm - 1) / bm * bm) * (double)((pr.view.N + bn - 1) / bn * bn) *
+           (double)pr.view.K * (double)pr.view.H;
+    }
+    return w;
+  };
+  std::stable_sort(fam.begin(), fam.end(), [&](const auto& a, const auto& b) { return work(a) > work(b); });
   GroupSet gs;
   std::vector<dev::GroupItem> host_items;
   std::vector<int64_t> host_starts;
@@ -1295,12 +1313,44 @@ GroupSet build_group_set(Executor& ex, const std::vector<int>& idx, int policy, 
   return gs;
 }
 
+// One persistent launch per family. With several families the first (the
+// one with the most work, see build_group_set) runs on `st` and
+// each other one on a side stream forked from `st` before it and joined back
+// after; the persistent grids of the later families take SMs as the earlier
+// ones' CTAs run out of tiles, instead of starting after their last tile.
 cudaError_t launch_group_set(Executor& ex, const GroupSet& gs, cudaStream_t st) {
-  cudaError_t e = cudaSuccess;
-  for (size_t l = 0; l < gs.family.size() && e == cudaSuccess; ++l)
-    e = dev::launch_grouped(gs.family[l], reinterpret_cast<dev::GroupItem*>(gs.buf) + gs.item0[l],
-                            reinterpret_cast<int64_t*>(gs.starts) + gs.start0[l], (int)gs.count[l],
-                            reinterpret_cast<unsigned long long*>(gs.counters + 256 * l), ex.status, ex.num_sms, st);
+  const size_t nf = gs.family.size();
+  auto launch = [&](size_t l, cudaStream_t s) {
+    return dev::launch_grouped(gs.family[l], reinterpret_cast<dev::GroupItem*>(gs.buf) + gs.item0[l],
+                               reinterpret_cast<int64_t*>(gs.starts) + gs.start0[l], (int)gs.count[l],
+                               reinterpret_cast<unsigned long long*>(gs.counters + 256 * l), ex.status, ex.num_sms,
+                               s);
+  };
+  if (nf <= 1) {
+    cudaError_t e = cudaSuccess;
+    for (size_t l = 0; l < nf && e == cudaSuccess; ++l) e = launch(l, st);
+    return e;
+  }
+  while (ex.family_streams.size() < nf - 1) {
+    cudaStream_t s = nullptr;
+    const cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    ex.family_streams.push_back(s);
+  }
+  while (ex.family_events.size() < nf) {
+    cudaEvent_t ev = nullptr;
+    const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    ex.family_events.push_back(ev);
+  }
+  cudaError_t e = cudaEventRecord(ex.family_events[0], st);
+  for (size_t l = 1; l < nf && e == cudaSuccess; ++l) e = cudaStreamWaitEvent(ex.family_streams[l - 1], ex.family_events[0], 0);
+  if (e == cudaSuccess) e = launch(0, st);
+  for (size_t l = 1; l < nf && e == cudaSuccess; ++l) {
+    e = launch(l, ex.family_streams[l - 1]);
+    if (e == cudaSuccess) e = cudaEventRecord(ex.family_events[l], ex.family_streams[l - 1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ex.family_events[l], 0);
+  }
   return e;
 }
 

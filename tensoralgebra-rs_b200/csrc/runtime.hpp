@@ -114,6 +114,11 @@ struct Executor {
   bool streaming = true;
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> stream_events;
+  // Side streams of a grouped submission whose items fall into several tile
+  // families: the families' persistent launches run concurrently (fork and
+  // join through events), so a later family fills the tail of an earlier one.
+  std::vector<cudaStream_t> family_streams;
+  std::vector<cudaEvent_t> family_events;
 
   static Executor* create(int device, uintptr_t stream);
   ~Executor();

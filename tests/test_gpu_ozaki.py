@@ -153,3 +153,40 @@ def test_ozaki_batch_innermost_conjugated_c3_layout(tp, ex, torch_cuda, orc):
     want = oracle_ref(orc, dt, A, B, None, D, 1.0, 0.0, d0)
     got, p = oz(tp, ex, torch_cuda, dt, A, B, None, D, 1.0, 0.0)
     assert orc.rel_frobenius(got, want) <= 1e-12, p.report()
+
+
+@pytest.mark.parametrize("dt,k", [("float64", 37), ("complex128", 37), ("float64", 900), ("complex128", 450)],
+                         ids=["f64-k37", "c64-k37", "f64-k900-two-pass", "c64-k450-two-pass"])
+def test_ozaki_batch_innermost_depths(tp, ex, torch_cuda, orc, dt, k):
+    """Batch-innermost operands (h = 35 entries, stride 1) at a depth that is
+    not a multiple of four (one pass over the operand: the whole depth of 16
+    batch entries in shared memory) and at depths past that kernel's shared
+    memory bound (the exponent scan and the slicing as two passes)."""
+    rng = np.random.default_rng(47 + k)
+    h, m, n = 35, 23, 19
+    A = Op(rnd(rng, dt, h * k * m), [h, k, m], [1, h, h * k], [9, 2, 0], conj=dt == "complex128")
+    B = Op(rnd(rng, dt, h * k * n), [h, k, n], [1, h, h * k], [9, 2, 1])
+    d0 = np.zeros(h * m * n, dtype=dt)
+    D = Op(d0, [h, m, n], [1, h, h * m], [9, 0, 1])
+    want = oracle_ref(orc, dt, A, B, None, D, 1.0, 0.0, d0)
+    got, p = oz(tp, ex, torch_cuda, dt, A, B, None, D, 1.0, 0.0)
+    assert orc.rel_frobenius(got, want) <= 1e-12, p.report()
+
+
+@pytest.mark.parametrize("dt", ["float64", "complex128"])
+def test_ozaki_batch_innermost_non_finite(tp, ex, torch_cuda, orc, dt):
+    """A NaN in one batch entry of one row of a batch-innermost A gives NaN in
+    that entry's output row only."""
+    rng = np.random.default_rng(49)
+    h, m, n, k = 40, 9, 7, 30
+    a = rnd(rng, dt, h * k * m)
+    a[5 + h * 11 + h * k * 4] = np.nan  # batch 5, k 11, row 4
+    A = Op(a, [h, k, m], [1, h, h * k], [9, 2, 0])
+    B = Op(rnd(rng, dt, h * k * n), [h, k, n], [1, h, h * k], [9, 2, 1])
+    D = Op(np.zeros(h * m * n, dtype=dt), [h, m, n], [1, h, h * m], [9, 0, 1])
+    got, _ = oz(tp, ex, torch_cuda, dt, A, B, None, D, 1.0, 0.0)
+    G = got.reshape(n, m, h)  # [j, i, b]
+    bad = np.isnan(G.real) | np.isnan(G.imag) if dt == "complex128" else np.isnan(G)
+    assert np.all(bad[:, 4, 5])
+    bad[:, 4, 5] = False
+    assert not np.any(bad)

@@ -60,12 +60,18 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
 // halves of |T| (a funnel shift across the boundary), packed four to a word
 // by byte permutes, and negated bytewise where x < 0: for a byte b <= 127,
 // ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
+// 2^k for k in [-1022, 1023], built from its bits.
+__device__ __forceinline__ double oz_pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
 template <int S>
 __device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[8]) {
-  const int k = 7 * S - e;  // scale exponent; above 1023 only for rows below 2^-967
+  // Scale 2^(7S - e) as s1 * s2 (two factors only for rows below 2^-967:
+  // 7S - e above 1023). e >= -1074 and e <= 1024 keep both exponents in the
+  // normal range; a non-finite row (its x are zeros) takes scale 1.
+  const int k = e == EXP_NONFINITE ? 0 : 7 * S - e;
   const bool two = k > 1023;
-  const double s1 = two ? ldexp(1.0, 1000) : ldexp(1.0, k);
-  const double s2 = two ? ldexp(1.0, k - 1000) : 1.0;
+  const double s1 = oz_pow2(two ? 1000 : k);
+  const double s2 = oz_pow2(two ? k - 1000 : 0);
   uint32_t lo[4], hi[4], negmask = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -367,72 +373,46 @@ __global__ void __launch_bounds__(256) ozaki_slice_hfast_c64_kernel(
 // One pass over a batch-innermost operand: a CTA holds OZ_HB batch entries of
 // one row, all of K, in shared memory, takes their exponents there and slices
 // them, so the operand is read from HBM once instead of once by the scan and
-// once by the slicing. The row's k offsets are staged in shared memory first;
-// then every element copy of the CTA is issued at once (cp.async, 16 bytes
-// per complex element when the operand is 16-byte aligned) and waited for
-// together, so a CTA keeps its whole block in flight. Shared layout
-// t[hl][swz(k)] (complex: re, im interleaved): the copies (8 lanes on 8 batch
-// entries at each of 4 k) and the slicing reads (lanes on consecutive quads
-// of k) both fall on distinct bank slots up to the width of a wavefront; swz
-// only permutes k inside its aligned group of four.
-constexpr int OZ_HB = 8;
-constexpr int OZ_PACK_THREADS = 128;
+// once by the slicing. Shared layout t[hl][swz(k)] with an odd row stride:
+// the loads (16 lanes on 16 batch entries at one k) and the slicing reads (32
+// lanes on 32 consecutive quads of k, one q at a time) both touch 16
+// distinct 8-byte bank slots per half-warp. swz only permutes k inside its
+// aligned group of four.
+constexpr int OZ_HB = 16;
 
 __device__ __forceinline__ int64_t oz_swz(int64_t k) { return k ^ ((k >> 4) & 3); }
 
-// Row stride of t in elements: odd for 16-byte complex elements (8 slots per
-// wavefront), 4 mod 16 for 8-byte real ones (16 slots).
-__host__ __device__ inline int64_t oz_hfast_stride(bool cplx, int64_t K) {
-  return cplx ? (K + 3) / 4 * 4 + 1 : (K + 15) / 16 * 16 + 4;
-}
-
-__device__ __forceinline__ void oz_cp16(void* s, const void* g) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void oz_cp8(void* s, const void* g) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(s)), "l"(g) : "memory");
-}
+__host__ __device__ inline int64_t oz_hfast_stride(int64_t K) { return (K + 3) / 4 * 4 + 1; }
 
 template <bool CPLX, int WHICH>
-__global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
+__global__ void __launch_bounds__(256, 2) ozaki_pack_hfast_kernel(
     const double* __restrict__ X, const int64_t* rows_scat, const int64_t* k_scat, const int64_t* h_scat,
     int64_t nrows, int64_t crows, int64_t K, int64_t kw, int64_t rows_pad, int64_t exp_pad, int64_t k_pad,
-    int64_t Kh, int64_t H, int conj, int S, int vec16, int* __restrict__ exps, int8_t* __restrict__ out) {
-  constexpr int EW = CPLX ? 2 : 1;  // doubles per element
-  constexpr int KL = OZ_PACK_THREADS / OZ_HB;  // k lanes of the copy phase
-  extern __shared__ __align__(16) double oz_t[];
-  __shared__ unsigned long long red[KL][OZ_HB];
+    int64_t Kh, int64_t H, int conj, int S, int* __restrict__ exps, int8_t* __restrict__ out) {
+  extern __shared__ double oz_t[];
+  __shared__ unsigned long long red[256 / OZ_HB][OZ_HB];
   __shared__ int ex_s[OZ_HB];
   const int tid = threadIdx.x, hl = tid % OZ_HB, kp = tid / OZ_HB;
-  const int64_t ks = oz_hfast_stride(CPLX, K);
-  int64_t* koff = reinterpret_cast<int64_t*>(oz_t + EW * OZ_HB * ks);
+  const int64_t ks = oz_hfast_stride(K);
+  double* t_re = oz_t;
+  double* t_im = oz_t + OZ_HB * ks;
   const int64_t r = blockIdx.x, h0 = (int64_t)blockIdx.y * OZ_HB;
-  for (int64_t k = tid; k < K; k += OZ_PACK_THREADS) koff[k] = k_scat[k];
-  __syncthreads();
   const bool live = r < nrows && h0 + hl < H;
-  if (live) {
-    const double* base = X + EW * (h_scat[h0 + hl] + rows_scat[r]);
-    double* trow = oz_t + EW * hl * ks;
-#pragma unroll 4
-    for (int64_t k = kp; k < K; k += KL) {
-      const double* e = base + EW * koff[k];
-      double* sd = trow + EW * oz_swz(k);
-      if (CPLX && vec16) {
-        oz_cp16(sd, e);
-      } else {
-        oz_cp8(sd, e);
-        if (CPLX) oz_cp8(sd + 1, e + 1);
-      }
-    }
-  }
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;\n" ::: "memory");
+  const double* base = X + (CPLX ? 2 : 1) * (live ? h_scat[h0 + hl] + rows_scat[r] : 0);
   unsigned long long best = 0ull;
   if (live) {
-    const double* trow = oz_t + EW * hl * ks;
-    for (int64_t k = kp; k < K; k += KL) {
-      const double* sd = trow + EW * oz_swz(k);
-      unsigned long long bits = mag_bits(sd[0]);
-      if constexpr (CPLX) bits = max_bits(bits, mag_bits(sd[1]));
+#pragma unroll 8
+    for (int64_t k = kp; k < K; k += 256 / OZ_HB) {
+      const double* e = base + (CPLX ? 2 : 1) * __ldg(k_scat + k);
+      const double re = e[0];
+      unsigned long long bits = mag_bits(re);
+      const int64_t pos = hl * ks + oz_swz(k);
+      t_re[pos] = re;
+      if constexpr (CPLX) {
+        const double im = e[1];
+        bits = max_bits(bits, mag_bits(im));
+        t_im[pos] = conj ? -im : im;
+      }
       best = bits > best ? bits : best;
     }
   }
@@ -441,7 +421,7 @@ __global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
   if (tid < OZ_HB) {
     unsigned long long b = red[0][tid];
 #pragma unroll
-    for (int j = 1; j < KL; ++j) b = red[j][tid] > b ? red[j][tid] : b;
+    for (int j = 1; j < 256 / OZ_HB; ++j) b = red[j][tid] > b ? red[j][tid] : b;
     int e = 0;
     if (b >= 0x7ff0000000000000ull) e = EXP_NONFINITE;
     else if (b != 0ull) frexp(__longlong_as_double((long long)b), &e);
@@ -451,8 +431,7 @@ __global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
   __syncthreads();
   if (r >= crows) return;
   const int64_t nq = kw / 4, plane = H * rows_pad * k_pad;
-  const double sgn = conj ? -1.0 : 1.0;
-  for (int64_t it = tid; it < OZ_HB * nq; it += OZ_PACK_THREADS) {
+  for (int64_t it = tid; it < OZ_HB * nq; it += 256) {
     const int hh = (int)(it / nq);
     const int64_t kq = (it - hh * nq) * 4, h = h0 + hh;
     if (h >= H) break;
@@ -462,14 +441,9 @@ __global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
     for (int q = 0; q < 4; ++q) {
       const int64_t k = kq + q;
       const bool in = k < K && e != EXP_NONFINITE && r < nrows;
-      const double* sd = oz_t + EW * (hh * ks + oz_swz(k));
-      if constexpr (CPLX) {
-        const double2 v = in ? *reinterpret_cast<const double2*>(sd) : make_double2(0.0, 0.0);
-        re[q] = v.x;
-        im[q] = sgn * v.y;
-      } else {
-        re[q] = in ? sd[0] : 0.0;
-      }
+      const int64_t pos = hh * ks + oz_swz(k);
+      re[q] = in ? t_re[pos] : 0.0;
+      if constexpr (CPLX) im[q] = in ? t_im[pos] : 0.0;
     }
     if constexpr (!CPLX) {
       write_slices(re, e, S, out + (h * rows_pad + r) * k_pad + kq, plane);
@@ -484,11 +458,8 @@ __global__ void __launch_bounds__(OZ_PACK_THREADS, 4) ozaki_pack_hfast_kernel(
   }
 }
 
-// Shared memory of the one-pass kernel (the block and the row's k offsets);
-// it runs when two CTAs fit on an SM (four at the C3 depth of 384).
-inline size_t oz_hfast_smem(bool cplx, int64_t K) {
-  return (size_t)(cplx ? 2 : 1) * OZ_HB * oz_hfast_stride(cplx, K) * 8 + (size_t)K * 8;
-}
+// Shared memory of the one-pass kernel; it runs when two CTAs fit on an SM.
+inline size_t oz_hfast_smem(bool cplx, int64_t K) { return (cplx ? 2 : 1) * OZ_HB * oz_hfast_stride(K) * 8; }
 constexpr size_t OZ_HFAST_SMEM_MAX = 100 * 1024;
 
 // Complex slicing for the general layouts (rows or k unit-stride): one load
@@ -858,11 +829,10 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
     const int64_t rows = exp_pad > crows ? exp_pad : crows;
     const dim3 grid((unsigned)rows, (unsigned)((L.H + OZ_HB - 1) / OZ_HB));
     const int64_t kw = CPLX ? L.k_half : L.k_pad;
-    const int vec16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0 ? 1 : 0;
     auto kern = which == 0 ? ozaki_pack_hfast_kernel<CPLX, 0> : ozaki_pack_hfast_kernel<CPLX, 1>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one_pass);
-    kern<<<grid, OZ_PACK_THREADS, one_pass, st>>>(X, rows_s, k_s, h_s, nrows, crows, K, kw, rows_pad, exp_pad,
-                                                  L.k_pad, L.k_half, L.H, conj, L.slices, vec16, exps, planes);
+    kern<<<grid, 256, one_pass, st>>>(X, rows_s, k_s, h_s, nrows, crows, K, kw, rows_pad, exp_pad, L.k_pad,
+                                      L.k_half, L.H, conj, L.slices, exps, planes);
   } else if (hfast) {
     ozaki_exp_hfast_kernel<CPLX><<<dim3((unsigned)exp_pad, (unsigned)((L.H + 31) / 32)), 256, 0, st>>>(
         X, rows_s, k_s, h_s, nrows, K, exp_pad, L.H, exps);

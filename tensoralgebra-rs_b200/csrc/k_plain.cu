@@ -379,6 +379,24 @@ struct AsyncGather {
       }
     }
   }
+  // The same from k offsets staged in shared memory (kscat_s[k - k_base]).
+  __device__ inline void load_idx_s(const int64_t* kscat_s, int64_t k_base, int64_t k0, int64_t K, int kfast,
+                                    int tid) {
+    if (kfast) {
+      int kk, rr;
+      coords(tid, 1, kk, rr);
+      const int64_t k = k0 + kk;
+      fixed = k < K ? kscat_s[k - k_base] : INT64_MIN;
+    } else {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        int kk, rr;
+        coords(tid + j * NT, 0, kk, rr);
+        const int64_t k = k0 + kk;
+        var[j] = k < K ? kscat_s[k - k_base] : INT64_MIN;
+      }
+    }
+  }
   // Copies of this thread's elements of the stage whose offsets are loaded.
   __device__ inline void issue(const T* base, R* s_re, R* s_im, int stride, int kfast, int tid) const {
 #pragma unroll
@@ -425,6 +443,11 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
   double(*As)[NPL][BK * SA] = reinterpret_cast<double(*)[NPL][BK * SA]>(dmma_ring);
   double(*Bs)[NPL][BK * SB] = reinterpret_cast<double(*)[NPL][BK * SB]>(dmma_ring + STAGES * Ring::A_STAGE);
   __shared__ int64_t am_s[BM], bn_s[BN], dm_s[BM], cm_s[BM], dn_s[BN], cn_s[BN];
+  // A K range of at most KS is short: its k offsets are staged with the row
+  // and column offsets, so no stage waits on a k-offset load before its
+  // copies can be issued (each such load is a memory round trip).
+  constexpr int KS = 64;
+  __shared__ int64_t ak_s[KS], bk_s[KS];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t m0 = mtile * BM, n0 = ntile * BN;
@@ -444,6 +467,15 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
     dn_s[i] = ok ? g.s.d_n[n] : 0;
     cn_s[i] = ok ? g.s.c_n[n] : 0;
   }
+  // This CTA's K range (the whole of K unless split).
+  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
+  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
+  const bool kstaged = ke - kb <= KS;
+  if (kstaged)
+    for (int i = tid; i < ke - kb; i += NT) {
+      ak_s[i] = g.s.a_k[kb + i];
+      bk_s[i] = g.s.b_k[kb + i];
+    }
   __syncthreads();
 
   const T* Ab = static_cast<const T*>(g.A) + g.s.h_a[h];
@@ -468,10 +500,16 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
         }
       }
 
-  // This CTA's K range (the whole of K unless split).
-  const int64_t kb = g.k_chunk ? split * g.k_chunk : 0;
-  const int64_t ke = g.k_chunk ? min(g.K, kb + g.k_chunk) : g.K;
   const int64_t nt = (ke - kb + BK - 1) / BK;
+  auto load_stage_idx = [&](int64_t k0) {
+    if (kstaged) {
+      ga.load_idx_s(ak_s, kb, k0, ke, g.a_kfast, tid);
+      gb.load_idx_s(bk_s, kb, k0, ke, g.b_kfast, tid);
+    } else {
+      ga.load_idx(g.s.a_k, k0, ke, g.a_kfast, tid);
+      gb.load_idx(g.s.b_k, k0, ke, g.b_kfast, tid);
+    }
+  };
   ga.init(am_s, m0, g.M, g.a_kfast, tid);
   gb.init(bn_s, n0, g.N, g.b_kfast, tid);
   // Prologue: stages 0 .. STAGES-2 in flight (one commit group each, empty
@@ -479,8 +517,7 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
 #pragma unroll
   for (int sidx = 0; sidx < STAGES - 1; ++sidx) {
     if (sidx < nt) {
-      ga.load_idx(g.s.a_k, kb + sidx * BK, ke, g.a_kfast, tid);
-      gb.load_idx(g.s.b_k, kb + sidx * BK, ke, g.b_kfast, tid);
+      load_stage_idx(kb + sidx * BK);
       ga.issue(Ab, As[sidx][0], As[sidx][NPL - 1], SA, g.a_kfast, tid);
       gb.issue(Bb, Bs[sidx][0], Bs[sidx][NPL - 1], SB, g.b_kfast, tid);
     }
@@ -491,10 +528,7 @@ __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, in
   const int fr = lane >> 2, fk = lane & 3;
   for (int64_t t = 0; t < nt; ++t) {
     const int64_t tp = t + STAGES - 1;  // the stage issued in this iteration
-    if (tp < nt) {
-      ga.load_idx(g.s.a_k, kb + tp * BK, ke, g.a_kfast, tid);
-      gb.load_idx(g.s.b_k, kb + tp * BK, ke, g.b_kfast, tid);
-    }
+    if (tp < nt) load_stage_idx(kb + tp * BK);
     cp_async_wait<STAGES - 2>();  // this thread's copies of stage t have landed
     __syncthreads();              // everyone's have; and stage t-1's buffer is free
     if (tp < nt) {

@@ -52,6 +52,9 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
   return ((w ^ 0x7f7f7f7fu) + 0x01010101u) ^ 0x80808080u;
 }
 
+// 2^k for k in [-1022, 1023], built from its bits.
+__device__ __forceinline__ double oz_pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
 // The S signed 7-bit slices of four values of one row with exponent e
 // (|x| < 2^e), written as one 4-byte word per plane. T = trunc(x 2^(7S - e)) is
 // exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
@@ -60,9 +63,6 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
 // halves of |T| (a funnel shift across the boundary), packed four to a word
 // by byte permutes, and negated bytewise where x < 0: for a byte b <= 127,
 // ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
-// 2^k for k in [-1022, 1023], built from its bits.
-__device__ __forceinline__ double oz_pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
-
 template <int S>
 __device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[8]) {
   // Scale 2^(7S - e) as s1 * s2 (two factors only for rows below 2^-967:
@@ -396,7 +396,12 @@ __global__ void __launch_bounds__(256, 2) ozaki_pack_hfast_kernel(
   const int64_t ks = oz_hfast_stride(K);
   double* t_re = oz_t;
   double* t_im = oz_t + OZ_HB * ks;
-  const int64_t r = blockIdx.x, h0 = (int64_t)blockIdx.y * OZ_HB;
+  // Batch groups vary fastest over the grid, so the CTAs resident together
+  // read all the batch entries of their rows: every batch run of an operand
+  // row is read at once, not the same part of each row by every SM (which
+  // loaded some DRAM channels twice as much as others).
+  const int64_t hgroups = (H + OZ_HB - 1) / OZ_HB;
+  const int64_t r = (int64_t)blockIdx.x / hgroups, h0 = ((int64_t)blockIdx.x % hgroups) * OZ_HB;
   const bool live = r < nrows && h0 + hl < H;
   const double* base = X + (CPLX ? 2 : 1) * (live ? h_scat[h0 + hl] + rows_scat[r] : 0);
   unsigned long long best = 0ull;
@@ -823,11 +828,12 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
                          int64_t K, const OzakiLayout& L, int64_t exp_pad, int64_t rows_pad,
                          int kfast, int hfast, int which, int conj, int* exps, int8_t* planes, cudaStream_t st) {
   const size_t one_pass = oz_hfast_smem(CPLX, K);
-  if (hfast && one_pass <= OZ_HFAST_SMEM_MAX) {
-    // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
-    const int64_t crows = CPLX && which == 0 ? rows_pad / 2 : rows_pad;
-    const int64_t rows = exp_pad > crows ? exp_pad : crows;
-    const dim3 grid((unsigned)rows, (unsigned)((L.H + OZ_HB - 1) / OZ_HB));
+  // Complex rows: rows_pad / 2 for A' (two embedded rows each), rows_pad for B'.
+  const int64_t crows = CPLX && which == 0 ? rows_pad / 2 : rows_pad;
+  const int64_t rows = exp_pad > crows ? exp_pad : crows;
+  const int64_t blocks = rows * ((L.H + OZ_HB - 1) / OZ_HB);
+  if (hfast && one_pass <= OZ_HFAST_SMEM_MAX && blocks <= 0x7fffffff) {
+    const dim3 grid((unsigned)blocks);
     const int64_t kw = CPLX ? L.k_half : L.k_pad;
     auto kern = which == 0 ? ozaki_pack_hfast_kernel<CPLX, 0> : ozaki_pack_hfast_kernel<CPLX, 1>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one_pass);

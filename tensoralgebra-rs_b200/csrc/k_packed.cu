@@ -10,7 +10,7 @@
 // order, so the tile kernels never pay for a general-stride gather: every
 // operand byte they read is a dense TMA box.
 //
-//  * simt_packed_kernel: FP32 FFMA, 128 x 128 tiles, 16-deep stages in a
+//  * simt_packed_kernel: FP32 FFMA, 128 x 128 tiles, 32-deep stages in a
 //    4-stage TMA ring (one producer warp), eight compute warps with 8 x 8
 //    outputs per thread; the running sums are restarted every 64 k and added
 //    into the totals with round-to-nearest adds (FP32 error near
@@ -192,13 +192,15 @@ __global__ void __launch_bounds__(256) plain_pack_kernel(const typename Elem<R, 
 
 // ------------------------------------------------------------ FFMA tile (f32)
 
-// Tile shapes of the FFMA kernel: 128 rows x BN columns, 16-deep stages, 256
-// compute threads each with 8 rows x BN/16 columns (groups of four columns
-// 64 apart), one producer warp. BN = 128 runs one CTA per SM (168 registers),
-// BN = 64 two (half the accumulators, twice the warps to hide latency).
+// Tile shapes of the FFMA kernel: 128 rows x BN columns, 32-deep stages (one
+// barrier wait and arrival per 32 k), 256 compute threads each with 8 rows x
+// BN/16 columns (groups of four columns 64 apart), one producer warp. BN = 128
+// runs one CTA per SM (168 registers), BN = 64 two (half the accumulators,
+// twice the warps to hide latency). Running sums restart every FLUSH stages
+// (64 k).
 template <int BN>
 struct SpCfg {
-  static constexpr int BM = 128, BK = 16, STAGES = BN == 128 ? 4 : 6, FLUSH = 4;
+  static constexpr int BM = 128, BK = 32, STAGES = 4, FLUSH = 2;
   static constexpr int TN = BN / 16, CG = TN / 4;  // columns per thread, groups of four
   static constexpr int A = BK * BM * 4, B = BK * BN * 4, STAGE = A + B;
   static constexpr int COMPUTE = 256, THREADS = COMPUTE + 32;

@@ -1136,12 +1136,12 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C64_DMMA_32x32: return "sm100.c64.dmma884.3m.32x32x8";
     case PLAIN_F64_DMMA_128x32: return "sm100.f64.dmma884.128x32x16";
     case PLAIN_C64_DMMA_128x32: return "sm100.c64.dmma884.3m.128x32x8";
-    case PLAIN_F32_PACKED_128x128: return "sm100.f32.simt.tma.packed.128x128x16";
-    case PLAIN_C32_PACKED_1M_64x128: return "sm100.c32.simt.tma.1m.64x128x16";
+    case PLAIN_F32_PACKED_128x128: return "sm100.f32.simt.tma.packed.128x128x32";
+    case PLAIN_C32_PACKED_1M_64x128: return "sm100.c32.simt.tma.1m.64x128x32";
     case PLAIN_F64_PACKED_64x64: return "sm100.f64.dmma884.tma.packed.64x64x16";
     case PLAIN_C64_PACKED_3M_64x32: return "sm100.c64.dmma884.tma.3m.64x32x16";
-    case PLAIN_F32_PACKED_128x64: return "sm100.f32.simt.tma.packed.128x64x16";
-    case PLAIN_C32_PACKED_1M_64x64: return "sm100.c32.simt.tma.1m.64x64x16";
+    case PLAIN_F32_PACKED_128x64: return "sm100.f32.simt.tma.packed.128x64x32";
+    case PLAIN_C32_PACKED_1M_64x64: return "sm100.c32.simt.tma.1m.64x64x32";
   }
   return "auto";
 }

@@ -370,10 +370,10 @@ def test_autotune_candidates(tp):
     assert {"sm100.f64.dmma884.64x64x16", "sm100.f64.dmma884.32x32x16", "sm100.f64.dmma884.128x32x16"} <= set(c1)
     assert any("+splitk" in c for c in c1) and len(c1) == len(set(c1))
     big = _gemm_product(tp, 4096, 4096, 4096, dt=0).report()["autotune_candidates"]
-    assert big[0] == "sm100.f32.simt.tma.packed.128x128x16"  # the model: packed, a full wave of tiles
+    assert big[0] == "sm100.f32.simt.tma.packed.128x128x32"  # the model: packed, a full wave of tiles
     assert sorted(big) == ["sm100.f32.simt.128x128x16", "sm100.f32.simt.64x64x16",
-                           "sm100.f32.simt.tma.packed.128x128x16",
-                           "sm100.f32.simt.tma.packed.128x64x16"]  # enough tiles: no split
+                           "sm100.f32.simt.tma.packed.128x128x32",
+                           "sm100.f32.simt.tma.packed.128x64x32"]  # enough tiles: no split
     shallow = _gemm_product(tp, 64, 64, 128).report()["autotune_candidates"]
     assert not any("+splitk" in c for c in shallow)  # halves of K = 128 would be 64 deep
     c32 = _gemm_product(tp, 300, 300, 300, dt=2).report()["autotune_candidates"]

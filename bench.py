@@ -755,7 +755,7 @@ def run_config(args, tp, torch, ex):
             for pb in prepared:
                 pb.run(ex)
 
-        for grouping in (True, False):
+        for grouping in ((True,) if args.grouped_only else (True, False)):
             ex.set_grouping(grouping)
             ms, kt = timed(step, args.steps if grouping else max(2, args.steps // 4), min(args.warmup, 3))
             out["grouped" if grouping else "per_item_loop"] = {"tflops": flop / (ms * 1e-3) / 1e12,
@@ -777,7 +777,8 @@ def run_config(args, tp, torch, ex):
                 pol[str(e.get("policy"))] = pol.get(str(e.get("policy")), 0) + 1
             out["grouped"]["autotune"] = {"list_policies": pol, "policy_names": {"0": "per-item model", "1": "large",
                                                                                  "2": "small", "3": "tall for N<=32"}}
-        out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
+        if "per_item_loop" in out:
+            out["speedup_grouped_vs_loop"] = out["grouped"]["tflops"] / out["per_item_loop"]["tflops"]
         # Per binary step (grouped), and the mixed roofline of the list: each
         # item-step bounded by max(flops / FP64 DMMA peak, bytes / HBM peak).
         es, fm = (16, 8) if cfg == "c4c" else (8, 2)
@@ -805,7 +806,7 @@ def run_config(args, tp, torch, ex):
         # every network in one grouped submission, intermediates in each
         # network's own arena.
         nets, net_in, net_out = [], [], []
-        for it, t in zip(items, dev):
+        for it, t in (() if args.grouped_only else zip(items, dev)):
             ext = c4_extents(it)
             ins = []
             for name, labs, cj in (("E", [0, 1, 2], False), ("Ma", [0, 3, 4], False), ("W", [1, 3, 5, 6], False),
@@ -815,13 +816,14 @@ def run_config(args, tp, torch, ex):
                                    [(0, 1), (2, 0), (1, 0)]))
             net_in.append([t["E"], t["Ma"], t["W"], t["Mb"]])
             net_out.append(torch.zeros_like(t["Ep"]))
-        prep_net = tp.PreparedNetworks(nets, net_in, net_out)  # argument arrays built once, like the lists'
-        ms_n, kt_n = timed(lambda: prep_net.run(ex), args.steps, min(args.warmup, 3))
-        diff = max(float((o - t["Ep"]).abs().max().item()) for o, t in zip(net_out, dev))
-        out["network_driver"] = {"tflops": flop / (ms_n * 1e-3) / 1e12, "ms_per_step": ms_n, "kernels": kt_n,
-                                 "arena_bytes": sum(n.workspace_size() for n in nets),
-                                 "max_abs_diff_vs_lists": diff}
-        del prep_net
+        if nets:
+            prep_net = tp.PreparedNetworks(nets, net_in, net_out)  # argument arrays built once, like the lists'
+            ms_n, kt_n = timed(lambda: prep_net.run(ex), args.steps, min(args.warmup, 3))
+            diff = max(float((o - t["Ep"]).abs().max().item()) for o, t in zip(net_out, dev))
+            out["network_driver"] = {"tflops": flop / (ms_n * 1e-3) / 1e12, "ms_per_step": ms_n, "kernels": kt_n,
+                                     "arena_bytes": sum(n.workspace_size() for n in nets),
+                                     "max_abs_diff_vs_lists": diff}
+            del prep_net
         for n in nets:
             n.close()
         del net_out
@@ -918,6 +920,8 @@ def main():
     ap.add_argument("--only-head", action="store_true", help="time the headline scheme only (profiling runs)")
     ap.add_argument("--items", type=int, default=4096, help="list length of config 4")
     ap.add_argument("--no-autotune", action="store_true", help="config 4: the model's tiles instead of autotuned ones")
+    ap.add_argument("--grouped-only", action="store_true",
+                    help="config 4: time the grouped lists only (no per-item loop, no network driver; profiling runs)")
     ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
     ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
     ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")

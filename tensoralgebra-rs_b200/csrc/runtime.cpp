@@ -870,66 +870,113 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   const PlanStats& stt = pr.packed.stats;
   const int64_t elem = (int64_t)dtype_size(p.dtype);
   const int sx = v.swapped ? SA : SB;  // the operand that plays B'
-  const std::vector<Axis>& nax = v.swapped ? stt.m_axes : stt.n_axes;
-  if (nax.empty() || v.H > 65535) return false;
-  const Axis& ca = nax.back();
-  const int64_t E = ca.extent;
-  if (E < 2) return false;
-  // Chunks that halve in size (E/2, E/4, ... down to about E/16, the rest
-  // last): the call ends with the kernels and the copy out of the last chunk
-  // only, so a small last chunk shortens that tail while the large first ones
-  // keep the kernels efficient. Every chunk keeps at least 256 columns.
-  const int64_t inner_n = v.N / E;
-  std::vector<int64_t> bounds{0};
-  while (bounds.back() < E) {
-    const int64_t left = E - bounds.back();
-    int64_t take = left / 2;
-    if (take * 16 < E || take * inner_n < 256 || (left - take) * inner_n < 256) take = left;
-    bounds.push_back(bounds.back() + take);
-  }
-  const int nchunks = (int)bounds.size() - 1;
-  if (nchunks < 2 || nchunks > 8) return false;
+  const int sy = v.swapped ? SB : SA;  // the operand that plays A'
+  if (v.H > 65535) return false;
   const auto stride_in = [](const Axis& a, int slot) {
     return slot == SA ? a.sa : slot == SB ? a.sb : slot == SC ? a.sc : a.sd;
   };
-  const auto others = [&](int slot) {
-    std::vector<std::pair<int64_t, int64_t>> out;
-    for (const std::vector<Axis>* role : {&stt.m_axes, &stt.n_axes, &stt.k_axes, &stt.h_axes})
-      for (const Axis& a : *role)
-        if (&a != &ca) out.push_back({a.extent, stride_in(a, slot)});
-    return out;
+  // One side of the product is chunked along its outermost axis (of D's N
+  // columns, or of its M rows), the other operand is copied whole first; the
+  // larger operand is the one chunked, so the kernels start after the smaller
+  // copy and the copies out of D start early (C2: B' 64 MB whole, then A'
+  // 128 MB in chunks of its outermost row axis).
+  struct Side {
+    bool rows = false;  // chunks of M (A' rows) instead of N (B' columns)
+    const Axis* ca = nullptr;
+    int64_t E = 0, inner = 0;
+    int slot = SB;  // the chunked operand
+    std::vector<int64_t> lo, hi;
+    std::vector<std::vector<ChunkCopy>> xcp, dcp;
   };
-  std::vector<std::vector<ChunkCopy>> bcp(nchunks), dcp(nchunks);
-  std::vector<int64_t> lo(nchunks), hi(nchunks);
-  for (int c = 0; c < nchunks; ++c) {
-    lo[c] = bounds[c];
-    hi[c] = bounds[c + 1];
-    if (!chunk_copies(others(sx), stride_in(ca, sx), E, lo[c], hi[c], elem, bcp[c]) ||
-        !chunk_copies(others(SD), stride_in(ca, SD), E, lo[c], hi[c], elem, dcp[c]))
-      return false;
-  }
+  const auto plan_side = [&](bool rows, Side& sd) {
+    const std::vector<Axis>& ax = rows ? (v.swapped ? stt.n_axes : stt.m_axes) : (v.swapped ? stt.m_axes : stt.n_axes);
+    if (ax.empty()) return false;
+    sd.rows = rows;
+    sd.ca = &ax.back();
+    sd.E = sd.ca->extent;
+    sd.slot = rows ? sy : sx;
+    if (sd.E < 2) return false;
+    // Chunks that halve in size (E/2, E/4, ... down to about E/16, the rest
+    // last): the call ends with the kernels and the copy out of the last
+    // chunk only, so a small last chunk shortens that tail while the large
+    // first ones keep the kernels efficient. Every chunk keeps at least 256
+    // rows or columns.
+    sd.inner = (rows ? v.M : v.N) / sd.E;
+    std::vector<int64_t> bounds{0};
+    while (bounds.back() < sd.E) {
+      const int64_t left = sd.E - bounds.back();
+      int64_t take = left / 2;
+      if (take * 16 < sd.E || take * sd.inner < 256 || (left - take) * sd.inner < 256) take = left;
+      bounds.push_back(bounds.back() + take);
+    }
+    const int nc = (int)bounds.size() - 1;
+    if (nc < 2 || nc > 8) return false;
+    const Axis* ca = sd.ca;
+    const auto others = [&](int slot) {
+      std::vector<std::pair<int64_t, int64_t>> out;
+      for (const std::vector<Axis>* role : {&stt.m_axes, &stt.n_axes, &stt.k_axes, &stt.h_axes})
+        for (const Axis& a : *role)
+          if (&a != ca) out.push_back({a.extent, stride_in(a, slot)});
+      return out;
+    };
+    sd.xcp.assign(nc, {});
+    sd.dcp.assign(nc, {});
+    sd.lo.assign(nc, 0);
+    sd.hi.assign(nc, 0);
+    for (int c = 0; c < nc; ++c) {
+      sd.lo[c] = bounds[c];
+      sd.hi[c] = bounds[c + 1];
+      if (!chunk_copies(others(sd.slot), stride_in(*ca, sd.slot), sd.E, sd.lo[c], sd.hi[c], elem, sd.xcp[c]) ||
+          !chunk_copies(others(SD), stride_in(*ca, SD), sd.E, sd.lo[c], sd.hi[c], elem, sd.dcp[c]))
+        return false;
+    }
+    return true;
+  };
+  int64_t span_lo = 0;
+  size_t bytes_x = 0, bytes_y = 0;
+  span_bytes(p, sx, &span_lo, &bytes_x);
+  span_bytes(p, sy, &span_lo, &bytes_y);
+  Side sd;
+  const bool prefer_rows = bytes_y > bytes_x;
+  if (!plan_side(prefer_rows, sd) && !plan_side(!prefer_rows, sd)) return false;
+  const bool rows = sd.rows;
+  const int nchunks = (int)sd.lo.size();
+  const std::vector<int64_t>& lo = sd.lo;
+  const std::vector<int64_t>& hi = sd.hi;
+  const int64_t inner = sd.inner;
+  const int chunked = sd.slot, whole = rows ? sx : sy;
   // Kernel configuration per chunk (the plain path: one launch each, no split-K).
   const bool split = pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6;
   std::vector<PlainChoice> pcs(nchunks);
   size_t scratch = 0;
+  // Rows and columns of chunk c.
+  const auto chunk_m = [&](int c) { return rows ? (hi[c] - lo[c]) * inner : v.M; };
+  const auto chunk_n = [&](int c) { return rows ? v.N : (hi[c] - lo[c]) * inner; };
   if (split) {
+    // The whole operand's planes (packed once), then room for the largest
+    // chunk's planes.
     const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
-    int64_t ncmax = 0;
-    for (int c = 0; c < nchunks; ++c) ncmax = std::max(ncmax, (hi[c] - lo[c]) * inner_n);
-    const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, v.M, ncmax, v.K, v.H);
-    scratch = align_up((size_t)L.planes * L.H * L.m_pad * L.k_pad * 2, 256) +
-              align_up((size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2, 256) + dev::split_tail_bytes(L, ex.num_sms) +
-              1024;
+    int64_t mmax = 0, nmax = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      mmax = std::max(mmax, chunk_m(c));
+      nmax = std::max(nmax, chunk_n(c));
+    }
+    const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, mmax, nmax, v.K, v.H);
+    const size_t whole_planes = rows ? (size_t)L.planes * L.H * L.n_pad * L.k_pad * 2
+                                     : (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
+    const size_t chunk_planes = rows ? (size_t)Lc.planes * Lc.H * Lc.m_pad * Lc.k_pad * 2
+                                     : (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2;
+    scratch = align_up(whole_planes, 256) + align_up(chunk_planes, 256) + dev::split_tail_bytes(L, ex.num_sms) + 1024;
   } else if (pr.scheme == Scheme::Plain) {
     for (int c = 0; c < nchunks; ++c) {
-      const int64_t nc = (hi[c] - lo[c]) * inner_n;
+      const int64_t mc = chunk_m(c), nc = chunk_n(c);
       PlainChoice& pc = pcs[c];
-      if (dev::use_tiny_batched(v.M, nc, v.K, v.H)) return false;
-      dev::choose_plain_launch((int)p.dtype, pr.kernel_pin, v.M, nc, v.K, v.H, ex.num_sms, &pc.kernel, &pc.splits,
+      if (dev::use_tiny_batched(mc, nc, v.K, v.H)) return false;
+      dev::choose_plain_launch((int)p.dtype, pr.kernel_pin, mc, nc, v.K, v.H, ex.num_sms, &pc.kernel, &pc.splits,
                                &pc.chunk);
       if (pc.splits > 1) return false;
       if (dev::is_packed_kernel(pc.kernel))
-        scratch = std::max(scratch, dev::packed_workspace_bytes(dev::packed_layout(pc.kernel, v.M, nc, v.K, v.H)) + 512);
+        scratch = std::max(scratch, dev::packed_workspace_bytes(dev::packed_layout(pc.kernel, mc, nc, v.K, v.H)) + 512);
     }
   } else {
     return false;
@@ -968,52 +1015,64 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   check_cuda(cudaStreamWaitEvent(ex.copy_in, ev[2 * nchunks + 2], 0), "cudaStreamWaitEvent");
   check_cuda(cudaStreamWaitEvent(ex.copy_out, ev[2 * nchunks + 2], 0), "cudaStreamWaitEvent");
 
-  // In: the whole of the A' operand, then B' chunk by chunk.
-  const int sy = v.swapped ? SB : SA;
-  check_cuda(cudaMemcpyAsync(st[sy].buf, static_cast<const char*>(st[sy].host) + st[sy].lo_bytes, st[sy].bytes,
-                             cudaMemcpyHostToDevice, ex.copy_in),
+  // In: the whole operand, then the chunked one chunk by chunk.
+  check_cuda(cudaMemcpyAsync(st[whole].buf, static_cast<const char*>(st[whole].host) + st[whole].lo_bytes,
+                             st[whole].bytes, cudaMemcpyHostToDevice, ex.copy_in),
              "host-to-device copy");
   check_cuda(cudaEventRecord(ev[0], ex.copy_in), "cudaEventRecord");
   for (int c = 0; c < nchunks; ++c) {
-    for (const ChunkCopy& cc : bcp[c])
-      check_cuda(cudaMemcpy2DAsync(st[sx].dev_origin + cc.off, cc.pitch,
-                                   static_cast<const char*>(st[sx].host) + cc.off, cc.pitch, cc.width, cc.rows,
+    for (const ChunkCopy& cc : sd.xcp[c])
+      check_cuda(cudaMemcpy2DAsync(st[chunked].dev_origin + cc.off, cc.pitch,
+                                   static_cast<const char*>(st[chunked].host) + cc.off, cc.pitch, cc.width, cc.rows,
                                    cudaMemcpyHostToDevice, ex.copy_in),
                  "host-to-device chunk copy");
     check_cuda(cudaEventRecord(ev[1 + c], ex.copy_in), "cudaEventRecord");
   }
 
-  // Kernels, chunk by chunk, on the executor's stream.
+  // Kernels, chunk by chunk, on the executor's stream. The split schemes
+  // pack the whole operand's planes once and each chunk's planes before its
+  // GEMM.
   check_cuda(cudaStreamWaitEvent(ex.stream, ev[0], 0), "cudaStreamWaitEvent");
   const dev::GemmArgs g = build_args(pr, ex, alpha, Scalar{}, false, st[SA].dev_origin, st[SB].dev_origin, nullptr,
                                      st[SD].dev_origin);
   dev::SplitLayout L{};
-  char* ap = scratch_ptr;
+  char* wp = scratch_ptr;  // the whole operand's planes
+  char* cp = scratch_ptr;  // the current chunk's planes
   if (split) {
     L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
     Timed t(ex, "split_pack");
-    check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
+    check_cuda(dev::launch_split_pack_f32(g, rows ? 1 : 0, L, wp, ex.stream), "split pack of the whole operand");
+    cp = wp + align_up(rows ? (size_t)L.planes * L.H * L.n_pad * L.k_pad * 2 : (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2,
+                       256);
   }
-  char* bp = ap + align_up((size_t)L.planes * L.H * L.m_pad * L.k_pad * 2, 256);
   for (int c = 0; c < nchunks; ++c) {
     check_cuda(cudaStreamWaitEvent(ex.stream, ev[1 + c], 0), "cudaStreamWaitEvent");
     dev::GemmArgs gc = g;
-    const int64_t n0 = lo[c] * inner_n;
-    gc.N = (hi[c] - lo[c]) * inner_n;
-    gc.s.b_n += n0;
-    gc.s.c_n += n0;
-    gc.s.d_n += n0;
-    gc.s.blk_b_n = (n0 % dev::SCATTER_BLOCK == 0) ? g.s.blk_b_n + n0 / dev::SCATTER_BLOCK : nullptr;
+    const int64_t x0 = lo[c] * inner;
+    if (rows) {
+      gc.M = chunk_m(c);
+      gc.s.a_m += x0;
+      gc.s.c_m += x0;
+      gc.s.d_m += x0;
+      gc.s.blk_a_m = (x0 % dev::SCATTER_BLOCK == 0) ? g.s.blk_a_m + x0 / dev::SCATTER_BLOCK : nullptr;
+    } else {
+      gc.N = chunk_n(c);
+      gc.s.b_n += x0;
+      gc.s.c_n += x0;
+      gc.s.d_n += x0;
+      gc.s.blk_b_n = (x0 % dev::SCATTER_BLOCK == 0) ? g.s.blk_b_n + x0 / dev::SCATTER_BLOCK : nullptr;
+    }
     if (split) {
-      const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, v.M, gc.N, v.K, v.H);
-      char* tail = reinterpret_cast<char*>(
-          align_up((uintptr_t)(bp + (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2), 256));
+      const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, gc.M, gc.N, v.K, v.H);
+      const size_t cbytes = rows ? (size_t)Lc.planes * Lc.H * Lc.m_pad * Lc.k_pad * 2
+                                 : (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2;
+      char* tail = reinterpret_cast<char*>(align_up((uintptr_t)(cp + cbytes), 256));
       {
         Timed t(ex, "split_pack");
-        check_cuda(dev::launch_split_pack_f32(gc, 1, Lc, bp, ex.stream), "split pack B");
+        check_cuda(dev::launch_split_pack_f32(gc, rows ? 0 : 1, Lc, cp, ex.stream), "split pack of a chunk");
       }
       Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
-      check_cuda(dev::launch_tc_bf16_gemm(gc, Lc, ap, bp, (int)pr.scheme, ex.stream, tail),
+      check_cuda(dev::launch_tc_bf16_gemm(gc, Lc, rows ? cp : wp, rows ? wp : cp, (int)pr.scheme, ex.stream, tail),
                  "tcgen05 contraction launch");
     } else {
       launch_plain(pr, ex, gc, pcs[c], scratch_ptr, scratch);
@@ -1031,7 +1090,7 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   // waits for the last copy, so draining it covers the whole call.
   for (int c = 0; c < nchunks; ++c) {
     check_cuda(cudaStreamWaitEvent(ex.copy_out, ev[1 + nchunks + c], 0), "cudaStreamWaitEvent");
-    for (const ChunkCopy& cc : dcp[c])
+    for (const ChunkCopy& cc : sd.dcp[c])
       check_cuda(cudaMemcpy2DAsync(const_cast<char*>(static_cast<const char*>(st[SD].host)) + cc.off, cc.pitch,
                                    st[SD].dev_origin + cc.off, cc.pitch, cc.width, cc.rows, cudaMemcpyDeviceToHost,
                                    ex.copy_out),

@@ -73,7 +73,7 @@ def test_half_width_ffma_tiles(tp, ex, torch_cuda, orc, dt):
         want = oracle_ref(orc, dt, A, B, C, D, al, be, d0)
         st, got, p = run(tp, ex, torch_cuda, dt, A, B, C, D, al, be, kernel=HALF[dt])
         assert st == 0, tp.last_error()
-        assert "x64x16" in p.report()["family"], p.report()["family"]
+        assert "x64x32" in p.report()["family"], p.report()["family"]
         assert orc.rel_frobenius(got, want) <= plain_tol(dt), (m, n, k, kfast)
     m, n, k = 96, 80, 1500
     A = Op(rnd(rng, dt, m * k), [m, k], [1, m], [0, 2])

@@ -43,8 +43,9 @@ def launches(kt, fragment):
 @pytest.mark.parametrize("pinned", [True, False], ids=["pinned", "pageable"])
 def test_c2_layout_streamed_bf16x6(tp, torch_cuda, orc, pinned):
     """f32 D[m1,n1,m2,n2] = sum A[k1,m1,k2,m2] B[n1,k2,n2,k1], extents 48,
-    A with leading stride 2: B' chunks are pitched copies (k1 is B's outermost
-    axis), D chunks contiguous."""
+    A with leading stride 2: A spans twice B's bytes, so B is copied whole and
+    A goes in contiguous chunks of its outermost axis m2, D out in pitched
+    copies (m2 is not D's outermost axis)."""
     torch = torch_cuda
     e = 48
     sa = [2, 2 * e, 2 * e * e, 2 * e ** 3]
@@ -67,7 +68,7 @@ def test_c2_layout_streamed_bf16x6(tp, torch_cuda, orc, pinned):
     ex.set_profiling(True)
     tp.check(p.execute(ex, 1.0, pa, pb, 0.0, None, pd))
     kt = ex.kernel_times(reset=True)
-    assert launches(kt, "tc_bf16x6_gemm") >= 2, kt  # chunks of n2 (24, 12, 6, 6)
+    assert launches(kt, "tc_bf16x6_gemm") >= 2, kt  # chunks of m2 (24, 12, 6, 6)
     streamed = dview.copy()
     ex.set_streaming(False)
     tp.check(p.execute(ex, 1.0, pa, pb, 0.0, None, pd))
@@ -87,9 +88,10 @@ def test_c2_layout_streamed_bf16x6(tp, torch_cuda, orc, pinned):
 
 def test_plain_f64_streamed_and_a_layout_that_does_not_stream(tp, torch_cuda, orc):
     """A plain f64 product of host operands (2048 x 1536 x 1024, 40 MiB in
-    all) runs streamed; the same product with D's columns reversed (a negative
-    stride) cannot be chunked into pitched copies and runs unstreamed. Both
-    agree with the oracle at 1e-13."""
+    all) runs streamed (A, the larger operand, in row chunks); the same
+    product with D's columns reversed (a negative stride) cannot be chunked
+    into pitched copies on either side and runs unstreamed. Both agree with
+    the oracle at 1e-13."""
     m, n, k = 2048, 1536, 1024
     g = np.random.default_rng(20261203 + 78)
     a = g.uniform(-1, 1, m * k)
@@ -102,7 +104,7 @@ def test_plain_f64_streamed_and_a_layout_that_does_not_stream(tp, torch_cuda, or
     tp.check(p.execute(ex, 1.0, a.ctypes.data, b.ctypes.data, 0.0, None, d.ctypes.data))
     kt = ex.kernel_times(reset=True)
     fam = p.report()["family"]
-    assert launches(kt, fam) >= 2, (fam, kt)  # column chunks (768, 384, 384)
+    assert launches(kt, fam) >= 2, (fam, kt)  # row chunks (1024, 512, 256, 256)
     want = np.zeros(m * n)
     orc.packed_contract(1.0, orc.View(a, [m, k], [1, m], [0, 2]), orc.View(b, [k, n], [1, k], [2, 1]), 0.0, None,
                         orc.View(want, [m, n], [1, m], [0, 1]))

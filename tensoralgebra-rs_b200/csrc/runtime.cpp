@@ -936,51 +936,62 @@ bool enqueue_streamed(Product& pr, Executor& ex, Scalar alpha, const Item& it) {
   size_t bytes_x = 0, bytes_y = 0;
   span_bytes(p, sx, &span_lo, &bytes_x);
   span_bytes(p, sy, &span_lo, &bytes_y);
+  // Kernel configuration per chunk (the plain path: one launch each, no
+  // split-K); a side whose chunks would need split-K or the tiny-batch kernel
+  // is not taken.
+  const bool split = pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6;
+  if (!split && pr.scheme != Scheme::Plain) return false;
+  std::vector<PlainChoice> pcs;
+  size_t scratch = 0;
+  const auto configure = [&](const Side& sd) {
+    const int nc = (int)sd.lo.size();
+    const auto cm = [&](int c) { return sd.rows ? (sd.hi[c] - sd.lo[c]) * sd.inner : v.M; };
+    const auto cn = [&](int c) { return sd.rows ? v.N : (sd.hi[c] - sd.lo[c]) * sd.inner; };
+    pcs.assign(nc, PlainChoice{});
+    scratch = 0;
+    if (split) {
+      // The whole operand's planes (packed once), then room for the largest
+      // chunk's planes.
+      const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
+      int64_t mmax = 0, nmax = 0;
+      for (int c = 0; c < nc; ++c) {
+        mmax = std::max(mmax, cm(c));
+        nmax = std::max(nmax, cn(c));
+      }
+      const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, mmax, nmax, v.K, v.H);
+      const size_t whole_planes = sd.rows ? (size_t)L.planes * L.H * L.n_pad * L.k_pad * 2
+                                          : (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
+      const size_t chunk_planes = sd.rows ? (size_t)Lc.planes * Lc.H * Lc.m_pad * Lc.k_pad * 2
+                                          : (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2;
+      scratch = align_up(whole_planes, 256) + align_up(chunk_planes, 256) + dev::split_tail_bytes(L, ex.num_sms) + 1024;
+      return true;
+    }
+    for (int c = 0; c < nc; ++c) {
+      const int64_t mc = cm(c), ncols = cn(c);
+      PlainChoice& pc = pcs[c];
+      if (dev::use_tiny_batched(mc, ncols, v.K, v.H)) return false;
+      dev::choose_plain_launch((int)p.dtype, pr.kernel_pin, mc, ncols, v.K, v.H, ex.num_sms, &pc.kernel, &pc.splits,
+                               &pc.chunk);
+      if (pc.splits > 1) return false;
+      if (dev::is_packed_kernel(pc.kernel))
+        scratch = std::max(scratch,
+                           dev::packed_workspace_bytes(dev::packed_layout(pc.kernel, mc, ncols, v.K, v.H)) + 512);
+    }
+    return true;
+  };
   Side sd;
   const bool prefer_rows = bytes_y > bytes_x;
-  if (!plan_side(prefer_rows, sd) && !plan_side(!prefer_rows, sd)) return false;
+  if (!(plan_side(prefer_rows, sd) && configure(sd)) && !(plan_side(!prefer_rows, sd) && configure(sd)))
+    return false;
   const bool rows = sd.rows;
   const int nchunks = (int)sd.lo.size();
   const std::vector<int64_t>& lo = sd.lo;
   const std::vector<int64_t>& hi = sd.hi;
   const int64_t inner = sd.inner;
   const int chunked = sd.slot, whole = rows ? sx : sy;
-  // Kernel configuration per chunk (the plain path: one launch each, no split-K).
-  const bool split = pr.scheme == Scheme::Bf16x3 || pr.scheme == Scheme::Bf16x6;
-  std::vector<PlainChoice> pcs(nchunks);
-  size_t scratch = 0;
   // Rows and columns of chunk c.
   const auto chunk_m = [&](int c) { return rows ? (hi[c] - lo[c]) * inner : v.M; };
   const auto chunk_n = [&](int c) { return rows ? v.N : (hi[c] - lo[c]) * inner; };
-  if (split) {
-    // The whole operand's planes (packed once), then room for the largest
-    // chunk's planes.
-    const dev::SplitLayout L = dev::split_layout((int)pr.scheme, v.M, v.N, v.K, v.H);
-    int64_t mmax = 0, nmax = 0;
-    for (int c = 0; c < nchunks; ++c) {
-      mmax = std::max(mmax, chunk_m(c));
-      nmax = std::max(nmax, chunk_n(c));
-    }
-    const dev::SplitLayout Lc = dev::split_layout((int)pr.scheme, mmax, nmax, v.K, v.H);
-    const size_t whole_planes = rows ? (size_t)L.planes * L.H * L.n_pad * L.k_pad * 2
-                                     : (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
-    const size_t chunk_planes = rows ? (size_t)Lc.planes * Lc.H * Lc.m_pad * Lc.k_pad * 2
-                                     : (size_t)Lc.planes * Lc.H * Lc.n_pad * Lc.k_pad * 2;
-    scratch = align_up(whole_planes, 256) + align_up(chunk_planes, 256) + dev::split_tail_bytes(L, ex.num_sms) + 1024;
-  } else if (pr.scheme == Scheme::Plain) {
-    for (int c = 0; c < nchunks; ++c) {
-      const int64_t mc = chunk_m(c), nc = chunk_n(c);
-      PlainChoice& pc = pcs[c];
-      if (dev::use_tiny_batched(mc, nc, v.K, v.H)) return false;
-      dev::choose_plain_launch((int)p.dtype, pr.kernel_pin, mc, nc, v.K, v.H, ex.num_sms, &pc.kernel, &pc.splits,
-                               &pc.chunk);
-      if (pc.splits > 1) return false;
-      if (dev::is_packed_kernel(pc.kernel))
-        scratch = std::max(scratch, dev::packed_workspace_bytes(dev::packed_layout(pc.kernel, mc, nc, v.K, v.H)) + 512);
-    }
-  } else {
-    return false;
-  }
 
   // Workspace: the staged spans of A, B and D, then the kernels' scratch.
   Staged st[4];

@@ -88,10 +88,11 @@ def test_c2_layout_streamed_bf16x6(tp, torch_cuda, orc, pinned):
 
 def test_plain_f64_streamed_and_a_layout_that_does_not_stream(tp, torch_cuda, orc):
     """A plain f64 product of host operands (2048 x 1536 x 1024, 40 MiB in
-    all) runs streamed (A, the larger operand, in row chunks); the same
-    product with D's columns reversed (a negative stride) cannot be chunked
-    into pitched copies on either side and runs unstreamed. Both agree with
-    the oracle at 1e-13."""
+    all) runs streamed: row chunks of A, the larger operand, would be too
+    small for a wave of tiles without split-K, so it runs in column chunks of
+    B; the same product with D's columns reversed (a negative stride) cannot
+    be chunked into pitched copies on either side and runs unstreamed. Both
+    agree with the oracle at 1e-13."""
     m, n, k = 2048, 1536, 1024
     g = np.random.default_rng(20261203 + 78)
     a = g.uniform(-1, 1, m * k)
@@ -104,7 +105,7 @@ def test_plain_f64_streamed_and_a_layout_that_does_not_stream(tp, torch_cuda, or
     tp.check(p.execute(ex, 1.0, a.ctypes.data, b.ctypes.data, 0.0, None, d.ctypes.data))
     kt = ex.kernel_times(reset=True)
     fam = p.report()["family"]
-    assert launches(kt, fam) >= 2, (fam, kt)  # row chunks (1024, 512, 256, 256)
+    assert launches(kt, fam) >= 2, (fam, kt)  # column chunks (768, 384, 384)
     want = np.zeros(m * n)
     orc.packed_contract(1.0, orc.View(a, [m, k], [1, m], [0, 2]), orc.View(b, [k, n], [1, k], [2, 1]), 0.0, None,
                         orc.View(want, [m, n], [1, m], [0, 1]))

@@ -61,6 +61,12 @@ struct PanelArgs {
   int64_t rows_pad, k_pad;  // panel extents (of the embedded real problem)
   int64_t plane_stride;     // elements between the planes of 3m
   int64_t H;
+  // Block order over the 1-D grid of gx k-tiles x gy row-tiles x H batch
+  // entries: batch fastest (hfast, for operands whose batch index has the
+  // smallest stride, so CTAs resident together read neighbouring batch
+  // entries of the same lines) or k fastest.
+  int64_t gx = 0, gy = 0;
+  int hfast = 0;
 };
 
 // One 32-row x 32-k tile of the source operand (rows = m for A', n for B'):
@@ -83,15 +89,28 @@ __global__ void __launch_bounds__(256) plain_pack_kernel(const typename Elem<R, 
   __shared__ R tre[32][33];
   __shared__ R tim[CPLX ? 32 : 1][33];
   const int tid = threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32, h = blockIdx.z;
+  int64_t bx, by, h;
+  {
+    const int64_t b = blockIdx.x;
+    if (o.hfast) {
+      h = b % o.H;
+      bx = (b / o.H) % o.gx;
+      by = b / o.H / o.gx;
+    } else {
+      bx = b % o.gx;
+      by = (b / o.gx) % o.gy;
+      h = b / o.gx / o.gy;
+    }
+  }
+  const int64_t r0 = by * 32, k0 = bx * 32;
   const T* base = X + h_scat[h];
   // A whole tile on regular blocks of both vectors (block size 32 = the
   // tile): one base offset and two strides, 16-byte vectors along a
   // unit-stride fast index when aligned.
   int64_t rs = SCATTER_IRREGULAR, ks = SCATTER_IRREGULAR;
   if (rows_blk && k_blk && r0 + 32 <= nrows && k0 + 32 <= K) {
-    rs = rows_blk[blockIdx.y];
-    ks = k_blk[blockIdx.x];
+    rs = rows_blk[by];
+    ks = k_blk[bx];
   }
   if (rs != SCATTER_IRREGULAR && ks != SCATTER_IRREGULAR) {
     const T* tb = base + rows_scat[r0] + k_scat[k0];
@@ -666,14 +685,17 @@ template <class R, bool CPLX, int MODE>
 cudaError_t run_pack(const GemmArgs& g, int which, const PanelArgs& o, int64_t src_rows, int64_t src_k,
                      cudaStream_t st) {
   const int64_t gy = (src_rows + 31) / 32, gx = (src_k + 31) / 32;
-  if (gy > 65535 || o.H > 65535 || gx > 0x7fffffff) return cudaErrorInvalidConfiguration;
-  dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)o.H);
+  if (gx * gy * o.H > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  PanelArgs og = o;
+  og.gx = gx;
+  og.gy = gy;
+  const dim3 grid((unsigned)(gx * gy * o.H));
   using T = typename Elem<R, CPLX>::type;
   const bool a = which == 0;
   plain_pack_kernel<R, CPLX, MODE><<<grid, 256, 0, st>>>(
       static_cast<const T*>(a ? g.A : g.B), a ? g.s.a_m : g.s.b_n, a ? g.s.a_k : g.s.b_k, a ? g.s.h_a : g.s.h_b,
       a ? g.s.blk_a_m : g.s.blk_b_n, a ? g.s.blk_a_k : g.s.blk_b_k, a ? g.M : g.N, g.K, a ? g.a_kfast : g.b_kfast,
-      CPLX ? (a ? g.conj_a : g.conj_b) : 0, o);
+      CPLX ? (a ? g.conj_a : g.conj_b) : 0, og);
   return cudaGetLastError();
 }
 
@@ -765,6 +787,8 @@ cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* p
   char* pb = pa + ((a_bytes + 255) & ~size_t(255));
   PanelArgs oa{pa, L.m_pad, L.k_pad, L.H * L.m_pad * L.k_pad, L.H};
   PanelArgs ob{pb, L.n_pad, L.k_pad, L.H * L.n_pad * L.k_pad, L.H};
+  oa.hfast = L.a_hfast;
+  ob.hfast = L.b_hfast;
   cudaError_t r;
   switch (L.kernel) {
     case PLAIN_F32_PACKED_128x128:

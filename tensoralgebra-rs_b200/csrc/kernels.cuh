@@ -169,6 +169,9 @@ struct PackedLayout {
   int planes = 1;
   int64_t m_pad = 0, n_pad = 0, k_pad = 0;  // of the (embedded) real problem
   int64_t H = 0;
+  // The pack pass walks batch entries fastest for an operand whose batch
+  // index has the smallest stride (set by the caller; the layout is the same).
+  int a_hfast = 0, b_hfast = 0;
 };
 bool is_packed_kernel(int kernel);
 // The dtype (TAPP numbering) a packed family computes in.

@@ -464,7 +464,15 @@ void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const Plain
     if (!dev::packed_fits(c.kernel, g.M, g.N, g.K, g.H))
       throw Error(ERR_UNSUPPORTED, std::string("kernel family ") + dev::plain_kernel_name(c.kernel) +
                                        " cannot take this shape (batch, rows or depth beyond its grid)");
-    const dev::PackedLayout L = dev::packed_layout(c.kernel, g.M, g.N, g.K, g.H);
+    dev::PackedLayout L = dev::packed_layout(c.kernel, g.M, g.N, g.K, g.H);
+    {
+      const auto step = [](const std::vector<int64_t>& x) {
+        return x.size() > 1 ? std::llabs(x[1] - x[0]) : (long long)INT64_MAX;
+      };
+      const OrientedView& v = pr.view;
+      L.a_hfast = (v.H >= 8 && step(v.h_a) < std::min(step(v.a_m), step(v.a_k))) ? 1 : 0;
+      L.b_hfast = (v.H >= 8 && step(v.h_b) < std::min(step(v.b_n), step(v.b_k))) ? 1 : 0;
+    }
     const size_t panels = dev::packed_workspace_bytes(L);
     const size_t part = c.splits > 1 ? (size_t)c.splits * g.H * g.M * g.N * dtype_size(pr.problem.dtype) + 256 : 0;
     if (panels + part + 256 > scratch_bytes) throw Error(ERR_INTERNAL, "packed workspace too small");

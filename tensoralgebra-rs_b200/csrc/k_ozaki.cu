@@ -530,12 +530,16 @@ template <int S>
 struct OzCfg {
   static constexpr int A_TILE = OZ_BM * OZ_SK;  // bytes of one A plane tile
   static constexpr int B_TILE = OZ_BN * OZ_SK;
-  static constexpr int STAGE = S * (A_TILE + B_TILE);
-  // As many stages as fit in about 200 KB (2 at seven slices; 32-deep
-  // stages of 32-byte rows, twice as many, measured slower on B200).
-  static constexpr int STAGES = (200 * 1024 / STAGE) < 6 ? (200 * 1024 / STAGE) : 6;
-  static constexpr int RING = STAGES * STAGE;
-  static constexpr int BAR = (2 * STAGES + 2) * 8 + 16;
+  // A and B slice tiles of a k-block live in two rings of their own: three A
+  // stages when they fit beside two B stages (seven slices: 3 x 56 KB + 2 x
+  // 28 KB), so more operand bytes are in flight per SM than two whole
+  // 84 KB stages allow.
+  static constexpr int A_STAGE = S * A_TILE, B_STAGE = S * B_TILE;
+  static constexpr int LIMIT = 222 * 1024;
+  static constexpr int A_STAGES = (3 * A_STAGE + 2 * B_STAGE <= LIMIT) ? 3 : 2;
+  static constexpr int B_STAGES = (A_STAGES * A_STAGE + 3 * B_STAGE <= LIMIT) ? 3 : 2;
+  static constexpr int RING = A_STAGES * A_STAGE + B_STAGES * B_STAGE;
+  static constexpr int BAR = (2 * A_STAGES + 2 * B_STAGES + 3) * 8 + 16;
   static constexpr int SMEM = 1024 + RING + BAR;
   static constexpr int TMEM_COLS = (S * OZ_BN <= 256) ? 256 : 512;
   static_assert(S * OZ_BN <= 512, "one INT32 accumulator per diagonal must fit in TMEM");
@@ -566,12 +570,17 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   using Cfg = OzCfg<S>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* ring = smem;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::RING);
-  uint64_t* empty = full + Cfg::STAGES;
-  uint64_t* accf = empty + Cfg::STAGES;
+  uint8_t* ring_a = smem;
+  uint8_t* ring_b = smem + Cfg::A_STAGES * Cfg::A_STAGE;
+  uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + Cfg::RING);
+  uint64_t* empty_a = full_a + Cfg::A_STAGES;
+  uint64_t* full_b = empty_a + Cfg::A_STAGES;
+  uint64_t* empty_b = full_b + Cfg::B_STAGES;
+  uint64_t* accf = empty_b + Cfg::B_STAGES;
   uint64_t* tmem_empty = accf + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tmem_empty + 1);
+  uint64_t* mma_done = tmem_empty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+  __shared__ uint32_t consumed_s;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nk = (kb1 - kb0) * (OZ_BK / OZ_SK);  // ring stages per tile
@@ -579,10 +588,16 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   const int64_t ntiles = tiles_n * tiles_m * g.H;
 
   if (warp == 0 && lane == 0) {
-    for (int i = 0; i < Cfg::STAGES; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], 1);
+    for (int i = 0; i < Cfg::A_STAGES; ++i) {
+      mbar_init(&full_a[i], 1);
+      mbar_init(&empty_a[i], 1);
     }
+    for (int i = 0; i < Cfg::B_STAGES; ++i) {
+      mbar_init(&full_b[i], 1);
+      mbar_init(&empty_b[i], 1);
+    }
+    mbar_init(mma_done, 1);
+    consumed_s = 0xffffffffu;
     mbar_init(accf, 1);
     mbar_init(tmem_empty, OZ_EPI_WARPS);  // one arrival per epilogue warp
     fence_barrier_init();
@@ -598,6 +613,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  uint32_t issued_a = 0, issued_b = 0;  // k-blocks whose A / B tiles the producer issued
   if (warp == 0) {
     if (lane == 0) {
       uint32_t it = 0;
@@ -605,23 +621,30 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
       for (int64_t tile = blockIdx.x; alive && tile < ntiles; tile += gridDim.x) {
         const int64_t nt = tile % tiles_n, mt = (tile / tiles_n) % tiles_m, h = tile / (tiles_n * tiles_m);
         for (int i = 0; i < nk; ++i, ++it) {
-          const int st = (int)(it % Cfg::STAGES);
-          const uint32_t round = it / Cfg::STAGES;
-          if (!mbar_wait(&empty[st], (round & 1u) ^ 1u)) {
+          const int kx = kb0 * OZ_BK + i * OZ_SK;
+          const int sa = (int)(it % Cfg::A_STAGES), sb = (int)(it % Cfg::B_STAGES);
+          if (!mbar_wait(&empty_a[sa], ((it / Cfg::A_STAGES) & 1u) ^ 1u)) {
             atomicOr(g.status, STATUS_WAIT_TIMEOUT);
             alive = false;
             break;
           }
-          mbar_arrive_expect_tx(&full[st], (uint32_t)Cfg::STAGE);
-          uint8_t* sbase = ring + st * Cfg::STAGE;
-          const int kx = kb0 * OZ_BK + i * OZ_SK;
+          mbar_arrive_expect_tx(&full_a[sa], (uint32_t)Cfg::A_STAGE);
 #pragma unroll
           for (int p = 0; p < S; ++p)
-            tma_load_2d(sbase + p * Cfg::A_TILE, &tmA, &full[st], kx, (int)((p * g.H + h) * m_pad + mt * OZ_BM));
+            tma_load_2d(ring_a + sa * Cfg::A_STAGE + p * Cfg::A_TILE, &tmA, &full_a[sa], kx,
+                        (int)((p * g.H + h) * m_pad + mt * OZ_BM));
+          issued_a = it + 1;
+          if (!mbar_wait(&empty_b[sb], ((it / Cfg::B_STAGES) & 1u) ^ 1u)) {
+            atomicOr(g.status, STATUS_WAIT_TIMEOUT);
+            alive = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full_b[sb], (uint32_t)Cfg::B_STAGE);
 #pragma unroll
           for (int p = 0; p < S; ++p)
-            tma_load_2d(sbase + S * Cfg::A_TILE + p * Cfg::B_TILE, &tmB, &full[st], kx,
+            tma_load_2d(ring_b + sb * Cfg::B_STAGE + p * Cfg::B_TILE, &tmB, &full_b[sb], kx,
                         (int)((p * g.H + h) * n_pad + nt * OZ_BN));
+          issued_b = it + 1;
         }
       }
     }
@@ -637,15 +660,15 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         }
         tc_fence_after();
         for (int i = 0; i < nk; ++i, ++it) {
-          const int st = (int)(it % Cfg::STAGES);
-          const uint32_t round = it / Cfg::STAGES;
-          if (!mbar_wait(&full[st], round & 1u)) {
+          const int sa = (int)(it % Cfg::A_STAGES), sb = (int)(it % Cfg::B_STAGES);
+          if (!mbar_wait(&full_a[sa], (it / Cfg::A_STAGES) & 1u) || !mbar_wait(&full_b[sb], (it / Cfg::B_STAGES) & 1u)) {
             atomicOr(g.status, STATUS_WAIT_TIMEOUT);
             alive = false;
             break;
           }
           tc_fence_after();
-          const uint32_t sbase = smem_u32(ring + st * Cfg::STAGE);
+          const uint32_t abase = smem_u32(ring_a + sa * Cfg::A_STAGE);
+          const uint32_t bbase = smem_u32(ring_b + sb * Cfg::B_STAGE);
           // A slice t meets B slices u = 0 .. S-1-t, whose diagonals t + u
           // are the consecutive TMEM column blocks from t * 64 on, and whose
           // tiles are consecutive 64-row blocks of one K-major operand in
@@ -655,22 +678,29 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
           // MMAs cover every diagonal and start them on the first k-block.
 #pragma unroll
           for (int t = 0; t < S; ++t) {
-            const uint64_t ad = sdesc_sw64(sbase + t * Cfg::A_TILE);
+            const uint64_t ad = sdesc_sw64(abase + t * Cfg::A_TILE);
 #pragma unroll
             for (int u0 = 0; u0 < S - t; u0 += 4) {
               const int cnt = (S - t - u0) < 4 ? (S - t - u0) : 4;
               const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN * cnt);
-              const uint64_t bd = sdesc_sw64(sbase + S * Cfg::A_TILE + u0 * Cfg::B_TILE);
+              const uint64_t bd = sdesc_sw64(bbase + u0 * Cfg::B_TILE);
 #pragma unroll
               for (int kk = 0; kk < OZ_SK / 32; ++kk)
                 umma_i8(tmem + (uint32_t)((t + u0) * OZ_BN), ad + 2 * kk, bd + 2 * kk, idesc,
                         (i | t | kk) != 0 ? 1u : 0u);
             }
           }
-          umma_commit(&empty[st]);
+          umma_commit(&empty_a[sa]);
+          umma_commit(&empty_b[sb]);
         }
         if (alive) umma_commit(accf);
       }
+      // Every MMA issued has finished reading shared memory and writing TMEM
+      // before the CTA ends (bounded); `consumed_s` tells the producer which
+      // k-blocks' copies nobody waited for.
+      umma_commit(mma_done);
+      (void)mbar_wait(mma_done, 0u);
+      consumed_s = it;
     }
   } else {
     const int lane_base = 32 * (warp & 3);
@@ -750,6 +780,14 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
 
   tc_fence_before();
   __syncthreads();
+  // After a timeout: wait (bounded) for the copies still in flight into the
+  // stages the MMA warp did not consume.
+  if (warp == 0 && lane == 0 && consumed_s != 0xffffffffu) {
+    for (uint32_t k = consumed_s; k < issued_a; ++k)
+      (void)mbar_wait(&full_a[k % Cfg::A_STAGES], (k / Cfg::A_STAGES) & 1u);
+    for (uint32_t k = consumed_s; k < issued_b; ++k)
+      (void)mbar_wait(&full_b[k % Cfg::B_STAGES], (k / Cfg::B_STAGES) & 1u);
+  }
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, Cfg::TMEM_COLS);

@@ -191,7 +191,7 @@ int grouped_family(const Product& p, int policy) {
       break;
     default: break;
   }
-  return dev::choose_grouped_kernel(dt, p.view.M, p.view.N);
+  return dev::choose_grouped_kernel(dt, p.view.M, p.view.N, p.view.K);
 }
 
 std::string choice_name(const PlainChoice& c, int dtype) {

@@ -1116,6 +1116,112 @@ struct DmmaTileOp {
   }
 };
 
+// Short-K f64 tile of grouped lists (K <= 64, N <= BN; grouped only): 128
+// rows x BN columns with the whole K extent in one shared-memory stage (one
+// round of cp.async through the scatter vectors, whose k offsets are staged
+// with the row and column offsets), then FP64 FMAs from registers, 4 rows x
+// BN/8 columns per thread with rows 32 apart, so each warp store covers 32
+// consecutive rows of D. One barrier per tile and no fragment bookkeeping:
+// far fewer instructions per output than a DMMA tile spends on these shapes
+// (step 2 of the C4 updates, K = N <= 64), and 256 threads with two CTAs per
+// SM to hide the latency of a tile's single load round.
+template <int BN>
+struct SkinnyRing {
+  static constexpr int BM = 128, KMAX = 64, SA = BM + 4, SB = BN + 4;
+  static constexpr int BYTES = KMAX * (SA + SB) * 8;
+};
+
+template <int BN>
+__device__ __forceinline__ void skinny_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
+  using Ring = SkinnyRing<BN>;
+  constexpr int BM = Ring::BM, KMAX = Ring::KMAX, SA = Ring::SA, SB = Ring::SB, NT = 256;
+  constexpr int TN = BN / 8;  // columns per thread: 8 column groups, one per warp
+  extern __shared__ __align__(16) double skinny_ring[];
+  double* As = skinny_ring;              // [k][row], row stride SA
+  double* Bs = skinny_ring + KMAX * SA;  // [k][col], row stride SB
+  __shared__ int64_t am_s[BM], dm_s[BM], cm_s[BM], bn_s[BN], dn_s[BN], cn_s[BN], ak_s[KMAX], bk_s[KMAX];
+  const int tid = threadIdx.x;
+  const int64_t m0 = mtile * BM, n0 = ntile * BN;
+  const int64_t K = g.K < KMAX ? g.K : KMAX;  // the host routes only K <= KMAX here
+  for (int i = tid; i < BM; i += NT) {
+    const int64_t m = m0 + i;
+    const bool ok = m < g.M;
+    am_s[i] = ok ? g.s.a_m[m] : 0;
+    dm_s[i] = ok ? g.s.d_m[m] : 0;
+    cm_s[i] = (ok && !g.e.beta_zero) ? g.s.c_m[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int64_t n = n0 + i;
+    const bool ok = n < g.N;
+    bn_s[i] = ok ? g.s.b_n[n] : 0;
+    dn_s[i] = ok ? g.s.d_n[n] : 0;
+    cn_s[i] = (ok && !g.e.beta_zero) ? g.s.c_n[n] : 0;
+  }
+  for (int i = tid; i < K; i += NT) {
+    ak_s[i] = g.s.a_k[i];
+    bk_s[i] = g.s.b_k[i];
+  }
+  __syncthreads();
+  {
+    // All copies issued back to back, 16 k at a time (few offsets held in
+    // registers); elements past K or past the operand's rows are zero-filled.
+    constexpr int KB = 16;
+    AsyncGather<double, false, BM, KB, NT> ga;
+    AsyncGather<double, false, BN, KB, NT> gb;
+    ga.init(am_s, m0, g.M, g.a_kfast, tid);
+    gb.init(bn_s, n0, g.N, g.b_kfast, tid);
+    const double* Ab = static_cast<const double*>(g.A) + g.s.h_a[h];
+    const double* Bb = static_cast<const double*>(g.B) + g.s.h_b[h];
+    for (int64_t k0 = 0; k0 < K; k0 += KB) {
+      ga.load_idx_s(ak_s, 0, k0, K, g.a_kfast, tid);
+      gb.load_idx_s(bk_s, 0, k0, K, g.b_kfast, tid);
+      ga.issue(Ab, As + k0 * SA, As + k0 * SA, SA, g.a_kfast, tid);
+      gb.issue(Bb, Bs + k0 * SB, Bs + k0 * SB, SB, g.b_kfast, tid);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+  }
+  __syncthreads();
+  const int tx = tid & 31, ty = tid >> 5;
+  double acc[4][TN];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
+  for (int k = 0; k < K; ++k) {
+    double a[4], b[TN];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = As[k * SA + tx + 32 * i];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) b[j] = Bs[k * SB + ty * TN + j];  // the same for the whole warp
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
+  const double* Cb = static_cast<const double*>(g.C) + (g.e.beta_zero ? 0 : g.s.h_c[h]);
+  double* Db = static_cast<double*>(g.D) + g.s.h_d[h];
+#pragma unroll
+  for (int j = 0; j < TN; ++j) {
+    const int cc = ty * TN + j;
+    if (n0 + cc >= g.N) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int rr = tx + 32 * i;
+      if (m0 + rr < g.M)
+        epilogue_store<double, false>(g.e, acc[i][j], 0.0, Cb + cm_s[rr] + cn_s[cc], Db + dm_s[rr] + dn_s[cc]);
+    }
+  }
+}
+
+template <int BN>
+struct SkinnyTileOp {
+  static constexpr int NT = 256;
+  static constexpr int SMEM = SkinnyRing<BN>::BYTES;
+  static constexpr int MIN_BLOCKS = 2;
+  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) { skinny_tile<BN>(g, h, mt, nt); }
+};
+
 template <int BM, int BN>
 dim3 grid_for(const GemmArgs& g) {
   const int64_t splits = g.k_chunk ? (g.K + g.k_chunk - 1) / g.k_chunk : 1;
@@ -1142,6 +1248,8 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C64_PACKED_3M_64x32: return "sm100.c64.dmma884.tma.3m.64x32x16";
     case PLAIN_F32_PACKED_128x64: return "sm100.f32.simt.tma.packed.128x64x32";
     case PLAIN_C32_PACKED_1M_64x64: return "sm100.c32.simt.tma.1m.64x64x32";
+    case PLAIN_F64_SKINNY_128x32: return "sm100.f64.fma.skinny.128x32xk64";
+    case PLAIN_F64_SKINNY_128x64: return "sm100.f64.fma.skinny.128x64xk64";
   }
   return "auto";
 }
@@ -1176,7 +1284,7 @@ int choose_plain_kernel(int dtype, int64_t M, int64_t N, int64_t K, int64_t H, i
   return PLAIN_AUTO;
 }
 
-int choose_grouped_kernel(int dtype, int64_t M, int64_t N) {
+int choose_grouped_kernel(int dtype, int64_t M, int64_t N, int64_t K) {
   // In a grouped launch the list fills the GPU, so the tile is chosen for
   // reuse and padding alone: the large tile unless it wastes much more of its
   // area on padding than the small one.
@@ -1190,6 +1298,8 @@ int choose_grouped_kernel(int dtype, int64_t M, int64_t N) {
     const double padded = (double)((M + bm - 1) / bm * bm) * (double)((N + bn - 1) / bn * bn);
     return (double)M * (double)N / padded;
   };
+  // Short-K f64 items (K <= 64, N <= 64, some rows): the skinny FMA tile.
+  if (dtype == 1 && K <= 64 && N <= 64 && M >= 128) return N <= 32 ? PLAIN_F64_SKINNY_128x32 : PLAIN_F64_SKINNY_128x64;
   const int L = large[dtype & 3], S = small[dtype & 3];
   const int best = util(L) >= 0.8 * util(S) ? L : S;
   // Narrow outputs (N <= 32) of many rows: the tall 128 x 32 tile amortises
@@ -1363,6 +1473,8 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_C64_PACKED_3M_64x32: *bm = 64; *bn = 32; return;
     case PLAIN_F32_PACKED_128x64: *bm = 128; *bn = 64; return;
     case PLAIN_C32_PACKED_1M_64x64: *bm = 64; *bn = 64; return;
+    case PLAIN_F64_SKINNY_128x32: *bm = 128; *bn = 32; return;
+    case PLAIN_F64_SKINNY_128x64: *bm = 128; *bn = 64; return;
   }
   *bm = *bn = 0;
 }
@@ -1373,7 +1485,7 @@ namespace {
 // filled before any capture by prepare_grouped: the persistent grid must not
 // exceed what can be resident at once, or the CTAs beyond it start only when
 // others have drained the queue.
-int g_grouped_per_sm[16] = {};
+int g_grouped_per_sm[24] = {};
 
 template <class Op>
 cudaError_t grouped_prepare_op(int kernel) {
@@ -1405,6 +1517,8 @@ using GDmmaC64L = DmmaTileOp<true, 32, 16, 8>;
 using GDmmaC64S = DmmaTileOp<true, 16, 16, 8>;
 using GDmmaF64T = DmmaTileOp<false, 64, 16, 16>;
 using GDmmaC64T = DmmaTileOp<true, 64, 16, 8>;
+using GSkinny32 = SkinnyTileOp<32>;
+using GSkinny64 = SkinnyTileOp<64>;
 
 }  // namespace
 
@@ -1421,6 +1535,8 @@ cudaError_t prepare_grouped(int kernel) {
     case PLAIN_C64_DMMA_32x32: return grouped_prepare_op<GDmmaC64S>(kernel);
     case PLAIN_F64_DMMA_128x32: return grouped_prepare_op<GDmmaF64T>(kernel);
     case PLAIN_C64_DMMA_128x32: return grouped_prepare_op<GDmmaC64T>(kernel);
+    case PLAIN_F64_SKINNY_128x32: return grouped_prepare_op<GSkinny32>(kernel);
+    case PLAIN_F64_SKINNY_128x64: return grouped_prepare_op<GSkinny64>(kernel);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1457,6 +1573,12 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
       break;
     case PLAIN_C64_DMMA_128x32:
       grouped_launch_op<GDmmaC64T>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_SKINNY_128x32:
+      grouped_launch_op<GSkinny32>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_SKINNY_128x64:
+      grouped_launch_op<GSkinny64>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
     default: return cudaErrorInvalidValue;
   }

@@ -88,7 +88,11 @@ enum PlainKernel : int {
   PLAIN_C64_PACKED_3M_64x32 = 13,   // 3m: three real products per complex MAC
   PLAIN_F32_PACKED_128x64 = 14,     // half-width FFMA tiles, two CTAs per SM
   PLAIN_C32_PACKED_1M_64x64 = 15,
-  PLAIN_LAST = 15,
+  PLAIN_LAST = 15,  // the last family a caller can pin
+  // Short-K f64 tiles (K <= 64) of grouped lists only: chosen by the model for
+  // a list item, never pinned or used by single launches.
+  PLAIN_F64_SKINNY_128x32 = 16,
+  PLAIN_F64_SKINNY_128x64 = 17,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).
@@ -134,7 +138,7 @@ inline bool use_tiny_batched(int64_t M, int64_t N, int64_t K, int64_t H) {
 cudaError_t launch_tiny_batched(int dtype, const GemmArgs& g, const TinyStrides& hs, int num_sms, cudaStream_t st);
 
 // Family of an item inside a grouped launch (the list fills the GPU).
-int choose_grouped_kernel(int dtype, int64_t M, int64_t N);
+int choose_grouped_kernel(int dtype, int64_t M, int64_t N, int64_t K);
 // One-launch choice with split-K: the family (or `pinned`) and the number of
 // K chunks (1 = no split). Deep contractions with fewer large tiles than SMs
 // take the large tile and split K so that about two CTAs run per SM.

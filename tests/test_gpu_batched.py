@@ -72,3 +72,50 @@ def test_grouped_list_matches_per_item_and_the_full_contraction(tp, torch_cuda, 
         got = grouped[i].reshape((it["a"], it["s"], it["b"]), order="F")
         assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-12, i
     ex.close()
+
+
+def test_short_k_f64_list_on_the_skinny_tiles(tp, torch_cuda, orc):
+    """A grouped f64 list of short-K items (K <= 64, N <= 64, M >= 128: the
+    skinny FMA tiles of grouped lists), in both operand orders (k-fast and
+    rows-fast A), with alpha, beta and C, against the oracle at the plain
+    bound and against the same list run one launch per item."""
+    torch = torch_cuda
+    rng = np.random.default_rng(2026)
+    shapes = [(130, 8, 8, True), (257, 16, 33, False), (512, 32, 64, True), (128, 64, 17, False), (300, 40, 64, True),
+              (999, 1, 5, False), (200, 33, 1, True)]
+    ex = tp.Executor()
+    items, hosts, devs = [], [], []
+    for (m, n, k, kfast) in shapes:
+        a = rng.uniform(-1, 1, m * k)
+        b = rng.uniform(-1, 1, k * n)
+        c = rng.uniform(-1, 1, m * n)
+        sa = [k, 1] if kfast else [1, m]
+        la, lb, lc = [0, 2], [2, 1], [0, 1]
+        prob = tp.Problem.from_labels(tp.F64, tp.OperandSpec(tp.LayoutSpec([m, k], sa)),
+                                      tp.OperandSpec(tp.LayoutSpec([k, n], [1, k])),
+                                      tp.OperandSpec(tp.LayoutSpec([m, n], [1, m])), la, lb, lc,
+                                      c=tp.OperandSpec(tp.LayoutSpec([m, n], [1, m])), lc=lc)
+        t = {"a": torch.from_numpy(a).cuda(), "b": torch.from_numpy(b).cuda(), "c": torch.from_numpy(c).cuda(),
+             "d": torch.zeros(m * n, dtype=torch.float64, device="cuda")}
+        devs.append(t)
+        hosts.append((a, b, c, sa))
+        items.append(tp.Item(tp.Plan(prob), 0.75, t["a"].data_ptr(), t["b"].data_ptr(), t["d"].data_ptr(),
+                             beta=-1.5, c=t["c"].data_ptr()))
+    pb = tp.PreparedBatch(items)
+    torch.cuda.synchronize()
+
+    def run(grouping):
+        ex.set_grouping(grouping)
+        pb.run(ex)
+        ex.synchronize()
+        return [t["d"].cpu().numpy().copy() for t in devs]
+
+    grouped = run(True)
+    single = run(False)
+    for (m, n, k, kfast), (a, b, c, sa), g, s in zip(shapes, hosts, grouped, single):
+        want = np.zeros(m * n)
+        orc.packed_contract(0.75, orc.View(a, [m, k], sa, [0, 2]), orc.View(b, [k, n], [1, k], [2, 1]), -1.5,
+                            orc.View(c, [m, n], [1, m], [0, 1]), orc.View(want, [m, n], [1, m], [0, 1]))
+        assert orc.rel_frobenius(g, want) <= 1e-13, (m, n, k, kfast)
+        assert np.linalg.norm(s - g) <= 1e-13 * np.linalg.norm(g), (m, n, k, kfast)
+    ex.close()

@@ -1124,7 +1124,8 @@ struct DmmaTileOp {
 // consecutive rows of D. One barrier per tile and no fragment bookkeeping:
 // far fewer instructions per output than a DMMA tile spends on these shapes
 // (step 2 of the C4 updates, K = N <= 64), and 256 threads with two CTAs per
-// SM to hide the latency of a tile's single load round.
+// SM to hide the latency of a tile's single load round. BN = 16, 32 or 64
+// keeps the padding of narrow outputs at most 2x.
 template <int BN>
 struct SkinnyRing {
   static constexpr int BM = 128, KMAX = 64, SA = BM + 4, SB = BN + 4;
@@ -1250,6 +1251,7 @@ const char* plain_kernel_name(int k) {
     case PLAIN_C32_PACKED_1M_64x64: return "sm100.c32.simt.tma.1m.64x64x32";
     case PLAIN_F64_SKINNY_128x32: return "sm100.f64.fma.skinny.128x32xk64";
     case PLAIN_F64_SKINNY_128x64: return "sm100.f64.fma.skinny.128x64xk64";
+    case PLAIN_F64_SKINNY_128x16: return "sm100.f64.fma.skinny.128x16xk64";
   }
   return "auto";
 }
@@ -1299,7 +1301,8 @@ int choose_grouped_kernel(int dtype, int64_t M, int64_t N, int64_t K) {
     return (double)M * (double)N / padded;
   };
   // Short-K f64 items (K <= 64, N <= 64, some rows): the skinny FMA tile.
-  if (dtype == 1 && K <= 64 && N <= 64 && M >= 128) return N <= 32 ? PLAIN_F64_SKINNY_128x32 : PLAIN_F64_SKINNY_128x64;
+  if (dtype == 1 && K <= 64 && N <= 64 && M >= 128)
+    return N <= 16 ? PLAIN_F64_SKINNY_128x16 : N <= 32 ? PLAIN_F64_SKINNY_128x32 : PLAIN_F64_SKINNY_128x64;
   const int L = large[dtype & 3], S = small[dtype & 3];
   const int best = util(L) >= 0.8 * util(S) ? L : S;
   // Narrow outputs (N <= 32) of many rows: the tall 128 x 32 tile amortises
@@ -1475,6 +1478,7 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_C32_PACKED_1M_64x64: *bm = 64; *bn = 64; return;
     case PLAIN_F64_SKINNY_128x32: *bm = 128; *bn = 32; return;
     case PLAIN_F64_SKINNY_128x64: *bm = 128; *bn = 64; return;
+    case PLAIN_F64_SKINNY_128x16: *bm = 128; *bn = 16; return;
   }
   *bm = *bn = 0;
 }
@@ -1519,6 +1523,7 @@ using GDmmaF64T = DmmaTileOp<false, 64, 16, 16>;
 using GDmmaC64T = DmmaTileOp<true, 64, 16, 8>;
 using GSkinny32 = SkinnyTileOp<32>;
 using GSkinny64 = SkinnyTileOp<64>;
+using GSkinny16 = SkinnyTileOp<16>;
 
 }  // namespace
 
@@ -1537,6 +1542,7 @@ cudaError_t prepare_grouped(int kernel) {
     case PLAIN_C64_DMMA_128x32: return grouped_prepare_op<GDmmaC64T>(kernel);
     case PLAIN_F64_SKINNY_128x32: return grouped_prepare_op<GSkinny32>(kernel);
     case PLAIN_F64_SKINNY_128x64: return grouped_prepare_op<GSkinny64>(kernel);
+    case PLAIN_F64_SKINNY_128x16: return grouped_prepare_op<GSkinny16>(kernel);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1579,6 +1585,9 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
       break;
     case PLAIN_F64_SKINNY_128x64:
       grouped_launch_op<GSkinny64>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_SKINNY_128x16:
+      grouped_launch_op<GSkinny16>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
     default: return cudaErrorInvalidValue;
   }

@@ -93,6 +93,7 @@ enum PlainKernel : int {
   // a list item, never pinned or used by single launches.
   PLAIN_F64_SKINNY_128x32 = 16,
   PLAIN_F64_SKINNY_128x64 = 17,
+  PLAIN_F64_SKINNY_128x16 = 18,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).

@@ -413,12 +413,12 @@ struct AsyncGather {
 };
 
 // Shape of the DMMA stage ring (dynamic shared memory, see dmma_tile).
-template <bool CPLX, int WM, int WN, int BK>
+template <bool CPLX, int WM, int WN, int BK, int STG = 4>
 struct DmmaRing {
   static constexpr int BM = 2 * WM, BN = 2 * WN;
   static constexpr int SA = BM + 4, SB = BN + 4;  // strides = 4 (mod 16) doubles: conflict-free fragment reads
   static constexpr int NPL = CPLX ? 2 : 1;
-  static constexpr int STAGES = 4;
+  static constexpr int STAGES = STG;
   static constexpr int A_STAGE = NPL * BK * SA, B_STAGE = NPL * BK * SB;  // doubles
   static constexpr int BYTES = STAGES * (A_STAGE + B_STAGE) * 8;
 };
@@ -427,10 +427,10 @@ struct DmmaRing {
 // warp a WM x WN tile of 16x8 DMMA tiles, fed by a ring of STAGES
 // shared-memory stages (dynamic shared memory of DmmaRing::BYTES) filled with
 // cp.async.
-template <bool CPLX, int WM, int WN, int BK>
+template <bool CPLX, int WM, int WN, int BK, int STG = 4>
 __device__ __forceinline__ void dmma_tile_async(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile,
                                           int64_t split = 0) {
-  using Ring = DmmaRing<CPLX, WM, WN, BK>;
+  using Ring = DmmaRing<CPLX, WM, WN, BK, STG>;
   constexpr int BM = Ring::BM, BN = Ring::BN, NT = 128;
   constexpr int SA = Ring::SA, SB = Ring::SB;
   constexpr int NPL = Ring::NPL;
@@ -1105,14 +1105,14 @@ struct SimtRingTileOp {
     simt_tile_async<CPLX, BM, BN, BK, TM, TN>(g, h, mt, nt);
   }
 };
-template <bool CPLX, int WM, int WN, int BK>
+template <bool CPLX, int WM, int WN, int BK, int STG = 4, int MINB = (WM == 64 ? 2 : 3)>
 struct DmmaTileOp {
   // Grouped lists (many short-K tiles) take the cp.async ring for real f64 too.
   static constexpr int NT = 128;
-  static constexpr int SMEM = DmmaRing<CPLX, WM, WN, BK>::BYTES;
-  static constexpr int MIN_BLOCKS = WM == 64 ? 2 : 3;  // the tall tile's ring needs 86 KB
+  static constexpr int SMEM = DmmaRing<CPLX, WM, WN, BK, STG>::BYTES;
+  static constexpr int MIN_BLOCKS = MINB;  // the tall tile's ring needs 86 KB
   __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
-    dmma_tile_async<CPLX, WM, WN, BK>(g, h, mt, nt);
+    dmma_tile_async<CPLX, WM, WN, BK, STG>(g, h, mt, nt);
   }
 };
 
@@ -1126,15 +1126,15 @@ struct DmmaTileOp {
 // (step 2 of the C4 updates, K = N <= 64), and 256 threads with two CTAs per
 // SM to hide the latency of a tile's single load round. BN = 16, 32 or 64
 // keeps the padding of narrow outputs at most 2x.
-template <int BN>
+template <int BN, int KM>
 struct SkinnyRing {
-  static constexpr int BM = 128, KMAX = 64, SA = BM + 4, SB = BN + 4;
+  static constexpr int BM = 128, KMAX = KM, SA = BM + 4, SB = BN + 4;
   static constexpr int BYTES = KMAX * (SA + SB) * 8;
 };
 
-template <int BN>
+template <int BN, int KM>
 __device__ __forceinline__ void skinny_tile(const GemmArgs& g, int64_t h, int64_t mtile, int64_t ntile) {
-  using Ring = SkinnyRing<BN>;
+  using Ring = SkinnyRing<BN, KM>;
   constexpr int BM = Ring::BM, KMAX = Ring::KMAX, SA = Ring::SA, SB = Ring::SB, NT = 256;
   constexpr int TN = BN / 8;  // columns per thread: 8 column groups, one per warp
   extern __shared__ __align__(16) double skinny_ring[];
@@ -1215,12 +1215,18 @@ __device__ __forceinline__ void skinny_tile(const GemmArgs& g, int64_t h, int64_
   }
 }
 
-template <int BN>
+// KM = 64 takes K <= 64 at two CTAs per SM; KM = 32 (K <= 32, most of the
+// C4 step-2 items) halves the A stage and runs three CTAs per SM (four with
+// 16 columns, whose accumulators leave room in 64 registers). Occupancy is
+// what these tiles need: their one load round per tile is latency.
+template <int BN, int KM>
 struct SkinnyTileOp {
   static constexpr int NT = 256;
-  static constexpr int SMEM = SkinnyRing<BN>::BYTES;
-  static constexpr int MIN_BLOCKS = 2;
-  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) { skinny_tile<BN>(g, h, mt, nt); }
+  static constexpr int SMEM = SkinnyRing<BN, KM>::BYTES;
+  static constexpr int MIN_BLOCKS = KM == 32 ? (BN == 16 ? 4 : 3) : 2;
+  __device__ static void run(const GemmArgs& g, int64_t h, int64_t mt, int64_t nt) {
+    skinny_tile<BN, KM>(g, h, mt, nt);
+  }
 };
 
 template <int BM, int BN>
@@ -1252,6 +1258,8 @@ const char* plain_kernel_name(int k) {
     case PLAIN_F64_SKINNY_128x32: return "sm100.f64.fma.skinny.128x32xk64";
     case PLAIN_F64_SKINNY_128x64: return "sm100.f64.fma.skinny.128x64xk64";
     case PLAIN_F64_SKINNY_128x16: return "sm100.f64.fma.skinny.128x16xk64";
+    case PLAIN_F64_SKINNY_128x16_K32: return "sm100.f64.fma.skinny.128x16xk32";
+    case PLAIN_F64_SKINNY_128x32_K32: return "sm100.f64.fma.skinny.128x32xk32";
   }
   return "auto";
 }
@@ -1301,6 +1309,8 @@ int choose_grouped_kernel(int dtype, int64_t M, int64_t N, int64_t K) {
     return (double)M * (double)N / padded;
   };
   // Short-K f64 items (K <= 64, N <= 64, some rows): the skinny FMA tile.
+  if (dtype == 1 && K <= 32 && N <= 32 && M >= 128)
+    return N <= 16 ? PLAIN_F64_SKINNY_128x16_K32 : PLAIN_F64_SKINNY_128x32_K32;
   if (dtype == 1 && K <= 64 && N <= 64 && M >= 128)
     return N <= 16 ? PLAIN_F64_SKINNY_128x16 : N <= 32 ? PLAIN_F64_SKINNY_128x32 : PLAIN_F64_SKINNY_128x64;
   const int L = large[dtype & 3], S = small[dtype & 3];
@@ -1479,6 +1489,8 @@ void plain_tile_shape(int kernel, int* bm, int* bn) {
     case PLAIN_F64_SKINNY_128x32: *bm = 128; *bn = 32; return;
     case PLAIN_F64_SKINNY_128x64: *bm = 128; *bn = 64; return;
     case PLAIN_F64_SKINNY_128x16: *bm = 128; *bn = 16; return;
+    case PLAIN_F64_SKINNY_128x16_K32: *bm = 128; *bn = 16; return;
+    case PLAIN_F64_SKINNY_128x32_K32: *bm = 128; *bn = 32; return;
   }
   *bm = *bn = 0;
 }
@@ -1515,15 +1527,21 @@ void grouped_launch_op(int kernel, const GroupItem* items, const int64_t* tile_s
 using GSimtF32L = SimtTileOp<float, false, 128, 128, 16, 8, 8>;
 using GSimtF32S = SimtTileOp<float, false, 64, 64, 16, 4, 4>;
 using GSimtC32 = SimtRingTileOp<true, 64, 64, 16, 4, 4>;
-using GDmmaF64L = DmmaTileOp<false, 32, 32, 16>;
-using GDmmaF64S = DmmaTileOp<false, 16, 16, 16>;
+// The f64 64 x 64 list tile runs three 16-deep stages (52 KB) and four CTAs
+// per SM (128 registers), trading a stage for a fourth CTA: list tiles are
+// short-K and latency-bound.
+using GDmmaF64L = DmmaTileOp<false, 32, 32, 16, 3, 4>;
+// The 32 x 32 list tiles fit five CTAs per SM in 96 registers.
+using GDmmaF64S = DmmaTileOp<false, 16, 16, 16, 4, 5>;
 using GDmmaC64L = DmmaTileOp<true, 32, 16, 8>;
-using GDmmaC64S = DmmaTileOp<true, 16, 16, 8>;
+using GDmmaC64S = DmmaTileOp<true, 16, 16, 8, 4, 5>;
 using GDmmaF64T = DmmaTileOp<false, 64, 16, 16>;
 using GDmmaC64T = DmmaTileOp<true, 64, 16, 8>;
-using GSkinny32 = SkinnyTileOp<32>;
-using GSkinny64 = SkinnyTileOp<64>;
-using GSkinny16 = SkinnyTileOp<16>;
+using GSkinny32 = SkinnyTileOp<32, 64>;
+using GSkinny64 = SkinnyTileOp<64, 64>;
+using GSkinny16 = SkinnyTileOp<16, 64>;
+using GSkinny16s = SkinnyTileOp<16, 32>;
+using GSkinny32s = SkinnyTileOp<32, 32>;
 
 }  // namespace
 
@@ -1543,6 +1561,8 @@ cudaError_t prepare_grouped(int kernel) {
     case PLAIN_F64_SKINNY_128x32: return grouped_prepare_op<GSkinny32>(kernel);
     case PLAIN_F64_SKINNY_128x64: return grouped_prepare_op<GSkinny64>(kernel);
     case PLAIN_F64_SKINNY_128x16: return grouped_prepare_op<GSkinny16>(kernel);
+    case PLAIN_F64_SKINNY_128x16_K32: return grouped_prepare_op<GSkinny16s>(kernel);
+    case PLAIN_F64_SKINNY_128x32_K32: return grouped_prepare_op<GSkinny32s>(kernel);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1588,6 +1608,12 @@ cudaError_t launch_grouped(int kernel, const GroupItem* items, const int64_t* ti
       break;
     case PLAIN_F64_SKINNY_128x16:
       grouped_launch_op<GSkinny16>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_SKINNY_128x16_K32:
+      grouped_launch_op<GSkinny16s>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
+      break;
+    case PLAIN_F64_SKINNY_128x32_K32:
+      grouped_launch_op<GSkinny32s>(kernel, items, tile_start, nitems, counter, status, num_sms, st);
       break;
     default: return cudaErrorInvalidValue;
   }

@@ -94,6 +94,8 @@ enum PlainKernel : int {
   PLAIN_F64_SKINNY_128x32 = 16,
   PLAIN_F64_SKINNY_128x64 = 17,
   PLAIN_F64_SKINNY_128x16 = 18,
+  PLAIN_F64_SKINNY_128x16_K32 = 19,  // K <= 32: half the A stage, three CTAs per SM
+  PLAIN_F64_SKINNY_128x32_K32 = 20,
 };
 
 // dtype: 0 f32, 1 f64, 2 c32, 3 c64 (TAPP numbering).

@@ -82,7 +82,7 @@ def test_short_k_f64_list_on_the_skinny_tiles(tp, torch_cuda, orc):
     torch = torch_cuda
     rng = np.random.default_rng(2026)
     shapes = [(130, 8, 8, True), (257, 16, 33, False), (512, 32, 64, True), (128, 64, 17, False), (300, 40, 64, True),
-              (999, 1, 5, False), (200, 33, 1, True)]
+              (999, 1, 5, False), (200, 33, 1, True), (260, 24, 30, False)]
     ex = tp.Executor()
     items, hosts, devs = [], [], []
     for (m, n, k, kfast) in shapes:

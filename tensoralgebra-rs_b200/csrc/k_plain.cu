@@ -1082,7 +1082,21 @@ __global__ void __launch_bounds__(NT, Tile::MIN_BLOCKS) grouped_kernel(const Gro
     }
     const int64_t local = t - tile_start[it];
     const int64_t tn = items[it].tiles_n, tm = items[it].tiles_m;
-    Tile::run(sg, local / (tm * tn), (local / tn) % tm, local % tn);
+    // Tile coordinates (batch, row tile, column tile); 32-bit divisions when
+    // the item's tile counts fit, as they do for any realistic item.
+    int64_t th, tmi, tni;
+    if (local < 0x7fffffff && tm * tn < 0x7fffffff) {
+      const uint32_t l = (uint32_t)local, per = (uint32_t)(tm * tn), n32 = (uint32_t)tn;
+      const uint32_t hq = l / per, r = l - hq * per, mq = r / n32;
+      th = hq;
+      tmi = mq;
+      tni = r - mq * n32;
+    } else {
+      th = local / (tm * tn);
+      tmi = (local / tn) % tm;
+      tni = local % tn;
+    }
+    Tile::run(sg, th, tmi, tni);
     __syncthreads();
   }
 }

@@ -97,17 +97,20 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def profiled_traffic(kernel):
+def profiled_traffic(kernel, config=None):
     """DRAM bytes per launch of `kernel` from the committed ncu summaries
-    (profiles/*.md lines `traffic_bytes_per_launch[<kernel>]: <bytes>`)."""
+    (profiles/*.md lines `traffic_bytes_per_launch[<config>/<kernel>]: <bytes>`
+    for one configuration's launch, else `traffic_bytes_per_launch[<kernel>]`)."""
     import glob
     import re
 
-    for path in sorted(glob.glob(os.path.join(REPO, "profiles", "*.md"))):
-        with open(path) as f:
-            m = re.search(r"traffic_bytes_per_launch\[" + re.escape(kernel) + r"\]:\s*(\d+)", f.read())
-        if m:
-            return int(m.group(1)), os.path.relpath(path, REPO)
+    keys = ([f"{config}/{kernel}"] if config else []) + [kernel]
+    for key in keys:
+        for path in sorted(glob.glob(os.path.join(REPO, "profiles", "*.md"))):
+            with open(path) as f:
+                m = re.search(r"traffic_bytes_per_launch\[" + re.escape(key) + r"\]:\s*(\d+)", f.read())
+            if m:
+                return int(m.group(1)), os.path.relpath(path, REPO)
     return None, None
 
 
@@ -617,7 +620,7 @@ def run_config(args, tp, torch, ex):
         if not kt:
             return
         k_ms = kt["ms"] / (steps or args.steps)
-        traffic, src = profiled_traffic(kernel)
+        traffic, src = profiled_traffic(kernel, cfg)
         entry["roofline"] = {"kernel": kernel, "pipe": peak_name, "achieved": pipe_flop_per_step / (k_ms * 1e-3) / 1e12,
                              "peak": pipe[peak_name], "unit": "TFLOP/s",
                              "frac": pipe_flop_per_step / (k_ms * 1e-3) / 1e12 / pipe[peak_name],

@@ -446,6 +446,21 @@ struct Timed {
   }
 };
 
+// Side streams and fork/join events of the executor, created on first use
+// (the executor's lock serialises the calls that use them).
+void ensure_side(Executor& ex, size_t streams, size_t events) {
+  while (ex.family_streams.size() < streams) {
+    cudaStream_t s = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate(side)");
+    ex.family_streams.push_back(s);
+  }
+  while (ex.family_events.size() < events) {
+    cudaEvent_t e = nullptr;
+    check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(side)");
+    ex.family_events.push_back(e);
+  }
+}
+
 // One plain execution in the configuration `c` (scratch: the split-K partials).
 void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const PlainChoice& c, char* scratch,
                   size_t scratch_bytes) {
@@ -545,9 +560,17 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
       char* bp = ap + (size_t)L.planes * L.H * L.m_pad * L.k_pad * 2;
       char* tail = reinterpret_cast<char*>(align_up((uintptr_t)(ap + planes_bytes), 256));
       {
+        // The two packs are independent: B's runs on a side stream forked
+        // from the executor's stream and joined back before the GEMM, so the
+        // two memory-bound passes overlap (and fill each other's tails).
         Timed t(ex, "split_pack");
+        ensure_side(ex, 1, 2);
+        check_cuda(cudaEventRecord(ex.family_events[0], ex.stream), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(ex.family_streams[0], ex.family_events[0], 0), "cudaStreamWaitEvent");
+        check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, ex.family_streams[0]), "split pack B");
+        check_cuda(cudaEventRecord(ex.family_events[1], ex.family_streams[0]), "cudaEventRecord");
         check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
-        check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, ex.stream), "split pack B");
+        check_cuda(cudaStreamWaitEvent(ex.stream, ex.family_events[1], 0), "cudaStreamWaitEvent");
       }
       Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
       check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream, tail),
@@ -1409,18 +1432,7 @@ cudaError_t launch_group_set(Executor& ex, const GroupSet& gs, cudaStream_t st) 
     for (size_t l = 0; l < nf && e == cudaSuccess; ++l) e = launch(l, st);
     return e;
   }
-  while (ex.family_streams.size() < nf - 1) {
-    cudaStream_t s = nullptr;
-    const cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return e;
-    ex.family_streams.push_back(s);
-  }
-  while (ex.family_events.size() < nf) {
-    cudaEvent_t ev = nullptr;
-    const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-    if (e != cudaSuccess) return e;
-    ex.family_events.push_back(ev);
-  }
+  ensure_side(ex, nf - 1, nf);
   cudaError_t e = cudaEventRecord(ex.family_events[0], st);
   for (size_t l = 1; l < nf && e == cudaSuccess; ++l) e = cudaStreamWaitEvent(ex.family_streams[l - 1], ex.family_events[0], 0);
   if (e == cudaSuccess) e = launch(0, st);
@@ -1521,6 +1533,14 @@ Executor::Graph& capture_grouped(Executor& ex, uint64_t key, const std::vector<i
       cudaFree(gr.buf);
       check_cuda(e, "cudaStreamCreate(capture)");
     }
+  }
+  // Side streams and events for concurrent family launches exist before the
+  // capture starts (nothing is created while it runs).
+  try {
+    ensure_side(ex, gs.family.size(), gs.family.size() + 1);
+  } catch (...) {
+    cudaFree(gr.buf);
+    throw;
   }
   const cudaError_t begin = cudaStreamBeginCapture(ex.capture_stream, cudaStreamCaptureModeThreadLocal);
   if (begin != cudaSuccess) {

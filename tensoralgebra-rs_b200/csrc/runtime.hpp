@@ -114,9 +114,9 @@ struct Executor {
   bool streaming = true;
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> stream_events;
-  // Side streams of a grouped submission whose items fall into several tile
-  // families: the families' persistent launches run concurrently (fork and
-  // join through events), so a later family fills the tail of an earlier one.
+  // Side streams and fork/join events: the persistent launches of a grouped
+  // submission's tile families run concurrently (a later family fills the
+  // tail of an earlier one), and so do the two split-precision packs.
   std::vector<cudaStream_t> family_streams;
   std::vector<cudaEvent_t> family_events;
 

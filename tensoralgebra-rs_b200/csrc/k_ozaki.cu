@@ -915,7 +915,7 @@ static void pack_operand(const double* X, const int64_t* rows_s, const int64_t* 
   }
 }
 
-cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st) {
+cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st, cudaStream_t st_b) {
   int8_t* ap = static_cast<int8_t*>(ws);
   int8_t* bp = ap + (size_t)L.slices * L.H * L.m_pad * L.k_pad;
   int* ea = reinterpret_cast<int*>(bp + (size_t)L.slices * L.H * L.n_pad * L.k_pad);
@@ -928,12 +928,12 @@ cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws,
     pack_operand<true>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast, L.a_hfast,
                        0, g.conj_a, ea, ap, st);
     pack_operand<true>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1,
-                       g.conj_b, eb, bp, st);
+                       g.conj_b, eb, bp, st_b);
   } else {
     pack_operand<false>(A, g.s.a_m, g.s.a_k, g.s.h_a, g.M, g.K, L, L.exp_a_pad, L.m_pad, g.a_kfast,
                         L.a_hfast, 0, 0, ea, ap, st);
     pack_operand<false>(B, g.s.b_n, g.s.b_k, g.s.h_b, g.N, g.K, L, L.n_pad, L.n_pad, g.b_kfast, L.b_hfast, 1, 0,
-                        eb, bp, st);
+                        eb, bp, st_b);
   }
   return cudaGetLastError();
 }

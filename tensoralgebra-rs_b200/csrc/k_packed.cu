@@ -780,7 +780,8 @@ size_t packed_workspace_bytes(const PackedLayout& L) {
   return ((a + 255) & ~size_t(255)) + ((b + 255) & ~size_t(255)) + 256;
 }
 
-cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* panels, cudaStream_t st) {
+cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* panels, cudaStream_t st,
+                               cudaStream_t st_b) {
   const size_t e = elem_bytes_of(L.kernel);
   const size_t a_bytes = (size_t)L.planes * L.H * L.m_pad * L.k_pad * e;
   char* pa = static_cast<char*>(panels);
@@ -795,20 +796,20 @@ cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* p
     case PLAIN_F32_PACKED_128x64:
       r = run_pack<float, false, PM_ROWS_FAST>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<float, false, PM_ROWS_FAST>(g, 1, ob, L.n_pad, L.k_pad, st);
+      return run_pack<float, false, PM_ROWS_FAST>(g, 1, ob, L.n_pad, L.k_pad, st_b);
     case PLAIN_C32_PACKED_1M_64x128:
     case PLAIN_C32_PACKED_1M_64x64:
       r = run_pack<float, true, PM_1M_A>(g, 0, oa, L.m_pad / 2, (L.k_pad + 1) / 2, st);
       if (r != cudaSuccess) return r;
-      return run_pack<float, true, PM_1M_B>(g, 1, ob, L.n_pad, (L.k_pad + 1) / 2, st);
+      return run_pack<float, true, PM_1M_B>(g, 1, ob, L.n_pad, (L.k_pad + 1) / 2, st_b);
     case PLAIN_F64_PACKED_64x64:
       r = run_pack<double, false, PM_K_FAST>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<double, false, PM_K_FAST>(g, 1, ob, L.n_pad, L.k_pad, st);
+      return run_pack<double, false, PM_K_FAST>(g, 1, ob, L.n_pad, L.k_pad, st_b);
     case PLAIN_C64_PACKED_3M_64x32:
       r = run_pack<double, true, PM_3M>(g, 0, oa, L.m_pad, L.k_pad, st);
       if (r != cudaSuccess) return r;
-      return run_pack<double, true, PM_3M>(g, 1, ob, L.n_pad, L.k_pad, st);
+      return run_pack<double, true, PM_3M>(g, 1, ob, L.n_pad, L.k_pad, st_b);
   }
   return cudaErrorInvalidValue;
 }

@@ -188,7 +188,9 @@ bool packed_fits(int kernel, int64_t M, int64_t N, int64_t K, int64_t H);
 PackedLayout packed_layout(int kernel, int64_t M, int64_t N, int64_t K, int64_t H);
 size_t packed_workspace_bytes(const PackedLayout& L);
 // Pack both operands into `panels` (packed_workspace_bytes of device memory).
-cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* panels, cudaStream_t st);
+// A' on `st`, B' on `st_b` (the same stream or one the caller joins back).
+cudaError_t launch_packed_pack(const GemmArgs& g, const PackedLayout& L, void* panels, cudaStream_t st,
+                               cudaStream_t st_b);
 // The tile kernel over the panels (with the epilogue, or split-K partials).
 cudaError_t launch_packed_gemm(const GemmArgs& g, const PackedLayout& L, const void* panels, cudaStream_t st);
 
@@ -235,7 +237,8 @@ struct OzakiLayout {
 OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K, int64_t H);
 size_t ozaki_workspace_bytes(const OzakiLayout& L);
 // Exponent scan and slicing of A' and B' into the workspace.
-cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st);
+// A' on `st`, B' on `st_b` (the same stream or one the caller joins back).
+cudaError_t launch_ozaki_pack(const GemmArgs& g, const OzakiLayout& L, void* ws, cudaStream_t st, cudaStream_t st_b);
 // Slice products over k-blocks [kb0, kb1) with the recombining epilogue.
 cudaError_t launch_ozaki_gemm(const GemmArgs& g, const OzakiLayout& L, const void* ws, int kb0, int kb1,
                               cudaStream_t st);

@@ -461,6 +461,20 @@ void ensure_side(Executor& ex, size_t streams, size_t events) {
   }
 }
 
+// Fork a side stream off the executor's stream (its work starts after what is
+// already queued there) and join it back (the executor's stream waits for
+// everything queued on the side).
+cudaStream_t fork_side(Executor& ex) {
+  ensure_side(ex, 1, 2);
+  check_cuda(cudaEventRecord(ex.family_events[0], ex.stream), "cudaEventRecord");
+  check_cuda(cudaStreamWaitEvent(ex.family_streams[0], ex.family_events[0], 0), "cudaStreamWaitEvent");
+  return ex.family_streams[0];
+}
+void join_side(Executor& ex) {
+  check_cuda(cudaEventRecord(ex.family_events[1], ex.family_streams[0]), "cudaEventRecord");
+  check_cuda(cudaStreamWaitEvent(ex.stream, ex.family_events[1], 0), "cudaStreamWaitEvent");
+}
+
 // One plain execution in the configuration `c` (scratch: the split-K partials).
 void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const PlainChoice& c, char* scratch,
                   size_t scratch_bytes) {
@@ -499,7 +513,10 @@ void launch_plain(Product& pr, Executor& ex, const dev::GemmArgs& g, const Plain
     }
     {
       Timed t(ex, "plain_pack");
-      check_cuda(dev::launch_packed_pack(gs, L, pp, ex.stream), "plain pack launch");
+      // A' and B' packs overlap: B' on a side stream joined back before the GEMM.
+      cudaStream_t side = fork_side(ex);
+      check_cuda(dev::launch_packed_pack(gs, L, pp, ex.stream, side), "plain pack launch");
+      join_side(ex);
     }
     {
       Timed t(ex, dev::plain_kernel_name(c.kernel));
@@ -564,13 +581,10 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
         // from the executor's stream and joined back before the GEMM, so the
         // two memory-bound passes overlap (and fill each other's tails).
         Timed t(ex, "split_pack");
-        ensure_side(ex, 1, 2);
-        check_cuda(cudaEventRecord(ex.family_events[0], ex.stream), "cudaEventRecord");
-        check_cuda(cudaStreamWaitEvent(ex.family_streams[0], ex.family_events[0], 0), "cudaStreamWaitEvent");
-        check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, ex.family_streams[0]), "split pack B");
-        check_cuda(cudaEventRecord(ex.family_events[1], ex.family_streams[0]), "cudaEventRecord");
+        cudaStream_t side = fork_side(ex);
+        check_cuda(dev::launch_split_pack_f32(g, 1, L, bp, side), "split pack B");
         check_cuda(dev::launch_split_pack_f32(g, 0, L, ap, ex.stream), "split pack A");
-        check_cuda(cudaStreamWaitEvent(ex.stream, ex.family_events[1], 0), "cudaStreamWaitEvent");
+        join_side(ex);
       }
       Timed t(ex, pr.scheme == Scheme::Bf16x3 ? "tc_bf16x3_gemm" : "tc_bf16x6_gemm");
       check_cuda(dev::launch_tc_bf16_gemm(g, L, ap, bp, (int)pr.scheme, ex.stream, tail),
@@ -590,7 +604,9 @@ void launch_contraction(Product& pr, Executor& ex, const dev::GemmArgs& g, bool 
       char* ws = reinterpret_cast<char*>(align_up((uintptr_t)scratch, 256));
       {
         Timed t(ex, "ozaki_pack");
-        check_cuda(dev::launch_ozaki_pack(g, L, ws, ex.stream), "Ozaki slice pack");
+        cudaStream_t side = fork_side(ex);  // B' packs on a side stream, joined back below
+        check_cuda(dev::launch_ozaki_pack(g, L, ws, ex.stream, side), "Ozaki slice pack");
+        join_side(ex);
       }
       const int nkb = (int)(L.k_pad / 64);
       for (int kb0 = 0; kb0 < nkb; kb0 += L.kb_chunk) {

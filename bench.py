@@ -925,7 +925,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="config 4: the model's tiles instead of autotuned ones")
     ap.add_argument("--grouped-only", action="store_true",
                     help="config 4: time the grouped lists only (no per-item loop, no network driver; profiling runs)")
-    ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 7)")
+    ap.add_argument("--slices", type=int, default=0, help="Ozaki INT8 slices for c1/c3 (0 = the default 6)")
     ap.add_argument("--dtype", default="f64", choices=["f32", "f64", "c32", "c64"], help="dtype of --config gemm")
     ap.add_argument("--size", type=int, default=4096, help="m = n = k of --config gemm")
     ap.add_argument("--kernel", type=int, default=0, help="tile family pinned for --config gemm (0 = the model's)")

@@ -284,7 +284,7 @@ enum {
   TPRIMS_PREC_OZAKI_INT8 = 3 /* f64/c64: INT8 slices, exact INT32 accumulation */
 };
 /* Choose the precision scheme of a product. `slices` is the INT8 slice count
-   for TPRIMS_PREC_OZAKI_INT8 (0 = the default for the dtype) and is ignored
+   for TPRIMS_PREC_OZAKI_INT8 (4..8; 0 = the default, 6) and is ignored
    otherwise. Refused (UNSUPPORTED) for a dtype the scheme does not apply to.
    The reference has no counterpart (its C ABI has no tuning call, product.rs:48). */
 TPRIMS_B200_EXPORT TAPP_error tprims_b200_product_set_precision(TAPP_tensor_product plan, int scheme, int slices);

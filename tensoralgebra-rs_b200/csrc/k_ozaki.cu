@@ -1,17 +1,19 @@
 // Ozaki-style INT8 slice contraction for f64 / c64 on the sm_100a tensor cores.
 //
 // Each row of A' (and each column of B') gets a power-of-two scale 2^e with
-// max |x| < 2^e over that row; the scaled values (|x| < 1) are cut into S
-// signed 7-bit slices, x = sum_t q_t 2^-7(t+1), q_t in [-127, 127], exactly
-// (each step multiplies by 128 and removes the integer part, both exact in
-// FP64). Slice products q_t(A) . q_u(B) accumulate exactly in INT32 on the
-// tensor cores (tcgen05.mma kind::i8); the pairs with t + u = g share the
-// weight 2^-7(g+2) and therefore one accumulator. Only pairs with t + u < S
-// are formed (S(S+1)/2 products), which drops terms below 2^-7S of the row and
-// column scales. The epilogue recombines the S accumulators in FP64 (smallest
-// weight first), applies the row and column scales, then alpha, beta and
-// conjugation (the write-back of crates/tprims-kernel/src/pack/writeback.rs:
-// 311-486).
+// max |x| < 2^e over that row. The scaled value x 2^(8S-2-e) is rounded to
+// the nearest integer T (|T| <= 2^(8S-2)), and T is written as S balanced
+// base-256 digits, T = sum_t d_t 256^(S-1-t): the S-1 low digits in
+// [-128, 127] (eight bits each, the whole INT8 range) and the top digit in
+// [-64, 64]. So x = 2^e sum_t d_t 2^-(8t+6), to within half a unit of
+// 2^(e-8S+2). Slice products d_t(A) . d_u(B) accumulate exactly in INT32 on
+// the tensor cores (tcgen05.mma kind::i8); the pairs with t + u = g share the
+// weight 2^-(8g+12) and therefore one accumulator. Only pairs with t + u < S
+// are formed (S(S+1)/2 products), which drops terms below about 2^-8S of the
+// row and column scales. The epilogue recombines the S accumulators in FP64
+// (smallest weight first), applies the row and column scales, then alpha,
+// beta and conjugation (the write-back of
+// crates/tprims-kernel/src/pack/writeback.rs:311-486).
 //
 // Complex operands are embedded as one real problem of twice the rows and
 // twice the depth: A' row 2r = [Re A_r, -Im A_r], row 2r+1 = [Im A_r, Re A_r],
@@ -20,7 +22,7 @@
 // imaginary parts of row r (the four real products of the planar method);
 // adjacent TMEM lanes hold them and the epilogue pairs them with a shuffle.
 //
-// INT32 exactness needs (g+1) K 127^2 < 2^31 for every diagonal g; the host
+// INT32 exactness needs (g+1) K 128^2 < 2^31 for every diagonal g; the host
 // splits deeper contractions into K chunks that accumulate into D (the KC-slab
 // rule of the reference, driver/tile.rs:312-350).
 #include <climits>
@@ -45,81 +47,91 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// Bytewise negation of four signed bytes each in [-127, 127]:
-// ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256, and (b ^ 0x7f) + 1 never exceeds 255,
-// so no carry crosses into the next byte.
-__device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
-  return ((w ^ 0x7f7f7f7fu) + 0x01010101u) ^ 0x80808080u;
-}
-
 // 2^k for k in [-1022, 1023], built from its bits.
 __device__ __forceinline__ double oz_pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
 
-// The S signed 7-bit slices of four values of one row with exponent e
-// (|x| < 2^e), written as one 4-byte word per plane. T = trunc(x 2^(7S - e)) is
-// exact in int64 (|T| < 2^(7S) <= 2^56) and its base-128 digits, with the sign
-// of x, are the slices: the same digits as repeatedly multiplying the scaled
-// value by 128 and removing the integer part. Digits are cut from the 32-bit
-// halves of |T| (a funnel shift across the boundary), packed four to a word
-// by byte permutes, and negated bytewise where x < 0: for a byte b <= 127,
-// ((b ^ 0x7f) + 1) ^ 0x80 = -b mod 256 without a carry into the next byte.
+// 0x80 in each of the S-1 low bytes: U = T + bias holds the S-1 low balanced
+// digits of T as d + 128 in its low bytes (each in [0, 255], so no carry
+// crosses a byte) and the top digit, in two's complement, from byte S-1 up.
+__host__ __device__ constexpr unsigned long long oz_bias(int S) {
+  unsigned long long c = 0ull;
+  for (int i = 0; i + 1 < S; ++i) c |= 0x80ull << (8 * i);
+  return c;
+}
+
+// T = round(x 2^(8S-2-e)) for four values of one row with exponent e
+// (|x| < 2^e): the product is exact in FP64 and |T| <= 2^(8S-2) <= 2^62. The
+// scale is s1 * s2 (two factors only for rows so small that 8S-2-e is above
+// 1023); e >= -1073 and e <= 1024 keep both exponents in the normal range. A
+// non-finite row (its x are zeros) takes scale 1.
 template <int S>
-__device__ inline void slice_words(const double (&x)[4], int e, uint32_t (&out)[8]) {
-  // Scale 2^(7S - e) as s1 * s2 (two factors only for rows below 2^-967:
-  // 7S - e above 1023). e >= -1074 and e <= 1024 keep both exponents in the
-  // normal range; a non-finite row (its x are zeros) takes scale 1.
-  const int k = e == EXP_NONFINITE ? 0 : 7 * S - e;
+__device__ __forceinline__ void oz_round(const double (&x)[4], int e, long long (&t)[4]) {
+  const int k = e == EXP_NONFINITE ? 0 : 8 * S - 2 - e;
   const bool two = k > 1023;
   const double s1 = oz_pow2(two ? 1000 : k);
   const double s2 = oz_pow2(two ? k - 1000 : 0);
-  uint32_t lo[4], hi[4], negmask = 0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const long long t = (long long)((x[q] * s1) * s2);  // truncation toward zero
-    const unsigned long long mag = (unsigned long long)(t < 0 ? -t : t);
-    lo[q] = (uint32_t)mag;
-    hi[q] = (uint32_t)(mag >> 32);
-    negmask |= (t < 0 ? 0xffu : 0u) << (8 * q);
-  }
+  for (int q = 0; q < 4; ++q) t[q] = __double2ll_rn((x[q] * s1) * s2);
+}
+
+// The S slice words of four biased values U = T + bias (plane sl holds the
+// digit of weight 256^(S-1-sl), one byte per value): byte i of each U, four
+// gathered into one word by byte permutes, with the bias taken off the low
+// digits by flipping their top bit ((d + 128) ^ 0x80 is d in two's
+// complement).
+template <int S>
+__device__ __forceinline__ void oz_planes(const unsigned long long (&u)[4], uint32_t (&out)[8]) {
 #pragma unroll
   for (int sl = 0; sl < S; ++sl) {
-    const int sh = 7 * (S - 1 - sl);
-    uint32_t d[4];
+    const int i = S - 1 - sl;
+    const uint32_t sel = (uint32_t)(i & 3) | ((uint32_t)(4 + (i & 3)) << 4);
+    uint32_t w4[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (sh + 7 <= 32) d[q] = lo[q] >> sh;
-      else if (sh >= 32) d[q] = hi[q] >> (sh - 32);
-      else d[q] = __funnelshift_r(lo[q], hi[q], sh);
-    }
-    // Low bytes of d[0..3] into one word (three byte permutes), then the
-    // 7-bit digits.
-    const uint32_t p01 = __byte_perm(d[0], d[1], 0x0040), p23 = __byte_perm(d[2], d[3], 0x0040);
-    const uint32_t w = __byte_perm(p01, p23, 0x5410) & 0x7f7f7f7fu;
-    out[sl] = (w & ~negmask) | (neg_bytes(w) & negmask);
+    for (int q = 0; q < 4; ++q) w4[q] = i < 4 ? (uint32_t)u[q] : (uint32_t)(u[q] >> 32);
+    const uint32_t p01 = __byte_perm(w4[0], w4[1], sel), p23 = __byte_perm(w4[2], w4[3], sel);
+    const uint32_t w = __byte_perm(p01, p23, 0x5410);
+    out[sl] = i < S - 1 ? w ^ 0x80808080u : w;
   }
 }
 
 template <int S>
 __device__ inline void write_slices_t(const double (&x)[4], int e, int8_t* o, int64_t plane) {
+  long long t[4];
+  oz_round<S>(x, e, t);
+  unsigned long long u[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) u[q] = (unsigned long long)t[q] + oz_bias(S);
   uint32_t w[8];
-  slice_words<S>(x, e, w);
+  oz_planes<S>(u, w);
 #pragma unroll
   for (int sl = 0; sl < S; ++sl) *reinterpret_cast<uint32_t*>(o + sl * plane) = w[sl];
 }
 
 // The four embedded copies of a complex quad of A' (rows 2r and 2r+1, both
-// depth halves: re, -im / im, re) from one digit pass per part: re is stored
-// twice and -im is the bytewise negation of im's slices.
+// depth halves: re, -im / im, re) from one rounding per part: re is stored
+// twice, and the digits of -im are those of -T (bias - T), since a balanced
+// digit -128 has no negation in INT8.
 template <int S>
 __device__ inline void write_slices_a_t(const double (&re)[4], const double (&im)[4], int e, int8_t* o0, int8_t* o1,
                                         int64_t kh, int64_t plane) {
-  uint32_t wr[8], wi[8];
-  slice_words<S>(re, e, wr);
-  slice_words<S>(im, e, wi);
+  long long tr[4], ti[4];
+  oz_round<S>(re, e, tr);
+  oz_round<S>(im, e, ti);
+  unsigned long long ur[4], ui[4], un[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    ur[q] = (unsigned long long)tr[q] + oz_bias(S);
+    ui[q] = (unsigned long long)ti[q] + oz_bias(S);
+    un[q] = oz_bias(S) - (unsigned long long)ti[q];
+  }
+  uint32_t wr[8], wi[8], wn[8];
+  oz_planes<S>(ur, wr);
+  oz_planes<S>(ui, wi);
+  oz_planes<S>(un, wn);
 #pragma unroll
   for (int sl = 0; sl < S; ++sl) {
     *reinterpret_cast<uint32_t*>(o0 + sl * plane) = wr[sl];
-    *reinterpret_cast<uint32_t*>(o0 + kh + sl * plane) = neg_bytes(wi[sl]);
+    *reinterpret_cast<uint32_t*>(o0 + kh + sl * plane) = wn[sl];
     *reinterpret_cast<uint32_t*>(o1 + sl * plane) = wi[sl];
     *reinterpret_cast<uint32_t*>(o1 + kh + sl * plane) = wr[sl];
   }
@@ -745,7 +757,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         for (int c = 0; c < OZ_EPI_COLS / 16; ++c)
           tmem_ld_32x32b_x16(tmem + lane_addr + (uint32_t)(gd * OZ_BN + col0 + c * 16), r[c]);
         tmem_ld_wait();
-        const double w = pow2(-7 * (gd + 2));
+        const double w = pow2(-8 * gd - 12);
 #pragma unroll
         for (int c = 0; c < OZ_EPI_COLS / 16; ++c)
 #pragma unroll
@@ -845,8 +857,8 @@ OzakiLayout ozaki_layout(int slices, bool cplx, int64_t M, int64_t N, int64_t K,
   L.k_pad = (L.k_emb + OZ_BK - 1) / OZ_BK * OZ_BK;
   L.exp_a_pad = (M + 31) / 32 * 32 + 32;
   L.H = H;
-  // INT32 exactness: (S) * k * 127^2 < 2^31 over one chunk of k-blocks.
-  int64_t kmax = ((int64_t)1 << 31) / ((int64_t)slices * 127 * 127);
+  // INT32 exactness: S * k * 128^2 < 2^31 over one chunk of k-blocks.
+  int64_t kmax = (((int64_t)1 << 31) - 1) / ((int64_t)slices * 128 * 128);
   L.kb_chunk = (int)(kmax / OZ_BK);
   if (L.kb_chunk < 1) L.kb_chunk = 1;
   return L;

@@ -9,7 +9,7 @@ complex128 on the same inputs; it is itself pinned to the reference's
 known answers and to the brute-force label oracle (tests/test_oracle.py).
 
 Bounds (relative Frobenius): plain f64 / c64 <= 1e-13, plain f32 <= 1e-6,
-bf16x6 <= 1e-6, bf16x3 <= 2e-5, Ozaki INT8 (7 slices) <= 1e-12."""
+bf16x6 <= 1e-6, bf16x3 <= 2e-5, Ozaki INT8 (6 slices) <= 1e-12."""
 import numpy as np
 import pytest
 

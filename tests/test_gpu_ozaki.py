@@ -1,6 +1,6 @@
 """The Ozaki INT8 slice scheme (f64 / c64 on tcgen05 kind::i8) against the
 extended-precision label oracle, through the C ABI. Stated bound: relative
-Frobenius error <= 1e-12 with the default 7 slices."""
+Frobenius error <= 1e-12 with the default 6 slices."""
 import numpy as np
 import pytest
 
@@ -97,7 +97,7 @@ def test_ozaki_c1_full_size(tp, ex, torch_cuda, orc):
 
 @pytest.mark.parametrize("dt", ["float64", "complex128"])
 def test_ozaki_deep_k_is_split_into_exact_chunks(tp, ex, torch_cuda, orc, dt):
-    # K = 40000 exceeds one INT32-exact chunk (about 19000 at 7 slices); later
+    # K = 40000 exceeds one INT32-exact chunk (about 21800 at 6 slices); later
     # chunks accumulate into D with beta = 1 and op_C = op_D.
     rng = np.random.default_rng(43)
     m, n, k = 5, 6, 40000
@@ -190,3 +190,29 @@ def test_ozaki_batch_innermost_non_finite(tp, ex, torch_cuda, orc, dt):
     assert np.all(bad[:, 4, 5])
     bad[:, 4, 5] = False
     assert not np.any(bad)
+
+
+@pytest.mark.parametrize("dt", ["float64", "complex128"])
+def test_ozaki_extreme_digits(tp, ex, torch_cuda, orc, dt):
+    # Entries at the top of their row's range, (1 - 2^-53) 2^p, round to
+    # T = 2^(8S-2): the top digit at its bound (64) over all-zero low digits.
+    # Exact powers of two, their negations and values one unit of the last
+    # slice apart exercise the digit -128 and its negation in the complex
+    # embedding (-Im A).
+    rng = np.random.default_rng(46)
+    m, n, k = 40, 24, 64
+    top = 1.0 - 2.0 ** -53
+    a = rng.choice([top, -top, 0.5, -0.5, 0.5 + 2.0 ** -47, -(0.5 + 2.0 ** -46), 2.0 ** -30], size=m * k)
+    a = a * np.repeat(2.0 ** rng.integers(-20, 20, size=m), k).reshape(m, k).T.reshape(-1)
+    b = rng.choice([top, -top, 0.25, -0.75, 2.0 ** -40], size=k * n)
+    if dt == "complex128":
+        a = a + 1j * np.roll(a, 3)
+        b = b - 1j * np.roll(b, 5)
+    A = Op(a.astype(dt), [m, k], [1, m], [0, 2], conj=dt == "complex128")
+    B = Op(b.astype(dt), [k, n], [1, k], [2, 1])
+    d0 = np.zeros(m * n, dtype=dt)
+    D = Op(d0, [m, n], [1, m], [0, 1])
+    want = oracle_ref(orc, dt, A, B, None, D, 1.0, 0.0, d0)
+    got, p = oz(tp, ex, torch_cuda, dt, A, B, None, D, 1.0, 0.0)
+    assert ".s6." in p.report()["family"], p.report()["family"]
+    assert orc.rel_frobenius(got, want) <= 1e-12

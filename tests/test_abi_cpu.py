@@ -249,6 +249,27 @@ def test_split_precision_applies_to_f32_only(tp):
     assert q.report()["scheme"] == "bf16x6"
 
 
+def test_ozaki_slice_count_default_and_range(tp):
+    """The Ozaki scheme takes 4 to 8 INT8 slices, six by default (21 slice
+    products), and applies to f64 / c64 only."""
+    specs = ({"ext": [2, 2], "str": [1, 2], "lab": [0, 2]}, {"ext": [2, 2], "str": [1, 2], "lab": [2, 1]},
+             {"ext": [2, 2], "str": [1, 2], "lab": [0, 1]})
+    for dt in (tp.F64, tp.C64):
+        p = _product(tp, *specs, dtype=dt)
+        p.set_precision(tp.PREC_OZAKI_INT8)
+        assert ".ozaki-int8.s6." in p.report()["family"], p.report()
+        p.set_precision(tp.PREC_OZAKI_INT8, 8)
+        assert ".ozaki-int8.s8." in p.report()["family"]
+        for bad in (3, 9):
+            with pytest.raises(tp.TprimsError) as e:
+                p.set_precision(tp.PREC_OZAKI_INT8, bad)
+            assert e.value.status == tp.ERR_INVALID_ARGUMENT
+    q = _product(tp, *specs, dtype=tp.F32)
+    with pytest.raises(tp.TprimsError) as e:
+        q.set_precision(tp.PREC_OZAKI_INT8)
+    assert e.value.status == tp.ERR_UNSUPPORTED
+
+
 def test_executor_handles_without_a_gpu(tp):
     import ctypes as C
 

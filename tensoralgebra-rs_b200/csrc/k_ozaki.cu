@@ -543,9 +543,10 @@ struct OzCfg {
   static constexpr int A_TILE = OZ_BM * OZ_SK;  // bytes of one A plane tile
   static constexpr int B_TILE = OZ_BN * OZ_SK;
   // A and B slice tiles of a k-block live in two rings of their own: three A
-  // stages when they fit beside two B stages (seven slices: 3 x 56 KB + 2 x
-  // 28 KB), so more operand bytes are in flight per SM than two whole
-  // 84 KB stages allow.
+  // stages when they fit beside two B stages, and a third B stage when it
+  // fits too (six slices: 3 x 48 KB + 3 x 24 KB; seven: 3 x 56 KB + 2 x
+  // 28 KB), so more operand bytes are in flight per SM than whole stages of
+  // both operands allow.
   static constexpr int A_STAGE = S * A_TILE, B_STAGE = S * B_TILE;
   static constexpr int LIMIT = 222 * 1024;
   static constexpr int A_STAGES = (3 * A_STAGE + 2 * B_STAGE <= LIMIT) ? 3 : 2;

@@ -270,6 +270,31 @@ def test_ozaki_slice_count_default_and_range(tp):
     assert e.value.status == tp.ERR_UNSUPPORTED
 
 
+def test_ozaki_workspace_follows_the_slice_count(tp):
+    """The Ozaki workspace of the C3 shape (c64, batch 64 innermost, 384^3,
+    conj A): S INT8 planes of the embedded A' (2M rows, padded to 128; depth
+    2K, each half padded to 64) and of B' (N rows, padded to 64), plus the
+    per-row and per-column exponents."""
+    b, e = 64, 384
+    h = tp.Handle()
+    info = tp.TensorInfo(tp.C64, [b, e, e], [1, b, b * e])
+    p = tp.TensorProduct.create(h, (1, info, [9, 2, 0]), (0, info, [9, 2, 1]), (0, info, [9, 0, 1]),
+                                (0, info, [9, 0, 1]))
+    p._keep = (h, info)
+
+    def expected(s):
+        k_emb = 2 * ((e + 63) // 64 * 64)
+        m_pad, n_pad = (2 * e + 127) // 128 * 128, (e + 63) // 64 * 64
+        exps = (b * ((e + 31) // 32 * 32 + 32) + b * n_pad) * 4
+        return s * b * m_pad * k_emb + s * b * n_pad * k_emb + exps + 1024
+
+    for s in (6, 7, 4, 8):
+        p.set_precision(tp.PREC_OZAKI_INT8, s)
+        assert p.report()["scratch_bytes"] == expected(s), (s, p.report()["scratch_bytes"], expected(s))
+    p.set_precision(tp.PREC_OZAKI_INT8)
+    assert p.report()["scratch_bytes"] == expected(6)
+
+
 def test_executor_handles_without_a_gpu(tp):
     import ctypes as C
 
